@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of swfwi's batched FWI gradient on B200.
+
+One step = one batched FWI gradient over all 96 shots of the 301 x 921 grid
+(dx 10 m, dt 1 ms, nt 4000, 15 Hz Ricker, 30-point sponge, seeded uneven
+receiver spreads of 200-921 points): forward modelling with boundary-strip
+save, direct-arrival mute, residual and FP64 objective, time derivative,
+back-propagation of the source field with adjoint receiver propagation and
+imaging, gradient scale/mask and the sum over shots.  Inputs are resident in
+HBM when the timed region starts (the velocity, the wavelet and all observed
+shots, 0.6 GB).
+
+value: stencil point-updates executed per second over the timed steps
+(Gpts/s), device-timed with CUDA events, max over ranks.  e2e: the same
+gradient through the C ABI from pinned host buffers, host-device copies
+inside the timed region.  --impl reference: the reference's own CPU code
+(oracle/_ref, OpenMP over all host cores) on a bounded sample of the same
+workload.
+
+Multi-GPU: replicas only (the workload runs on one GPU; N ranks run N
+independent copies, value = all ranks' point-updates / max time).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FD Gpts/s (% HBM roofline); FWI wall-clock to equal model L2, learned vs plain"
+CONFIG = "batched"
+CPU_SAMPLE_NT = 1500
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic_per_point():
+    """DRAM bytes per stencil point-update from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "fd_step_batched_traffic.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_point_update:\s*([0-9.]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+def backward_steps(nt: int, dt: float) -> int:
+    """Back-propagation steps calgradient performs (fwiframework.cpp:146-176):
+    it runs from nt-1 down and stops after the first step with dt*it <= 0.3 s."""
+    n = 0
+    dt32 = np.float32(dt)
+    for it in range(nt - 1, -1, -1):
+        n += 1
+        t = float(np.float32(dt32 * np.float32(it)))
+        if not t > 0.3:
+            break
+    return n
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, fl in rows for i, v in enumerate(fl) if v.lower() == "active"})
+        sm = sorted(r[0] for r in rows)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def setup_workload(torch, arith):
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    s = sv.config(CONFIG)
+    vtrue = sv.layered_model(s.nx, s.nz, seed=2024)
+    vinit = sv.smooth(vtrue, 15.0).astype(np.float32)
+    m = S.Damp4t10d.from_survey(s, arith=arith)
+    ext = torch.from_numpy(m.expandDomain(vtrue)).cuda()
+    exi_h = m.expandDomain(vinit)
+    exi = torch.from_numpy(exi_h).cuda()
+    wlt_h = S.ricker_wavelet(s.nt, s.fm, s.dt, 1.0)
+    wlt = torch.from_numpy(wlt_h).cuda()
+    ids = np.arange(s.ns, dtype=np.int32)
+    nxpad, nzpad, ns, ngmax, nt = m.dims()
+    dobs = torch.zeros((ns, nt, ngmax), dtype=torch.float32, device="cuda")
+    m.bindVelocity(ext)
+    m.forward_batch(wlt, dobs, ids)          # observed data: the true model
+    m.bindVelocity(exi)
+    torch.cuda.synchronize()
+    return s, m, exi, exi_h, wlt, wlt_h, dobs, ids
+
+
+def cpu_reference_sample(nt_sample=CPU_SAMPLE_NT, repeats=1):
+    """The reference's gradient loop on one shot of the workload with the
+    time axis cut to nt_sample steps, OpenMP over all host cores."""
+    import oracle
+    from swfwi_b200 import survey as sv
+    if not oracle.available():
+        return None
+    s = sv.config(CONFIG)
+    off, gx, _ = s.spreads
+    n0 = int(off[1] - off[0])
+    ss = s.scaled(nt=nt_sample, ns=1, ng=n0, gxbeg=int(gx[0]), spreads=None)
+    R = oracle.RefLib()
+    M = R.model(ss)
+    vtrue = sv.layered_model(s.nx, s.nz, seed=2024)
+    vinit = sv.smooth(vtrue, 15.0).astype(np.float32)
+    wlt = R.ricker(ss.nt, ss.fm, ss.dt)
+    M.expand_domain(vtrue)
+    dobs = M.fwi_forward(wlt, 0)[None]
+    M.expand_domain(vinit)
+    pts = (M.nxpad - 12) * (M.nzpad - 12)
+    updates = pts * (2 * ss.nt + 2 * backward_steps(ss.nt, ss.dt))
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        M.fwi_gradient(wlt, dobs)
+        times.append(time.perf_counter() - t0)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"seconds": min(times), "updates": updates, "cores": cores,
+            "sample": f"one shot ({n0} receivers), nt={ss.nt}, full {M.nxpad}x{M.nzpad} padded grid, "
+                      f"reference gradient loop (FwiForwardModeling, mute, residual, transVsrc, "
+                      f"calgradient, scale/mask)"}
+
+
+def run_reference(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    import oracle
+    if not oracle.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled "
+                          "from its sources) is not built"}))
+        return 0
+    for _ in range(args.warmup):
+        cpu_reference_sample(repeats=1)
+    tot_t, tot_u, info = 0.0, 0, None
+    for _ in range(args.steps):
+        info = cpu_reference_sample(repeats=1)
+        tot_t += info["seconds"]
+        tot_u += info["updates"]
+    v = tot_u / tot_t / 1e9
+    line = {"metric": METRIC, "value": v, "unit": "Gpts/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_t / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "batched FWI gradient sample (reference CPU)", "grid": "301x921",
+                       "nt": CPU_SAMPLE_NT, "shots": 1},
+            "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": info["cores"], "kind": "reference",
+                             "sample": info["sample"]},
+            "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--arith", default="ref", choices=["ref", "fast"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import swfwi_b200 as S
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    arith = S.ARITH_REF if args.arith == "ref" else S.ARITH_FAST
+    s, m, exi, exi_h, wlt, wlt_h, dobs, ids = setup_workload(torch, arith)
+    nxpad, nzpad, ns, ngmax, nt = m.dims()
+    grad = torch.zeros((nxpad, nzpad), dtype=torch.float32, device="cuda")
+
+    for _ in range(max(args.warmup, 0)):
+        m.gradient_batch(wlt, dobs, ids, grad)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    S.stats_reset()
+    S.stats_enable_step_timing(True)
+    clk = ClockSampler(local)
+    clk.start()
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    objs = None
+    for _ in range(args.steps):
+        objs = m.gradient_batch(wlt, dobs, ids, grad)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1)
+    st = S.stats_read()
+    S.stats_enable_step_timing(False)
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    updates_rank = st["step_point_updates"]
+    value = updates_rank * world / (ms_max * 1e-3) / 1e9
+
+    # dominant kernel: the stencil step, timed per launch with CUDA events
+    peak, peak_kind = measured_peaks()
+    step_gbs = st["step_bytes"] / (st["step_ms"] * 1e-3) / 1e9 if st["step_ms"] > 0 else 0.0
+    per_launch_pts = st["step_point_updates"] / max(st["step_launches"], 1)
+    tpp = profile_traffic_per_point()
+    roofline = {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                "frac": step_gbs / peak, "peak_basis": peak_kind,
+                "traffic": (tpp * per_launch_pts) if tpp else None,
+                "kernel": "fd_step_tile", "launches": st["step_launches"],
+                "avg_launch_us": st["step_ms"] * 1e3 / max(st["step_launches"], 1),
+                "bytes_per_launch": st["step_bytes"] / max(st["step_launches"], 1),
+                "stencil_share_of_step": st["step_ms"] / ms if ms > 0 else None}
+
+    # end to end through the C ABI from pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        dobs_h = torch.empty(dobs.shape, dtype=torch.float32, pin_memory=True)
+        dobs_h.copy_(dobs.cpu())
+        exi_p = torch.from_numpy(exi_h).pin_memory()
+        wlt_p = torch.from_numpy(wlt_h).pin_memory()
+        grad_p = torch.empty((nxpad, nzpad), dtype=torch.float32, pin_memory=True)
+        m.gradient_host(exi_p.numpy(), wlt_p.numpy(), dobs_h.numpy(), ids, grad_p.numpy())
+        S.stats_reset()
+        S.stats_enable_step_timing(True)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            m.gradient_host(exi_p.numpy(), wlt_p.numpy(), dobs_h.numpy(), ids, grad_p.numpy())
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        st2 = S.stats_read()
+        S.stats_enable_step_timing(False)
+        if dist is not None:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        h2d = exi_p.numel() * 4 + wlt_p.numel() * 4 + dobs_h.numel() * 4
+        e2e = {"value": st2["step_point_updates"] * world / dt / 1e9, "unit": "Gpts/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(grad_p.numel() * 4 + 8 * ns),
+               "ms_per_step": dt / args.e2e_steps * 1e3}
+        m.bindVelocity(exi)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            info = cpu_reference_sample()
+            if info:
+                cpu = {"value": info["updates"] / info["seconds"] / 1e9, "unit": "Gpts/s",
+                       "cores": info["cores"], "kind": "reference", "sample": info["sample"],
+                       "seconds": info["seconds"]}
+        except Exception as e:   # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Gpts/s", "cores": 0, "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched FWI gradient, 96 shots, 301x921 grid (993x337 padded), "
+                                       "nt=4000, uneven spreads 200-921",
+                           "shots": int(ns), "nt": int(nt), "grid": [int(nxpad), int(nzpad)],
+                           "arith": args.arith, "strips": "f32",
+                           "point_updates_per_step": updates_rank / args.steps,
+                           "l2": "inputs larger than L2 (strips 14 GB, fields 0.5 GB): no flush",
+                           "parallelism": f"replicas{world}",
+                           "objective_last_step": float(np.sum(objs)) if objs is not None else None},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(st["kernel_launches"]), "clocks": clocks}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,265 @@
+/*
+ * swfwi_gpu.h - C ABI of the B200 (sm_100a) implementation of swfwi's 2D
+ * acoustic FWI path.
+ *
+ * Conventions (the reference's, kept so callers can switch):
+ *  - Grids are x-major with z contiguous: p[ix*nzpad + iz].
+ *  - nxpad = nx + 2*nb + 12, nzpad = nz + nb + 12 (free surface on top,
+ *    nb sponge cells left/right/bottom, a 6-cell stencil halo all round).
+ *  - Velocities handed to the propagator are padded and transformed,
+ *    vt = dx^2 / (v^2 dt^2).
+ *  - Seismic data are time-major per shot: d[it*ng + ig]; a set of shots is
+ *    [shot][it][ig].
+ *  - Field, data and velocity pointers are DEVICE pointers unless a function
+ *    says "host"; scalar outputs are host pointers.
+ *  - Every entry point returns a status (SWFWI_OK = 0).  swfwi_last_error()
+ *    gives the text of the last failure on the calling thread.
+ *  - Calls on one handle are ordered on that handle's CUDA stream
+ *    (swfwi_damp4t10d_set_stream); functions that return host values
+ *    synchronise that stream.
+ */
+#ifndef SWFWI_GPU_H
+#define SWFWI_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SWFWI_OK = 0,
+  SWFWI_ERR_BAD_ARG = 1,   /* invalid size, index or pointer */
+  SWFWI_ERR_OOM = 2,       /* device or host allocation failed */
+  SWFWI_ERR_TIMEOUT = 3,   /* a bounded device wait gave up */
+  SWFWI_ERR_NONFINITE = 4, /* NaN/Inf found where a finite value is required */
+  SWFWI_ERR_CUDA = 5,      /* CUDA runtime error */
+  SWFWI_ERR_STATE = 6      /* call made in the wrong state (e.g. no velocity bound) */
+};
+
+/* Arithmetic of the stencil.
+ *  REF : float fields, every operation rounded exactly as the reference's C
+ *        source is on x86-64 (bit-identical results).
+ *  FAST: float fields, FP32 with fused multiply-add (tolerance parity).
+ *  F64 : the same scheme in double, used as the FP64 oracle. */
+enum { SWFWI_ARITH_REF = 0, SWFWI_ARITH_FAST = 1, SWFWI_ARITH_F64 = 2 };
+
+/* Storage of the boundary strips used to rebuild the source wavefield
+ * backwards.  F32 is exact; F16/BF16 keep one scale per strip and step. */
+enum { SWFWI_STRIP_F32 = 0, SWFWI_STRIP_F16 = 1, SWFWI_STRIP_BF16 = 2 };
+
+const char *swfwi_status_string(int status);
+const char *swfwi_last_error(void);
+int swfwi_version(void);
+
+/* ------------------------------------------------------------------------
+ * Drop-in stencil steps.  Same arguments and in-place semantics as the
+ * reference kernels, on device memory, plus a CUDA stream (NULL = default
+ * stream).  nx, nz are padded sizes, vel is transformed, nb is the damping
+ * ramp length (the reference passes Damp4t10d::bx0 = sponge + 6).  prev is
+ * overwritten on [6, nx-6) x [6, nz-6) with the next field; u2 is accepted
+ * for signature compatibility and not touched (the Laplacian stays on chip),
+ * so it may be NULL.  REF arithmetic: bit-identical to the reference.
+ * ---------------------------------------------------------------------- */
+
+/* replaces fd4t10s_damp_zjh_2d_vtrans, src/modeling/fd4t10s-damp-zjh.h:11 */
+int swfwi_fd4t10s_damp_zjh_2d_vtrans(float *prev, const float *curr, const float *vel, float *u2,
+                                     int nx, int nz, int nb, void *stream);
+/* replaces fd4t10s_zjh_2d_vtrans, src/modeling/fd4t10s-zjh.h:11 */
+int swfwi_fd4t10s_zjh_2d_vtrans(float *prev, const float *curr, const float *vel, float *u2, int nx,
+                                int nz, void *stream);
+/* Either step with a chosen arithmetic (REF or FAST) and nshots fields
+ * laid out shot_stride floats apart sharing one velocity (batched form of
+ * the two functions above; same per-field semantics). */
+int swfwi_fd4t10s_step_batch(float *prev, const float *curr, const float *vel, int nx, int nz,
+                             int nb, int damped, int arith, int nshots, long long shot_stride,
+                             void *stream);
+/* FP64 oracle step (double fields and velocity). */
+int swfwi_fd4t10s_step_f64(double *prev, const double *curr, const double *vel, int nx, int nz,
+                           int nb, int damped, void *stream);
+
+/* ------------------------------------------------------------------------
+ * ShotPosition (src/common/shot-position.h:13-27): a regular line of
+ * points, point i at z = szbeg + i*jsz, x = sxbeg + i*jsx (unpadded grid
+ * indices).  nz is the unpadded model depth, as in the reference.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int szbeg, sxbeg, jsz, jsx, ns, nz;
+} swfwi_shot_position;
+
+/* ------------------------------------------------------------------------
+ * Damp4t10d (src/modeling/damp4t10d.h:18-87): the propagator object.
+ * ---------------------------------------------------------------------- */
+typedef struct swfwi_damp4t10d swfwi_damp4t10d;
+
+/* Damp4t10d::Damp4t10d (damp4t10d.cpp:367-376). */
+int swfwi_damp4t10d_create(swfwi_damp4t10d **out, const swfwi_shot_position *src,
+                           const swfwi_shot_position *geo, float dt, float dx, float fm, int nb,
+                           int nt);
+int swfwi_damp4t10d_destroy(swfwi_damp4t10d *h);
+/* Order this handle's work on a caller stream (cudaStream_t); NULL returns
+ * to the handle's own stream. */
+int swfwi_damp4t10d_set_stream(swfwi_damp4t10d *h, void *stream);
+int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith);
+int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
+/* Per-shot receiver lists (uneven spreads; not in the reference, whose
+ * ShotPosition is one common line): shot s has receivers
+ * [offsets[s], offsets[s+1]) of gx/gz (unpadded, host arrays).  The
+ * common line set at creation stays the one the single-shot calls use. */
+int swfwi_damp4t10d_set_receivers_per_shot(swfwi_damp4t10d *h, const int *offsets, const int *gx,
+                                           const int *gz);
+int swfwi_damp4t10d_dims(const swfwi_damp4t10d *h, int *nxpad, int *nzpad, int *ns, int *ng,
+                         int *nt);
+/* Damp4t10d::expandDomain (damp4t10d.cpp:138-151).  Host arrays:
+ * vel [nx][nz] in m/s -> exvel [nxpad][nzpad] transformed.  Also fixes the
+ * grid size of the handle (as binding the expanded Velocity does). */
+int swfwi_damp4t10d_expand_domain(swfwi_damp4t10d *h, const float *vel, int nx, int nz,
+                                  float *exvel);
+/* Fix the grid size without expanding (for a velocity expanded
+ * elsewhere): nx, nz unpadded. */
+int swfwi_damp4t10d_set_model_size(swfwi_damp4t10d *h, int nx, int nz);
+/* Damp4t10d::bindVelocity (damp4t10d.cpp:159-161): the padded transformed
+ * velocity, device; kept by pointer as the reference keeps a reference.
+ * Re-bind after changing it in place. */
+int swfwi_damp4t10d_bind_velocity(swfwi_damp4t10d *h, const float *exvel);
+/* stepForward (damp4t10d.cpp:153-157): damped step, p0 <- F(p0, p1). */
+int swfwi_damp4t10d_step_forward(swfwi_damp4t10d *h, float *p0, float *p1);
+/* stepBackward (damp4t10d.cpp:188-191): undamped step. */
+int swfwi_damp4t10d_step_backward(swfwi_damp4t10d *h, float *p0, float *p1);
+/* addSource/subSource for one shot (curSrcPos = allSrcPos.clip(shot));
+ * shot_id = -1: every source, source[is] (addEncodedSource /
+ * subEncodedSource, damp4t10d.cpp:193-214, 378-384).  source is device. */
+int swfwi_damp4t10d_add_source(swfwi_damp4t10d *h, float *p, const float *source, int shot_id);
+int swfwi_damp4t10d_sub_source(swfwi_damp4t10d *h, float *p, const float *source, int shot_id);
+/* addSource(p, vsrc_it, allGeoPos): inject one value per receiver. */
+int swfwi_damp4t10d_add_receiver_source(swfwi_damp4t10d *h, float *p, const float *vsrc_it);
+/* recordSeis (damp4t10d.cpp:163-180, 386-388). */
+int swfwi_damp4t10d_record_seis(swfwi_damp4t10d *h, float *seis_it, const float *p);
+/* initBndryVector/writeBndry/readBndry (damp4t10d.cpp:447-536): FP32
+ * strips, reference layout, bndr holds nt * size floats. */
+int swfwi_damp4t10d_bndry_size(const swfwi_damp4t10d *h, int *size);
+int swfwi_damp4t10d_write_bndry(swfwi_damp4t10d *h, float *bndr, const float *p, int it);
+int swfwi_damp4t10d_read_bndry(swfwi_damp4t10d *h, const float *bndr, float *p, int it);
+/* maskGradient :216-226, scaleGradient :309-319, refillBoundary :228-252 */
+int swfwi_damp4t10d_mask_gradient(swfwi_damp4t10d *h, float *grad);
+int swfwi_damp4t10d_scale_gradient(swfwi_damp4t10d *h, float *grad);
+int swfwi_damp4t10d_refill_boundary(swfwi_damp4t10d *h, float *vel);
+/* fwiRemoveDirectArrival (shot_id >= 0) / removeDirectArrival (shot_id =
+ * -1), damp4t10d.cpp:321-365, 390-394: data [nt][ng] in place. */
+int swfwi_damp4t10d_remove_direct_arrival(swfwi_damp4t10d *h, float *data, int shot_id);
+/* FwiForwardModeling (damp4t10d.cpp:272-289): wlt [nt] -> dcal [nt][ng]. */
+int swfwi_damp4t10d_fwi_forward_modeling(swfwi_damp4t10d *h, const float *wlt, float *dcal,
+                                         int shot_id);
+/* EssForwardModeling (damp4t10d.cpp:291-307): encsrc [nt][ns]. */
+int swfwi_damp4t10d_ess_forward_modeling(swfwi_damp4t10d *h, const float *encsrc, float *dcal);
+
+/* ------------------------------------------------------------------------
+ * Batched whole-shot operations (the fast path): nshots shots of
+ * shot_ids[] (host) run as one set of launches per time step.
+ * ---------------------------------------------------------------------- */
+/* FwiForwardModeling for every listed shot: dcal [nshots][nt][ng]. */
+int swfwi_damp4t10d_forward_batch(swfwi_damp4t10d *h, const float *wlt, float *dcal,
+                                  const int *shot_ids, int nshots);
+/* The per-shot gradient loop of FwiFramework::epoch (fwiframework.cpp:
+ * 274-324) for the listed shots: forward modelling, direct-arrival mute of
+ * observed and modelled data, residual, objective, time derivative,
+ * calgradient (:114-177), scaleGradient, maskGradient, and the sum over
+ * shots in list order.  dobs [ns][nt][ng] (device, all shots), grad
+ * [nxpad][nzpad] (device, overwritten), obj [nshots] (host, FP64 sums of
+ * squared residuals). */
+int swfwi_damp4t10d_gradient_batch(swfwi_damp4t10d *h, const float *wlt, const float *dobs,
+                                   const int *shot_ids, int nshots, float *grad, double *obj);
+/* Same from HOST buffers (copies in and out inside the call): exvel
+ * [nxpad][nzpad], wlt [nt], dobs [nshots][nt][ng] for the listed shots,
+ * grad [nxpad][nzpad]. */
+int swfwi_gradient_host(swfwi_damp4t10d *h, const float *exvel, const float *wlt,
+                        const float *dobs, const int *shot_ids, int nshots, float *grad,
+                        double *obj);
+/* Encoded-source gradient (essfwiframework.cpp:114-173) on device:
+ * encsrc [nt][ns], vsrc [nt][ng]; grad accumulates (not scaled). */
+int swfwi_damp4t10d_calgradient_ess(swfwi_damp4t10d *h, const float *encsrc, const float *vsrc,
+                                    float *grad);
+/* Plain per-shot gradient (fwiframework.cpp:114-177) on device; grad
+ * accumulates (not scaled). */
+int swfwi_damp4t10d_calgradient_fwi(swfwi_damp4t10d *h, const float *wlt, const float *vsrc,
+                                    float *grad, int shot_id);
+/* FP64 oracle run of the per-shot gradient scheme (double fields, exact
+ * strips): vel is the float transformed velocity (device), wlt/vsrc/grad are
+ * double (device); grad accumulates. */
+int swfwi_damp4t10d_calgradient_fwi_f64(swfwi_damp4t10d *h, const float *vel, const double *wlt,
+                                        const double *vsrc, double *grad, int shot_id);
+/* FP64 forward modelling of one shot (double dcal, device). */
+int swfwi_damp4t10d_fwi_forward_modeling_f64(swfwi_damp4t10d *h, const float *vel,
+                                             const double *wlt, double *dcal, int shot_id);
+
+/* ------------------------------------------------------------------------
+ * Per-iteration arithmetic (device arrays of n = nxpad*nzpad floats).
+ * ---------------------------------------------------------------------- */
+/* updateGrad (fwiframework.cpp:42-72): PR+ conjugate gradient; the dot
+ * products are accumulated in FP64.  pre, dir updated in place. */
+int swfwi_update_grad(float *pre_gradient, const float *cur_gradient, float *update_direction,
+                      int n, int iter, void *stream);
+/* calMaxAlpha2_3 (updatesteplenop.cpp:25-47). */
+int swfwi_cal_max_alpha(const float *vel, const float *grad, int n, float dt, float dx, float maxdv,
+                        float *alpha2, float *alpha3, void *stream);
+/* UpdateVelOp::update (updatevelop.cpp:11-37), vmin/vmax in m/s. */
+int swfwi_update_vel(float *new_vel, const float *vel, const float *grad, int n, float steplen,
+                     float vmin, float vmax, float dx, float dt, void *stream);
+/* second_order_virtual_source_forth_accuracy over [nt][ng] (transVsrc,
+ * fwiframework.cpp:75-105), out of place. */
+int swfwi_trans_vsrc(float *out, const float *in, int nt, int ng, void *stream);
+/* sum of squares of n floats in FP64 (cal_objective, common.cpp:231-241). */
+int swfwi_cal_objective(const float *r, long long n, double *obj, void *stream);
+/* parabolaVertex (parabola-vertex.cpp:12-33), host. */
+int swfwi_parabola_vertex(float x1, float y1, float x2, float y2, float x3, float y3,
+                          float max_alpha3, float *xv, float *yv);
+/* rickerWavelet (ricker-wavelet.cpp:15-31), host. */
+int swfwi_ricker_wavelet(float *wlt, int nt, float fm, float dt, float amp);
+/* RandomCodes::genPlus1Minus1 (random-code.cpp:2-22): +-1 codes of a
+ * minstd_rand stream with the given seed, after skip earlier batches of
+ * n codes.  Host. */
+int swfwi_random_codes(int seed, int skip, int n, int *codes);
+
+/* ------------------------------------------------------------------------
+ * FwiFramework / EssFwiFramework (src/fwi/fwiframework.h:16-53,
+ * src/essfwi/essfwiframework.h:16-53) with their step-length and velocity
+ * update operators.  encoded = 0: plain FWI over all shots; 1: one
+ * +-1-encoded supershot per epoch.  wlt [nt], dobs [ns][nt][ng]: host.
+ * ---------------------------------------------------------------------- */
+typedef struct swfwi_fwi swfwi_fwi;
+int swfwi_fwi_create(swfwi_fwi **out, swfwi_damp4t10d *method, const float *exvel, float vmin,
+                     float vmax, int nita, float maxdv, const float *wlt, const float *dobs,
+                     int encoded);
+int swfwi_fwi_destroy(swfwi_fwi *h);
+int swfwi_fwi_epoch(swfwi_fwi *h, int iter);
+int swfwi_fwi_get_update_obj(const swfwi_fwi *h, float *obj);
+int swfwi_fwi_get_init_obj(const swfwi_fwi *h, float *obj);
+/* current padded transformed velocity, host [nxpad][nzpad] */
+int swfwi_fwi_get_velocity(swfwi_fwi *h, float *exvel);
+/* sfWriteVel (damp4t10d.cpp:254-265) without the file: interior velocity in
+ * m/s, host [nx][nz]. */
+int swfwi_fwi_write_vel(swfwi_fwi *h, float *vel);
+/* last epoch's step length and trial record: alpha[4], obj[4] (host) */
+int swfwi_fwi_last_line_search(const swfwi_fwi *h, float *alpha, float *obj);
+
+/* ------------------------------------------------------------------------
+ * Measurement (no counterpart in the reference, which prints wall-clock
+ * timers only, src/common/timer.h:14-29).  Process-wide counters of kernel
+ * launches and, when enabled, CUDA-event timing of every stencil launch on
+ * its own stream with its algorithmic work (interior point-updates; bytes =
+ * 12 per point-update plus 4 per point per velocity model read).
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  long long kernel_launches;
+  long long step_launches;
+  double step_ms;
+  double step_point_updates;
+  double step_bytes;
+} swfwi_stats;
+int swfwi_stats_reset(void);
+int swfwi_stats_enable_step_timing(int on);
+/* waits for the timed launches to finish */
+int swfwi_stats_read(swfwi_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWFWI_GPU_H */

@@ -1,0 +1,518 @@
+"""swfwi_b200: swfwi's 2D acoustic FWI path on NVIDIA B200 (sm_100a).
+
+The product is the shared library ``libswfwi_b200.so`` (C ABI in
+``include/swfwi_gpu.h``).  This module is a thin ctypes mirror of the
+reference's C++ interface for tests, benchmarks and Python callers:
+
+* ``fd4t10s_damp_zjh_2d_vtrans`` / ``fd4t10s_zjh_2d_vtrans``: the drop-in
+  stencil steps (src/modeling/fd4t10s-*.h).
+* ``ShotPosition``, ``Damp4t10d``: the propagator (src/modeling/damp4t10d.h),
+  method names as in the reference.
+* ``FwiFramework``, ``EssFwiFramework``: the inversion drivers
+  (src/fwi/fwiframework.h, src/essfwi/essfwiframework.h).
+
+Device arrays are torch CUDA tensors (torch is used for device memory and
+streams only; every computation runs in the library's kernels).  There is
+no CPU fallback: loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libswfwi_b200.so")
+
+ARITH_REF, ARITH_FAST, ARITH_F64 = 0, 1, 2
+STRIP_F32, STRIP_F16, STRIP_BF16 = 0, 1, 2
+
+
+class SwfwiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"swfwi status {status}: {msg}")
+        self.status = status
+
+
+class Stats(C.Structure):
+    _fields_ = [("kernel_launches", C.c_longlong), ("step_launches", C.c_longlong),
+                ("step_ms", C.c_double), ("step_point_updates", C.c_double), ("step_bytes", C.c_double)]
+
+
+class _ShotPos(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("szbeg", "sxbeg", "jsz", "jsx", "ns", "nz")]
+
+
+_lib = None
+_vp, _fp, _dp, _ip = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)
+
+_SIGS = {
+    "swfwi_fd4t10s_damp_zjh_2d_vtrans": [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp],
+    "swfwi_fd4t10s_zjh_2d_vtrans": [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_fd4t10s_step_batch": [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_longlong, _vp],
+    "swfwi_fd4t10s_step_f64": [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp],
+    "swfwi_damp4t10d_create": [C.POINTER(_vp), C.POINTER(_ShotPos), C.POINTER(_ShotPos), C.c_float,
+                               C.c_float, C.c_float, C.c_int, C.c_int],
+    "swfwi_damp4t10d_destroy": [_vp],
+    "swfwi_damp4t10d_set_stream": [_vp, _vp],
+    "swfwi_damp4t10d_set_arith": [_vp, C.c_int],
+    "swfwi_damp4t10d_set_strip_format": [_vp, C.c_int],
+    "swfwi_damp4t10d_set_receivers_per_shot": [_vp, _ip, _ip, _ip],
+    "swfwi_damp4t10d_dims": [_vp, _ip, _ip, _ip, _ip, _ip],
+    "swfwi_damp4t10d_expand_domain": [_vp, _fp, C.c_int, C.c_int, _fp],
+    "swfwi_damp4t10d_set_model_size": [_vp, C.c_int, C.c_int],
+    "swfwi_damp4t10d_bind_velocity": [_vp, _vp],
+    "swfwi_damp4t10d_step_forward": [_vp, _vp, _vp],
+    "swfwi_damp4t10d_step_backward": [_vp, _vp, _vp],
+    "swfwi_damp4t10d_add_source": [_vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_sub_source": [_vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_add_receiver_source": [_vp, _vp, _vp],
+    "swfwi_damp4t10d_record_seis": [_vp, _vp, _vp],
+    "swfwi_damp4t10d_bndry_size": [_vp, _ip],
+    "swfwi_damp4t10d_write_bndry": [_vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_read_bndry": [_vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_mask_gradient": [_vp, _vp],
+    "swfwi_damp4t10d_scale_gradient": [_vp, _vp],
+    "swfwi_damp4t10d_refill_boundary": [_vp, _vp],
+    "swfwi_damp4t10d_remove_direct_arrival": [_vp, _vp, C.c_int],
+    "swfwi_damp4t10d_fwi_forward_modeling": [_vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_ess_forward_modeling": [_vp, _vp, _vp],
+    "swfwi_damp4t10d_forward_batch": [_vp, _vp, _vp, _ip, C.c_int],
+    "swfwi_damp4t10d_gradient_batch": [_vp, _vp, _vp, _ip, C.c_int, _vp, _dp],
+    "swfwi_gradient_host": [_vp, _fp, _fp, _fp, _ip, C.c_int, _fp, _dp],
+    "swfwi_damp4t10d_calgradient_ess": [_vp, _vp, _vp, _vp],
+    "swfwi_damp4t10d_calgradient_fwi": [_vp, _vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_calgradient_fwi_f64": [_vp, _vp, _vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_fwi_forward_modeling_f64": [_vp, _vp, _vp, _vp, C.c_int],
+    "swfwi_update_grad": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_cal_max_alpha": [_vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float, _fp, _fp, _vp],
+    "swfwi_update_vel": [_vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                         C.c_float, _vp],
+    "swfwi_trans_vsrc": [_vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_cal_objective": [_vp, C.c_longlong, _dp, _vp],
+    "swfwi_parabola_vertex": [C.c_float] * 7 + [_fp, _fp],
+    "swfwi_ricker_wavelet": [_fp, C.c_int, C.c_float, C.c_float, C.c_float],
+    "swfwi_random_codes": [C.c_int, C.c_int, C.c_int, _ip],
+    "swfwi_fwi_create": [C.POINTER(_vp), _vp, _fp, C.c_float, C.c_float, C.c_int, C.c_float, _fp,
+                         _fp, C.c_int],
+    "swfwi_fwi_destroy": [_vp],
+    "swfwi_fwi_epoch": [_vp, C.c_int],
+    "swfwi_fwi_get_update_obj": [_vp, _fp],
+    "swfwi_fwi_get_init_obj": [_vp, _fp],
+    "swfwi_fwi_get_velocity": [_vp, _fp],
+    "swfwi_fwi_write_vel": [_vp, _fp],
+    "swfwi_fwi_last_line_search": [_vp, _fp, _fp],
+    "swfwi_stats_reset": [],
+    "swfwi_stats_enable_step_timing": [C.c_int],
+    "swfwi_stats_read": [C.POINTER(Stats)],
+    "swfwi_status_string": [C.c_int],
+    "swfwi_last_error": [],
+    "swfwi_version": [],
+}
+
+
+def lib() -> C.CDLL:
+    """The loaded C ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: run `python -m swfwi_b200.build` "
+                          "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.swfwi_status_string.restype = C.c_char_p
+        L.swfwi_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_SIGS)
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        msg = lib().swfwi_last_error().decode(errors="replace")
+        raise SwfwiError(status, msg)
+
+
+def _ptr(t) -> C.c_void_p:
+    """Device pointer of a torch CUDA tensor (or an int address)."""
+    if t is None:
+        return C.c_void_p(0)
+    if isinstance(t, int):
+        return C.c_void_p(t)
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor: this library has no CPU path")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream=None) -> C.c_void_p:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _host_f32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(_fp)
+
+
+# ---------------------------------------------------------------- drop-in
+def fd4t10s_damp_zjh_2d_vtrans(prev, curr, vel, nb: int, u2=None, stream=None) -> None:
+    """Damped step in place over ``prev`` ([nx][nz] float32 CUDA tensors),
+    bit-identical to the reference kernel."""
+    nx, nz = prev.shape
+    _check(lib().swfwi_fd4t10s_damp_zjh_2d_vtrans(_ptr(prev), _ptr(curr), _ptr(vel), _ptr(u2), nx, nz,
+                                                  nb, _stream(stream)))
+
+
+def fd4t10s_zjh_2d_vtrans(prev, curr, vel, u2=None, stream=None) -> None:
+    nx, nz = prev.shape
+    _check(lib().swfwi_fd4t10s_zjh_2d_vtrans(_ptr(prev), _ptr(curr), _ptr(vel), _ptr(u2), nx, nz,
+                                             _stream(stream)))
+
+
+def fd4t10s_step_batch(prev, curr, vel, nb: int, damped: bool = True, arith: int = ARITH_REF,
+                       stream=None) -> None:
+    """Batched step over prev/curr of shape [nshots][nx][nz]."""
+    nsh, nx, nz = prev.shape
+    _check(lib().swfwi_fd4t10s_step_batch(_ptr(prev), _ptr(curr), _ptr(vel), nx, nz, nb, int(damped),
+                                          arith, nsh, nx * nz, _stream(stream)))
+
+
+def fd4t10s_step_f64(prev, curr, vel, nb: int, damped: bool = True, stream=None) -> None:
+    nx, nz = prev.shape
+    _check(lib().swfwi_fd4t10s_step_f64(_ptr(prev), _ptr(curr), _ptr(vel), nx, nz, nb, int(damped),
+                                        _stream(stream)))
+
+
+# ---------------------------------------------------------------- stats
+def stats_reset() -> None:
+    _check(lib().swfwi_stats_reset())
+
+
+def stats_enable_step_timing(on: bool = True) -> None:
+    _check(lib().swfwi_stats_enable_step_timing(int(on)))
+
+
+def stats_read() -> dict:
+    st = Stats()
+    _check(lib().swfwi_stats_read(C.byref(st)))
+    return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+# ---------------------------------------------------------------- helpers
+def ricker_wavelet(nt: int, fm: float, dt: float, amp: float = 1.0) -> np.ndarray:
+    w = np.zeros(nt, np.float32)
+    _check(lib().swfwi_ricker_wavelet(w.ctypes.data_as(_fp), nt, fm, dt, amp))
+    return w
+
+
+def random_codes(seed: int, n: int, skip: int = 0) -> np.ndarray:
+    c = np.zeros(n, np.int32)
+    _check(lib().swfwi_random_codes(seed, skip, n, c.ctypes.data_as(_ip)))
+    return c
+
+
+def parabola_vertex(x1, y1, x2, y2, x3, y3, max_alpha3):
+    a, b = C.c_float(), C.c_float()
+    _check(lib().swfwi_parabola_vertex(x1, y1, x2, y2, x3, y3, max_alpha3, C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def update_grad(pre, cur, direction, it: int, stream=None) -> None:
+    _check(lib().swfwi_update_grad(_ptr(pre), _ptr(cur), _ptr(direction), cur.numel(), it,
+                                   _stream(stream)))
+
+
+def cal_max_alpha(vel, grad, dt, dx, maxdv, stream=None):
+    a2, a3 = C.c_float(), C.c_float()
+    _check(lib().swfwi_cal_max_alpha(_ptr(vel), _ptr(grad), vel.numel(), dt, dx, maxdv, C.byref(a2),
+                                     C.byref(a3), _stream(stream)))
+    return a2.value, a3.value
+
+
+def update_vel(new_vel, vel, grad, steplen, vmin, vmax, dx, dt, stream=None) -> None:
+    _check(lib().swfwi_update_vel(_ptr(new_vel), _ptr(vel), _ptr(grad), vel.numel(), steplen, vmin,
+                                  vmax, dx, dt, _stream(stream)))
+
+
+def trans_vsrc(out, inp, stream=None) -> None:
+    nt, ng = inp.shape
+    _check(lib().swfwi_trans_vsrc(_ptr(out), _ptr(inp), nt, ng, _stream(stream)))
+
+
+def cal_objective(r, stream=None) -> float:
+    o = C.c_double()
+    _check(lib().swfwi_cal_objective(_ptr(r), r.numel(), C.byref(o), _stream(stream)))
+    return o.value
+
+
+# ---------------------------------------------------------------- propagator
+class ShotPosition:
+    """A regular line of points (src/common/shot-position.h)."""
+
+    def __init__(self, szbeg: int, sxbeg: int, jsz: int, jsx: int, ns: int, nz: int):
+        self.c = _ShotPos(szbeg, sxbeg, jsz, jsx, ns, nz)
+        self.ns = ns
+
+    def getx(self, i: int) -> int:
+        return self.c.sxbeg + i * self.c.jsx
+
+    def getz(self, i: int) -> int:
+        return self.c.szbeg + i * self.c.jsz
+
+
+class Damp4t10d:
+    """The propagator (src/modeling/damp4t10d.h:18-87) on the GPU.
+
+    Work is ordered on torch's current CUDA stream at construction time
+    (``set_stream`` changes it)."""
+
+    def __init__(self, all_src: ShotPosition, all_geo: ShotPosition, dt: float, dx: float, fm: float,
+                 nb: int, nt: int, arith: int = ARITH_REF, stream=None):
+        h = C.c_void_p()
+        _check(lib().swfwi_damp4t10d_create(C.byref(h), C.byref(all_src.c), C.byref(all_geo.c), dt, dx,
+                                            fm, nb, nt))
+        self.h = h
+        self.src, self.geo = all_src, all_geo
+        self.dt, self.dx, self.fm, self.nb, self.nt = dt, dx, fm, nb, nt
+        self.ns, self.ng = all_src.ns, all_geo.ns
+        self._vel = None
+        self.set_stream(stream)
+        self.set_arith(arith)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().swfwi_damp4t10d_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    @classmethod
+    def from_survey(cls, s, **kw) -> "Damp4t10d":
+        src = ShotPosition(s.szbeg, s.sxbeg, s.jsz, s.jsx, s.ns, s.nz)
+        geo = ShotPosition(s.gzbeg, s.gxbeg, s.jgz, s.jgx, s.ng, s.nz)
+        m = cls(src, geo, s.dt, s.dx, s.fm, s.nb, s.nt, **kw)
+        m.setModelSize(s.nx, s.nz)
+        if s.spreads is not None:
+            m.setReceiversPerShot(*s.spreads)
+        return m
+
+    def set_stream(self, stream=None):
+        self.stream = _stream(stream)
+        _check(lib().swfwi_damp4t10d_set_stream(self.h, self.stream))
+
+    def set_arith(self, arith: int):
+        _check(lib().swfwi_damp4t10d_set_arith(self.h, arith))
+        self.arith = arith
+
+    def setReceiversPerShot(self, offsets, gx, gz):
+        o = np.ascontiguousarray(offsets, np.int32)
+        x = np.ascontiguousarray(gx, np.int32)
+        z = np.ascontiguousarray(gz, np.int32)
+        _check(lib().swfwi_damp4t10d_set_receivers_per_shot(self.h, o.ctypes.data_as(_ip),
+                                                            x.ctypes.data_as(_ip), z.ctypes.data_as(_ip)))
+
+    def setModelSize(self, nx: int, nz: int):
+        _check(lib().swfwi_damp4t10d_set_model_size(self.h, nx, nz))
+
+    def dims(self):
+        v = [C.c_int() for _ in range(5)]
+        _check(lib().swfwi_damp4t10d_dims(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)   # nxpad, nzpad, ns, ngmax, nt
+
+    def getnx(self):
+        return self.dims()[0]
+
+    def getnz(self):
+        return self.dims()[1]
+
+    def getng(self):
+        return self.dims()[3]
+
+    def expandDomain(self, vel: np.ndarray) -> np.ndarray:
+        """Host [nx][nz] m/s -> host [nxpad][nzpad] transformed."""
+        v, vp = _host_f32(vel)
+        nx, nz = v.shape
+        out = np.zeros((nx + 2 * self.nb + 12, nz + self.nb + 12), np.float32)
+        _check(lib().swfwi_damp4t10d_expand_domain(self.h, vp, nx, nz, out.ctypes.data_as(_fp)))
+        return out
+
+    def bindVelocity(self, exvel):
+        self._vel = exvel   # keep it alive: the library holds the pointer
+        _check(lib().swfwi_damp4t10d_bind_velocity(self.h, _ptr(exvel)))
+
+    def stepForward(self, p0, p1):
+        _check(lib().swfwi_damp4t10d_step_forward(self.h, _ptr(p0), _ptr(p1)))
+
+    def stepBackward(self, p0, p1):
+        _check(lib().swfwi_damp4t10d_step_backward(self.h, _ptr(p0), _ptr(p1)))
+
+    def addSource(self, p, source, shot_id: int = -1):
+        _check(lib().swfwi_damp4t10d_add_source(self.h, _ptr(p), _ptr(source), shot_id))
+
+    def subSource(self, p, source, shot_id: int = -1):
+        _check(lib().swfwi_damp4t10d_sub_source(self.h, _ptr(p), _ptr(source), shot_id))
+
+    def addEncodedSource(self, p, encsrc_it):
+        self.addSource(p, encsrc_it, -1)
+
+    def subEncodedSource(self, p, encsrc_it):
+        self.subSource(p, encsrc_it, -1)
+
+    def addReceiverSource(self, p, vsrc_it):
+        _check(lib().swfwi_damp4t10d_add_receiver_source(self.h, _ptr(p), _ptr(vsrc_it)))
+
+    def recordSeis(self, seis_it, p):
+        _check(lib().swfwi_damp4t10d_record_seis(self.h, _ptr(seis_it), _ptr(p)))
+
+    def bndrySize(self) -> int:
+        n = C.c_int()
+        _check(lib().swfwi_damp4t10d_bndry_size(self.h, C.byref(n)))
+        return n.value
+
+    def initBndryVector(self, nt: int):
+        import torch
+        return torch.zeros(nt * self.bndrySize(), dtype=torch.float32, device="cuda")
+
+    def writeBndry(self, bndr, p, it: int):
+        _check(lib().swfwi_damp4t10d_write_bndry(self.h, _ptr(bndr), _ptr(p), it))
+
+    def readBndry(self, bndr, p, it: int):
+        _check(lib().swfwi_damp4t10d_read_bndry(self.h, _ptr(bndr), _ptr(p), it))
+
+    def maskGradient(self, g):
+        _check(lib().swfwi_damp4t10d_mask_gradient(self.h, _ptr(g)))
+
+    def scaleGradient(self, g):
+        _check(lib().swfwi_damp4t10d_scale_gradient(self.h, _ptr(g)))
+
+    def refillBoundary(self, v):
+        _check(lib().swfwi_damp4t10d_refill_boundary(self.h, _ptr(v)))
+
+    def removeDirectArrival(self, data):
+        _check(lib().swfwi_damp4t10d_remove_direct_arrival(self.h, _ptr(data), -1))
+
+    def fwiRemoveDirectArrival(self, data, shot_id: int):
+        _check(lib().swfwi_damp4t10d_remove_direct_arrival(self.h, _ptr(data), shot_id))
+
+    def FwiForwardModeling(self, wlt, dcal, shot_id: int):
+        _check(lib().swfwi_damp4t10d_fwi_forward_modeling(self.h, _ptr(wlt), _ptr(dcal), shot_id))
+
+    def EssForwardModeling(self, encsrc, dcal):
+        _check(lib().swfwi_damp4t10d_ess_forward_modeling(self.h, _ptr(encsrc), _ptr(dcal)))
+
+    # ---- batched ----
+    def forward_batch(self, wlt, dcal, shot_ids):
+        ids = np.ascontiguousarray(shot_ids, np.int32)
+        _check(lib().swfwi_damp4t10d_forward_batch(self.h, _ptr(wlt), _ptr(dcal), ids.ctypes.data_as(_ip),
+                                                   ids.size))
+
+    def gradient_batch(self, wlt, dobs, shot_ids, grad) -> np.ndarray:
+        ids = np.ascontiguousarray(shot_ids, np.int32)
+        obj = np.zeros(ids.size, np.float64)
+        _check(lib().swfwi_damp4t10d_gradient_batch(self.h, _ptr(wlt), _ptr(dobs), ids.ctypes.data_as(_ip),
+                                                    ids.size, _ptr(grad), obj.ctypes.data_as(_dp)))
+        return obj
+
+    def gradient_host(self, exvel: np.ndarray, wlt: np.ndarray, dobs: np.ndarray, shot_ids,
+                      grad_out: np.ndarray | None = None):
+        """The batched gradient from host buffers (copies in and out)."""
+        ids = np.ascontiguousarray(shot_ids, np.int32)
+        v, vp = _host_f32(exvel)
+        w, wp = _host_f32(wlt)
+        d, dp = _host_f32(dobs)
+        g = grad_out if grad_out is not None else np.zeros_like(v)
+        obj = np.zeros(ids.size, np.float64)
+        _check(lib().swfwi_gradient_host(self.h, vp, wp, dp, ids.ctypes.data_as(_ip), ids.size,
+                                         g.ctypes.data_as(_fp), obj.ctypes.data_as(_dp)))
+        return g, obj
+
+    def calgradient_ess(self, encsrc, vsrc, grad):
+        _check(lib().swfwi_damp4t10d_calgradient_ess(self.h, _ptr(encsrc), _ptr(vsrc), _ptr(grad)))
+
+    def calgradient_fwi(self, wlt, vsrc, grad, shot_id: int):
+        _check(lib().swfwi_damp4t10d_calgradient_fwi(self.h, _ptr(wlt), _ptr(vsrc), _ptr(grad), shot_id))
+
+    def calgradient_fwi_f64(self, vel, wlt64, vsrc64, grad64, shot_id: int):
+        _check(lib().swfwi_damp4t10d_calgradient_fwi_f64(self.h, _ptr(vel), _ptr(wlt64), _ptr(vsrc64),
+                                                         _ptr(grad64), shot_id))
+
+    def FwiForwardModeling_f64(self, vel, wlt64, dcal64, shot_id: int):
+        _check(lib().swfwi_damp4t10d_fwi_forward_modeling_f64(self.h, _ptr(vel), _ptr(wlt64), _ptr(dcal64),
+                                                              shot_id))
+
+
+class _Framework:
+    encoded = 0
+
+    def __init__(self, method: Damp4t10d, exvel: np.ndarray, vmin: float, vmax: float, nita: int,
+                 maxdv: float, wlt: np.ndarray, dobs: np.ndarray):
+        v, vp = _host_f32(exvel)
+        w, wp = _host_f32(wlt)
+        d, dp = _host_f32(dobs)
+        h = C.c_void_p()
+        _check(lib().swfwi_fwi_create(C.byref(h), method.h, vp, vmin, vmax, nita, maxdv, wp, dp,
+                                      self.encoded))
+        self.h = h
+        self.method = method
+        self.shape = v.shape
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().swfwi_fwi_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def epoch(self, it: int):
+        _check(lib().swfwi_fwi_epoch(self.h, it))
+
+    def getUpdateObj(self) -> float:
+        o = C.c_float()
+        _check(lib().swfwi_fwi_get_update_obj(self.h, C.byref(o)))
+        return o.value
+
+    def getInitObj(self) -> float:
+        o = C.c_float()
+        _check(lib().swfwi_fwi_get_init_obj(self.h, C.byref(o)))
+        return o.value
+
+    def velocity(self) -> np.ndarray:
+        out = np.zeros(self.shape, np.float32)
+        _check(lib().swfwi_fwi_get_velocity(self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def writeVel(self) -> np.ndarray:
+        nxpad, nzpad = self.shape
+        nb = self.method.nb
+        out = np.zeros((nxpad - 2 * nb - 12, nzpad - nb - 12), np.float32)
+        _check(lib().swfwi_fwi_write_vel(self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def lastLineSearch(self):
+        a = np.zeros(4, np.float32)
+        o = np.zeros(4, np.float32)
+        _check(lib().swfwi_fwi_last_line_search(self.h, a.ctypes.data_as(_fp), o.ctypes.data_as(_fp)))
+        return a, o
+
+
+class FwiFramework(_Framework):
+    """Plain per-shot FWI (src/fwi/fwiframework.h)."""
+    encoded = 0
+
+
+class EssFwiFramework(_Framework):
+    """Encoded simultaneous-source FWI (src/essfwi/essfwiframework.h)."""
+    encoded = 1

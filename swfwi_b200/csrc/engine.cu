@@ -1,0 +1,624 @@
+// Propagator: Damp4t10d on the GPU (src/modeling/damp4t10d.cpp) and the
+// batched shot loops of the FWI frameworks.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <utility>
+#include "engine.hpp"
+
+namespace swfwi {
+
+namespace {
+constexpr int kPartials = 256;   // FP64 partial sums per slot in reductions
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+}  // namespace
+
+// ---- stencil launch timing (CUDA events around each step launch) -------
+StepTimer &step_timer() {
+  static StepTimer t;
+  return t;
+}
+
+void StepTimer::reset() {
+  std::lock_guard<std::mutex> g(mu);
+  used = 0;
+  launches = 0;
+  points = bytes = 0;
+  g_kernel_launches.store(0);
+}
+
+void StepTimer::read(double &ms, long long &n, double &pts, double &b) {
+  std::lock_guard<std::mutex> g(mu);
+  ms = 0;
+  for (size_t i = 0; i < used; i++) {
+    SWFWI_CUDA(cudaEventSynchronize(pool[i].second));
+    float t = 0;
+    SWFWI_CUDA(cudaEventElapsedTime(&t, pool[i].first, pool[i].second));
+    ms += t;
+  }
+  n = launches;
+  pts = points;
+  b = bytes;
+}
+
+// One FD step for n slots; when timing is on, brackets it with events on
+// the launching stream and books its algorithmic work: every interior point
+// of every slot is updated (12 B: read current and previous, write next),
+// and the velocity shared by the slots is read once (4 B a point).
+void timed_step(int arith, bool damped, int tx, const StepArgs &a, int n, cudaStream_t st) {
+  StepTimer &t = step_timer();
+  bool on = t.enabled.load(std::memory_order_relaxed);
+  std::pair<cudaEvent_t, cudaEvent_t> ev{};
+  if (on) {
+    std::lock_guard<std::mutex> g(t.mu);
+    if (t.used == t.pool.size()) {
+      cudaEvent_t x, y;
+      SWFWI_CUDA(cudaEventCreate(&x));
+      SWFWI_CUDA(cudaEventCreate(&y));
+      t.pool.emplace_back(x, y);
+    }
+    ev = t.pool[t.used++];
+    double pts = (double)(a.nx - 12) * (a.nz - 12);
+    size_t el = arith == ARITH_F64 ? 8 : 4;
+    t.launches++;
+    t.points += pts * n;
+    t.bytes += pts * n * 3 * el + pts * el * ((n + a.shots_per_vel - 1) / a.shots_per_vel);
+    SWFWI_CUDA(cudaEventRecord(ev.first, st));
+  }
+  launch_step(arith, damped, true, tx, a, n, st);
+  if (on) SWFWI_CUDA(cudaEventRecord(ev.second, st));
+}
+
+Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, float fm_, int nb_,
+                       int nt_)
+    : nx(0), nz(0), nb(nb_), nt(nt_), ns(src.n), ng(geo.n), ngmax(geo.n), dt(dt_), dx(dx_),
+      fm(fm_), nxpad(0), nzpad(0), fstride(0), bsize(0) {
+  SWFWI_REQUIRE(nb_ >= 0 && nt_ > 0 && src.n > 0 && geo.n > 0, "bad propagator sizes");
+  SWFWI_REQUIRE(dt_ > 0 && dx_ > 0 && fm_ > 0, "dt, dx, fm must be positive");
+  // Damp4t10d::Damp4t10d (damp4t10d.cpp:367-376)
+  bz0 = 6;
+  bx0 = bxn = bzn = nb_ + 6;
+  // fwiRemoveDirectArrival: t_width = 1.5 / fm in double stored as float,
+  // half_len = t_width / dt truncated (damp4t10d.cpp:322, 391).
+  float t_width = (float)(1.5 / (double)fm_);
+  half_len = (int)(t_width / dt_);
+  SWFWI_CUDA(cudaStreamCreateWithFlags(&own_st_, cudaStreamNonBlocking));
+  st_ = own_st_;
+  h_src_x.resize(ns);
+  h_src_z.resize(ns);
+  for (int i = 0; i < ns; i++) {
+    h_src_x[i] = src.x(i);
+    h_src_z[i] = src.z(i);
+  }
+  h_geo_x.resize(ng);
+  h_geo_z.resize(ng);
+  for (int i = 0; i < ng; i++) {
+    h_geo_x[i] = geo.x(i);
+    h_geo_z[i] = geo.z(i);
+  }
+  h_rec_count.assign(ns, ng);
+  h_rec_x.resize((size_t)ns * ng);
+  h_rec_z.resize((size_t)ns * ng);
+  for (int s = 0; s < ns; s++)
+    for (int i = 0; i < ng; i++) {
+      h_rec_x[(size_t)s * ng + i] = h_geo_x[i];
+      h_rec_z[(size_t)s * ng + i] = h_geo_z[i];
+    }
+}
+
+Propagator::~Propagator() {
+  if (own_st_) cudaStreamDestroy(own_st_);
+}
+
+void Propagator::set_stream(cudaStream_t s) { st_ = s ? s : own_st_; }
+
+void Propagator::set_receivers_per_shot(const int *offsets, const int *gx, const int *gz) {
+  SWFWI_REQUIRE(offsets && gx && gz, "null receiver arrays");
+  SWFWI_REQUIRE(offsets[0] == 0, "offsets[0] must be 0");
+  int m = 0;
+  for (int s = 0; s < ns; s++) {
+    int c = offsets[s + 1] - offsets[s];
+    SWFWI_REQUIRE(c > 0, "every shot needs at least one receiver");
+    m = std::max(m, c);
+  }
+  ngmax = m;
+  h_rec_count.resize(ns);
+  h_rec_x.assign((size_t)ns * ngmax, -1);
+  h_rec_z.assign((size_t)ns * ngmax, -1);
+  for (int s = 0; s < ns; s++) {
+    h_rec_count[s] = offsets[s + 1] - offsets[s];
+    for (int i = 0; i < h_rec_count[s]; i++) {
+      h_rec_x[(size_t)s * ngmax + i] = gx[offsets[s] + i];
+      h_rec_z[(size_t)s * ngmax + i] = gz[offsets[s] + i];
+    }
+  }
+  if (nxpad) upload_geometry();
+}
+
+// expandDomain (damp4t10d.cpp:138-151): edge replication by nb
+// (expandBndry :96-124, free surface on top), transform
+// v -> dx^2/(v^2 dt^2) (transvel :126-130), then a 6-cell halo all round
+// (expandForStencil/fillForStencil :47-94).  Host float arithmetic in the
+// reference's order.
+void Propagator::expand_domain(const float *v, float *out) const {
+  SWFWI_REQUIRE(nx > 0 && nz > 0, "model size unknown");
+  int nxb = nx + 2 * nb, nzb = nz + nb;
+  std::vector<float> b((size_t)nxb * nzb);
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) b[(size_t)(nb + ix) * nzb + iz] = v[(size_t)ix * nz + iz];
+  for (int ix = 0; ix < nb; ix++)
+    for (int iz = 0; iz < nz; iz++) {
+      b[(size_t)ix * nzb + iz] = v[iz];
+      b[(size_t)(nb + nx + ix) * nzb + iz] = v[(size_t)(nx - 1) * nz + iz];
+    }
+  for (int ix = 0; ix < nxb; ix++)
+    for (int iz = 0; iz < nb; iz++) b[(size_t)ix * nzb + nz + iz] = b[(size_t)ix * nzb + nz - 1];
+  for (float &x : b) x = (dx * dx) / (x * x * dt * dt);
+  const int h = 6;
+  int nzp = nzb + 2 * h, nxp = nxb + 2 * h;
+  for (int ix = h; ix < nxb + h; ix++)
+    for (int iz = h; iz < nzb + h; iz++)
+      out[(size_t)ix * nzp + iz] = b[(size_t)(ix - h) * nzb + (iz - h)];
+  for (int ix = h; ix < nxb + h; ix++) {
+    for (int iz = 0; iz < h; iz++) out[(size_t)ix * nzp + iz] = out[(size_t)ix * nzp + h];
+    for (int iz = nzb + h; iz < nzp; iz++) out[(size_t)ix * nzp + iz] = out[(size_t)ix * nzp + nzb + h - 1];
+  }
+  for (int iz = 0; iz < nzp; iz++) {
+    for (int ix = 0; ix < h; ix++) out[(size_t)ix * nzp + iz] = out[(size_t)h * nzp + iz];
+    for (int ix = nxb + h; ix < nxp; ix++) out[(size_t)ix * nzp + iz] = out[(size_t)(nxb + h - 1) * nzp + iz];
+  }
+}
+
+void Propagator::upload_geometry() {
+  std::vector<int> sp(ns), sx(ns), sz(ns), gp(ng), gxp(ng), gzp(ng);
+  for (int i = 0; i < ns; i++) {
+    sx[i] = h_src_x[i] + bx0;
+    sz[i] = h_src_z[i] + bz0;
+    SWFWI_REQUIRE(sx[i] >= 6 && sx[i] < nxpad - 6 && sz[i] >= 6 && sz[i] < nzpad - 6,
+                  "source outside the computing zone");
+    sp[i] = sx[i] * nzpad + sz[i];
+  }
+  for (int i = 0; i < ng; i++) {
+    gxp[i] = h_geo_x[i] + bx0;
+    gzp[i] = h_geo_z[i] + bz0;
+    SWFWI_REQUIRE(gxp[i] >= 6 && gxp[i] < nxpad - 6 && gzp[i] >= 6 && gzp[i] < nzpad - 6,
+                  "receiver outside the computing zone");
+    gp[i] = gxp[i] * nzpad + gzp[i];
+  }
+  std::vector<int> rp((size_t)ns * ngmax, -1), rx((size_t)ns * ngmax, -1), rz((size_t)ns * ngmax, -1);
+  for (int s = 0; s < ns; s++)
+    for (int i = 0; i < ngmax; i++) {
+      size_t k = (size_t)s * ngmax + i;
+      if (h_rec_x[k] < 0) continue;
+      rx[k] = h_rec_x[k] + bx0;
+      rz[k] = h_rec_z[k] + bz0;
+      SWFWI_REQUIRE(rx[k] >= 6 && rx[k] < nxpad - 6 && rz[k] >= 6 && rz[k] < nzpad - 6,
+                    "receiver outside the computing zone");
+      rp[k] = rx[k] * nzpad + rz[k];
+    }
+  // Positions within one injection set must be distinct (the reference adds
+  // sequentially; the device adds in parallel).
+  {
+    std::vector<int> t = sp;
+    std::sort(t.begin(), t.end());
+    SWFWI_REQUIRE(std::adjacent_find(t.begin(), t.end()) == t.end(), "duplicate source positions");
+    for (int s = 0; s < ns; s++) {
+      std::vector<int> r(rp.begin() + (size_t)s * ngmax, rp.begin() + (size_t)(s + 1) * ngmax);
+      r.erase(std::remove(r.begin(), r.end(), -1), r.end());
+      std::sort(r.begin(), r.end());
+      SWFWI_REQUIRE(std::adjacent_find(r.begin(), r.end()) == r.end(), "duplicate receiver positions");
+    }
+  }
+  d_src_pos_.upload(sp, st_);
+  d_src_x_.upload(sx, st_);
+  d_src_z_.upload(sz, st_);
+  d_geo_pos_.upload(gp, st_);
+  d_geo_x_.upload(gxp, st_);
+  d_geo_z_.upload(gzp, st_);
+  d_rec_pos_.upload(rp, st_);
+  d_rec_x_.upload(rx, st_);
+  d_rec_z_.upload(rz, st_);
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Propagator::bind_velocity(const float *exvel) {
+  SWFWI_REQUIRE(exvel != nullptr, "null velocity");
+  SWFWI_REQUIRE(nxpad > 12 && nzpad > 12, "padded size unknown");
+  vel_ = exvel;
+  rcp_for_ = nullptr;   // contents may have changed: recompute 1/vt lazily
+}
+
+const float *Propagator::rcp_of(const float *vel) {
+  SWFWI_REQUIRE(vel != nullptr, "no velocity bound");
+  long long n = (long long)nxpad * nzpad;
+  if (vel == vel_) {
+    if (rcp_for_ != vel_) {
+      rcp_.resize(n);
+      launch_reciprocal(rcp_.get(), vel_, n, st_);
+      rcp_for_ = vel_;
+    }
+    return rcp_.get();
+  }
+  trial_rcp_.resize(n);
+  launch_reciprocal(trial_rcp_.get(), vel, n, st_);
+  return trial_rcp_.get();
+}
+
+StepArgs Propagator::step_args(void *prev, const void *curr, const void *velrcp, int n) const {
+  StepArgs a;
+  a.prev = prev;
+  a.curr = curr;
+  a.vel = velrcp;
+  a.nx = nxpad;
+  a.nz = nzpad;
+  a.bx0 = bx0;
+  a.shot_stride = fstride;
+  a.vel_stride = 0;
+  a.shots_per_vel = std::max(n, 1);
+  return a;
+}
+
+// ---- single-field operations ------------------------------------------
+void Propagator::step_forward(float *p0, float *p1) {
+  SWFWI_REQUIRE(p0 && p1, "null field");
+  timed_step(arith, true, tile_tx, step_args(p0, p1, rcp_of(vel_), 1), 1, st_);
+}
+
+void Propagator::step_backward(float *p0, float *p1) {
+  SWFWI_REQUIRE(p0 && p1, "null field");
+  timed_step(arith, false, tile_tx, step_args(p0, p1, rcp_of(vel_), 1), 1, st_);
+}
+
+void Propagator::manip_source(float *p, const float *src, int shot_id, int sign) {
+  SWFWI_REQUIRE(p && src, "null pointer");
+  SWFWI_REQUIRE(shot_id >= -1 && shot_id < ns, "shot id out of range");
+  PointSet ps;
+  if (shot_id >= 0) {
+    ps = {d_src_pos_.get() + shot_id, 1, nullptr};
+  } else {
+    ps = {d_src_pos_.get(), ns, nullptr};
+  }
+  launch_inject<float>(p, 0, 1, ps, src, 0, 1, sign, st_);
+}
+
+void Propagator::add_receiver_source(float *p, const float *vsrc_it) {
+  SWFWI_REQUIRE(p && vsrc_it, "null pointer");
+  launch_inject<float>(p, 0, 1, PointSet{d_geo_pos_.get(), ng, nullptr}, vsrc_it, 0, 1, +1, st_);
+}
+
+void Propagator::record_seis(float *seis, const float *p) {
+  SWFWI_REQUIRE(seis && p, "null pointer");
+  launch_record<float>(seis, 0, p, 0, 1, PointSet{d_geo_pos_.get(), ng, nullptr}, st_);
+}
+
+void Propagator::write_bndry(float *bndr, const float *p, int it) {
+  SWFWI_REQUIRE(bndr && p && it >= 0, "bad strip arguments");
+  launch_strip_write<float>(bndr + (long long)it * bsize, 0, p, 0, 1, nxpad, nzpad, bx0, st_);
+}
+
+void Propagator::read_bndry(const float *bndr, float *p, int it) {
+  SWFWI_REQUIRE(bndr && p && it >= 0, "bad strip arguments");
+  launch_strip_read<float>(bndr + (long long)it * bsize, 0, p, 0, 1, nxpad, nzpad, bx0, st_);
+}
+
+namespace {
+__global__ void k_mask(float *g, int nxpad, int nzpad, int bx0, int bz0, int bxn, int bzn) {
+  int n = nxpad * nzpad;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    int ix = q / nzpad, iz = q - ix * nzpad;
+    if (ix < bx0 || iz < bz0 || ix >= nxpad - bxn || iz >= nzpad - bzn) g[q] = 0.f;
+  }
+}
+__global__ void k_scale(float *g, int nxpad, int nzpad, int bx0, int bz0, int bxn, int bzn) {
+  int nzi = nzpad - bz0 - bzn;
+  int nxi = nxpad - bx0 - bxn;
+  int n = nxi * nzi;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    int ix = q / nzi, iz = q - ix * nzi;
+    if (iz < 1) continue;
+    float *p = g + (long long)(ix + bx0) * nzpad + iz + bz0;
+    *p = __fmul_rn(*p, __fsqrt_rn((float)iz));
+  }
+}
+}  // namespace
+
+void Propagator::mask_gradient(float *g) {
+  SWFWI_REQUIRE(g, "null gradient");
+  k_mask<<<592, 256, 0, st_>>>(g, nxpad, nzpad, bx0, bz0, bxn, bzn);
+  g_kernel_launches++;
+}
+
+void Propagator::scale_gradient(float *g) {
+  SWFWI_REQUIRE(g, "null gradient");
+  k_scale<<<592, 256, 0, st_>>>(g, nxpad, nzpad, bx0, bz0, bxn, bzn);
+  g_kernel_launches++;
+}
+
+void Propagator::refill_boundary(float *v) {
+  SWFWI_REQUIRE(v, "null array");
+  launch_refill_boundary(v, nxpad, nzpad, bz0, bzn, bx0, bxn, st_);
+}
+
+void Propagator::remove_direct_arrival(float *data, int shot_id, const float *vel) {
+  SWFWI_REQUIRE(data, "null data");
+  SWFWI_REQUIRE(shot_id >= -1 && shot_id < ns, "shot id out of range");
+  const float *v = vel ? vel : vel_;
+  SWFWI_REQUIRE(v, "no velocity bound");
+  int s = shot_id < 0 ? 0 : shot_id;   // removeDirectArrival uses source 0
+  d_win1_.resize((size_t)2 * ng);
+  launch_mute_windows(d_win1_.get(), v, nxpad, nzpad, d_src_x_.get() + s, d_src_z_.get() + s,
+                      d_geo_x_.get(), d_geo_z_.get(), 0, ng, nullptr, half_len, nt, 1, st_);
+  launch_apply_mute(data, 0, d_win1_.get(), nt, ng, 1, st_);
+}
+
+template <typename T>
+void Propagator::ensure_work(Work<T> &w, int n, bool strips, int ngrec) {
+  size_t f = (size_t)n * fstride;
+  w.p0.resize(f);
+  w.p1.resize(f);
+  if (strips) w.strips.resize((size_t)n * nt * bsize);
+  w.partials.resize((size_t)n * kPartials);
+  w.obj.resize(n);
+  (void)ngrec;
+}
+
+template <typename T>
+void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
+                             long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
+                             bool save_strips, const void *velrcp) {
+  ensure_work(w, n, save_strips, ngrec);
+  T *p0 = w.p0.get(), *p1 = w.p1.get();
+  w.p0.zero(st_);
+  w.p1.zero(st_);
+  int ar = sizeof(T) == 8 ? ARITH_F64 : arith;
+  long long bstride = (long long)nt * bsize;
+  for (int it = 0; it < nt; it++) {
+    // addSource -> stepForward -> swap -> recordSeis / writeBndry
+    // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
+    launch_inject<T>(p1, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
+                     +1, st_);
+    timed_step(ar, true, tile_tx, step_args(p0, p1, velrcp, n), n, st_);
+    std::swap(p0, p1);
+    if (dcal)
+      launch_record<T>(dcal + (long long)it * ngrec, (long long)nt * ngrec, p0, fstride, n, rec, st_);
+    if (save_strips)
+      launch_strip_write<T>(w.strips.get() + (long long)it * bsize, bstride, p0, fstride, n, nxpad,
+                            nzpad, bx0, st_);
+  }
+  // leave the final (current, next) pair for a backward sweep
+  if (p0 != w.p0.get()) std::swap(w.p0, w.p1);
+}
+
+template <typename T>
+void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
+                              long long slot_stride, int i_stride, PointSet rec, int ngrec,
+                              const T *vsrc, const void *velrcp) {
+  size_t f = (size_t)n * fstride;
+  w.g0.resize(f);
+  w.g1.resize(f);
+  w.g0.zero(st_);
+  w.g1.zero(st_);
+  T *sp0 = w.p0.get(), *sp1 = w.p1.get(), *gp0 = w.g0.get(), *gp1 = w.g1.get();
+  int ar = sizeof(T) == 8 ? ARITH_F64 : arith;
+  long long bstride = (long long)nt * bsize;
+  int npts = nxpad * nzpad;
+  for (int it = nt - 1; it >= 0; it--) {
+    // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
+    // subSource; receiver addSource -> stepForward -> swap; image.
+    launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad,
+                         nzpad, bx0, st_);
+    std::swap(sp0, sp1);
+    timed_step(ar, false, tile_tx, step_args(sp0, sp1, velrcp, n), n, st_);
+    launch_inject<T>(sp0, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
+                     -1, st_);
+    launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1,
+                     +1, st_);
+    timed_step(ar, true, tile_tx, step_args(gp0, gp1, velrcp, n), n, st_);
+    std::swap(gp0, gp1);
+    float t = dt * (float)it;
+    float scale;
+    if ((double)t > 0.4) scale = 1.0f;
+    else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
+    else break;
+    launch_image<T>(w.image.get(), fstride, sp0, gp0, fstride, n, npts, scale, st_);
+  }
+}
+
+void Propagator::fwi_forward(const float *wlt, float *dcal, int shot_id) {
+  SWFWI_REQUIRE(wlt && dcal, "null pointer");
+  SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
+  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, rcp_of(vel_));
+}
+
+void Propagator::ess_forward(const float *encsrc, float *dcal, const float *vel) {
+  SWFWI_REQUIRE(encsrc && dcal, "null pointer");
+  PointSet src{d_src_pos_.get(), ns, nullptr};
+  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false,
+                     rcp_of(vel ? vel : vel_));
+}
+
+int Propagator::max_batch() const {
+  size_t freeb = 0, total = 0;
+  if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) return 1;
+  // per slot: p0,p1,g0,g1,image fields; strips; dcal,res,vsrc data
+  double per = 5.0 * fstride * 4 + (double)nt * bsize * 4 + 3.0 * nt * ngmax * 4 + 4096;
+  double budget = 0.85 * (double)freeb;
+  // memory already held by this propagator's work space counts as free
+  budget += (double)(w_.p0.size() + w_.p1.size() + w_.g0.size() + w_.g1.size() + w_.image.size() +
+                     w_.strips.size() + w_.dcal.size() + w_.res.size() + w_.vsrc.size()) * 4;
+  int m = (int)(budget / per);
+  return std::max(1, std::min(m, ns));
+}
+
+void Propagator::forward_batch(const float *wlt, float *dcal, const int *ids, int n,
+                               const float *vel) {
+  SWFWI_REQUIRE(wlt && dcal && ids && n > 0, "bad batch arguments");
+  for (int i = 0; i < n; i++) SWFWI_REQUIRE(ids[i] >= 0 && ids[i] < ns, "shot id out of range");
+  const float *rcp = rcp_of(vel ? vel : vel_);
+  int mb = max_batch();
+  for (int c0 = 0; c0 < n; c0 += mb) {
+    int k = std::min(mb, n - c0);
+    w_.slot_shot.upload(ids + c0, k, st_);
+    PointSet src{d_src_pos_.get(), 1, w_.slot_shot.get()};
+    PointSet rec{d_rec_pos_.get(), ngmax, w_.slot_shot.get()};
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, dcal + (long long)c0 * nt * ngmax,
+                       false, rcp);
+  }
+}
+
+void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *ids, int n,
+                                float *grad, double *obj, bool accumulate, const int *rows) {
+  SWFWI_REQUIRE(wlt && dobs && ids && grad && n > 0, "bad batch arguments");
+  for (int i = 0; i < n; i++) SWFWI_REQUIRE(ids[i] >= 0 && ids[i] < ns, "shot id out of range");
+  const float *rcp = rcp_of(vel_);
+  int mb = max_batch();
+  long long dn = (long long)nt * ngmax;
+  for (int c0 = 0; c0 < n; c0 += mb) {
+    int k = std::min(mb, n - c0);
+    w_.slot_shot.upload(ids + c0, k, st_);
+    const int *ss = w_.slot_shot.get();
+    const int *rr = ss;
+    if (rows) {
+      w_.slot_row.upload(rows + c0, k, st_);
+      rr = w_.slot_row.get();
+    }
+    PointSet src{d_src_pos_.get(), 1, ss};
+    PointSet rec{d_rec_pos_.get(), ngmax, ss};
+    w_.dcal.resize((size_t)k * dn);
+    w_.res.resize((size_t)k * dn);
+    w_.vsrc.resize((size_t)k * dn);
+    w_.win.resize((size_t)k * ngmax * 2);
+    w_.image.resize((size_t)k * fstride);
+    w_.image.zero(st_);
+    // FwiForwardModeling and calgradient's forward sweep model the same
+    // field from the same source: one sweep records dcal and saves strips.
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), true, rcp);
+    launch_mute_windows(w_.win.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
+                        d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
+    launch_muted_residual(w_.res.get(), dobs, dn, rr, w_.dcal.get(), w_.win.get(), w_.win.get(), nt,
+                          ngmax, k, st_);
+    launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);
+    launch_trans_vsrc(w_.vsrc.get(), w_.res.get(), nt, ngmax, k, st_);
+    run_backward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.vsrc.get(), rcp);
+    launch_finalize_gradient(grad, w_.image.get(), fstride, k, nxpad, nzpad, bx0,
+                             (accumulate || c0 > 0) ? 1 : 0, st_);
+    if (obj) {
+      SWFWI_CUDA(cudaMemcpyAsync(obj + c0, w_.obj.get(), sizeof(double) * k, cudaMemcpyDeviceToHost,
+                                 st_));
+    }
+  }
+  if (obj) SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+double Propagator::trial_objective_fwi(const float *wlt, const float *dobs, const int *ids, int n,
+                                       const float *trial_vel) {
+  SWFWI_REQUIRE(wlt && dobs && ids && trial_vel && n > 0, "bad trial arguments");
+  const float *rcp = rcp_of(trial_vel);
+  int mb = max_batch();
+  long long dn = (long long)nt * ngmax;
+  std::vector<double> h;
+  double total = 0.0;
+  DevBuf<int> win_obs;
+  for (int c0 = 0; c0 < n; c0 += mb) {
+    int k = std::min(mb, n - c0);
+    w_.slot_shot.upload(ids + c0, k, st_);
+    const int *ss = w_.slot_shot.get();
+    PointSet src{d_src_pos_.get(), 1, ss};
+    PointSet rec{d_rec_pos_.get(), ngmax, ss};
+    w_.dcal.resize((size_t)k * dn);
+    w_.res.resize((size_t)k * dn);
+    w_.win.resize((size_t)k * ngmax * 2);
+    win_obs.resize((size_t)k * ngmax * 2);
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), false, rcp);
+    // modelled data muted with the trial velocity, observed data with the
+    // current one (updatesteplenop.cpp:77 and essfwiframework.cpp:205)
+    launch_mute_windows(w_.win.get(), trial_vel, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
+                        d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
+    launch_mute_windows(win_obs.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
+                        d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
+    launch_muted_residual(w_.res.get(), dobs, dn, ss, w_.dcal.get(), win_obs.get(), w_.win.get(),
+                          nt, ngmax, k, st_);
+    launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);
+    h.resize(k);
+    SWFWI_CUDA(cudaMemcpyAsync(h.data(), w_.obj.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, st_));
+    SWFWI_CUDA(cudaStreamSynchronize(st_));
+    for (int i = 0; i < k; i++) total += h[i];
+  }
+  return total;
+}
+
+void Propagator::calgradient_ess(const float *encsrc, const float *vsrc, float *grad) {
+  SWFWI_REQUIRE(encsrc && vsrc && grad, "null pointer");
+  const float *rcp = rcp_of(vel_);
+  PointSet src{d_src_pos_.get(), ns, nullptr};
+  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  w_.image.resize((size_t)fstride);
+  SWFWI_CUDA(cudaMemcpyAsync(w_.image.get(), grad, sizeof(float) * nxpad * nzpad,
+                             cudaMemcpyDeviceToDevice, st_));
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp);
+  run_backward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, rcp);
+  SWFWI_CUDA(cudaMemcpyAsync(grad, w_.image.get(), sizeof(float) * nxpad * nzpad,
+                             cudaMemcpyDeviceToDevice, st_));
+}
+
+void Propagator::calgradient_fwi(const float *wlt, const float *vsrc, float *grad, int shot_id) {
+  SWFWI_REQUIRE(wlt && vsrc && grad, "null pointer");
+  SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
+  const float *rcp = rcp_of(vel_);
+  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  w_.image.resize((size_t)fstride);
+  SWFWI_CUDA(cudaMemcpyAsync(w_.image.get(), grad, sizeof(float) * nxpad * nzpad,
+                             cudaMemcpyDeviceToDevice, st_));
+  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp);
+  run_backward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, rcp);
+  SWFWI_CUDA(cudaMemcpyAsync(grad, w_.image.get(), sizeof(float) * nxpad * nzpad,
+                             cudaMemcpyDeviceToDevice, st_));
+}
+
+void Propagator::calgradient_fwi_f64(const float *vel, const double *wlt, const double *vsrc,
+                                     double *grad, int shot_id) {
+  SWFWI_REQUIRE(vel && wlt && vsrc && grad, "null pointer");
+  SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
+  long long np = (long long)nxpad * nzpad;
+  DevBuf<double> r64(np);
+  launch_to_f64_reciprocal(r64.get(), vel, np, st_);
+  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  wd_.image.resize((size_t)fstride);
+  SWFWI_CUDA(cudaMemcpyAsync(wd_.image.get(), grad, sizeof(double) * np, cudaMemcpyDeviceToDevice, st_));
+  run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, r64.get());
+  run_backward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, r64.get());
+  SWFWI_CUDA(cudaMemcpyAsync(grad, wd_.image.get(), sizeof(double) * np, cudaMemcpyDeviceToDevice, st_));
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Propagator::fwi_forward_f64(const float *vel, const double *wlt, double *dcal, int shot_id) {
+  SWFWI_REQUIRE(vel && wlt && dcal, "null pointer");
+  SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
+  long long np = (long long)nxpad * nzpad;
+  DevBuf<double> r64(np);
+  launch_to_f64_reciprocal(r64.get(), vel, np, st_);
+  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, r64.get());
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+// Called once the padded size is known (from expandDomain or a bind).
+void Propagator::set_dims(int nxpad_, int nzpad_) {
+  SWFWI_REQUIRE(nxpad_ > 2 * bx0 && nzpad_ > bz0 + bzn, "grid smaller than its padding");
+  if (nxpad == nxpad_ && nzpad == nzpad_) return;
+  nxpad = nxpad_;
+  nzpad = nzpad_;
+  nx = nxpad - 2 * nb - 12;
+  nz = nzpad - nb - 12;
+  fstride = round_up((long long)nxpad * nzpad, 64);
+  bsize = strip_size(nxpad, nzpad, bx0);
+  upload_geometry();
+}
+
+}  // namespace swfwi

@@ -1,0 +1,72 @@
+// FWI drivers over the propagator: the plain per-shot framework
+// (src/fwi/fwiframework.cpp), the encoded-source framework
+// (src/essfwi/essfwiframework.cpp) and their step-length search
+// (src/essfwi/updatesteplenop.cpp) and velocity update
+// (src/essfwi/updatevelop.cpp).
+#pragma once
+#include <cstdint>
+#include <functional>
+#include <vector>
+#include "engine.hpp"
+
+namespace swfwi {
+
+// RandomCodes (src/common/random-code.cpp:2-22): Boost.Random minstd_rand
+// (x <- 48271 x mod 2^31-1, seed 0 -> 1) mapped to {0,1} by Boost's
+// uniform_int bucketing (bucket = (brange+1)/2 over the engine range
+// [1, 2^31-2]), then to -1/+1.
+class RandomCodes {
+ public:
+  explicit RandomCodes(int seed);
+  std::vector<int> gen_plus1_minus1(int n);
+
+ private:
+  uint64_t x_;
+  int draw();
+};
+
+// parabolaVertex (src/common/parabola-vertex.cpp:12-33).
+void parabola_vertex(float x1, float y1, float x2, float y2, float x3, float y3, float max_alpha3,
+                     float &xv, float &yv);
+
+// The step-length search of UpdateSteplenOp (updatesteplenop.cpp:25-285)
+// over an objective function of the step.
+struct StepSearch {
+  int nita = 0;
+  float maxdv = 0;
+  bool preserved_init = false;
+  float preserved_alpha = 0;
+  // last search, for inspection
+  float alpha[4] = {0, 0, 0, 0}, obj[4] = {0, 0, 0, 0};
+  // calsteplen: returns the step; objval receives its objective
+  float calsteplen(const std::function<float(float)> &f, float obj_val1, float max_alpha3,
+                   float &objval);
+};
+
+class FwiRunner {
+ public:
+  FwiRunner(Propagator &p, const float *exvel_host, float vmin, float vmax, int nita, float maxdv,
+            const float *wlt_host, const float *dobs_host, bool encoded);
+  void epoch(int iter);
+  float update_obj = 0, init_obj = 0;
+  void get_velocity(float *host);
+  void write_vel(float *host);   // sfWriteVel without the file
+  StepSearch search;
+
+ private:
+  Propagator &p_;
+  bool encoded_;
+  float vmin_t_, vmax_t_;   // UpdateVelOp bounds in transformed units
+  int n_;                   // nxpad*nzpad
+  DevBuf<float> vel_, trial_, g_, g0_, dir_, wlt_, dobs_, encsrc_, encobs_, dcal_, vsrc_, res_;
+  DevBuf<int> codes_;
+  DevBuf<double> scratch_;
+  RandomCodes codes_gen_;
+  std::vector<int> ids_;
+  void update_grad(int iter);
+  void plain_epoch(int iter);
+  void ess_epoch(int iter);
+  double sumsq(const float *x, long long n);
+};
+
+}  // namespace swfwi

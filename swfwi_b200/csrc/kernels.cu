@@ -1,0 +1,677 @@
+// Kernels around the stencil; see kernels.cuh for the reference citations.
+#include <atomic>
+#include <cmath>
+#include "kernels.cuh"
+
+namespace swfwi {
+
+std::atomic<long long> g_kernel_launches{0};
+
+namespace {
+constexpr int kThreads = 256;
+inline void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+inline unsigned grid_for(long long n, int threads = kThreads) {
+  long long g = (n + threads - 1) / threads;
+  return (unsigned)(g < 1 ? 1 : (g > 2147483647LL ? 2147483647LL : g));
+}
+
+// Exact float add/sub regardless of the caller's arithmetic mode: the
+// reference's manipSource is one float operation per point.
+template <typename T>
+__device__ __forceinline__ T exact_add(T a, T b) { return a + b; }
+template <>
+__device__ __forceinline__ float exact_add<float>(float a, float b) { return __fadd_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T exact_sub(T a, T b) { return a - b; }
+template <>
+__device__ __forceinline__ float exact_sub<float>(float a, float b) { return __fsub_rn(a, b); }
+
+// Deterministic FP64 block reduction with warp shuffles.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? ws[threadIdx.x] : 0.0;
+  if (w == 0)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  return v;
+}
+}  // namespace
+
+// ---------------------------------------------------------------- inject
+template <typename T>
+__global__ void k_inject(T *field, long long shot_stride, int nslots, PointSet ps, const T *vals,
+                         long long val_slot_stride, int val_stride, int sign) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = blockIdx.y;
+  if (i >= ps.per_shot || slot >= nslots) return;
+  int shot = ps.slot_shot ? ps.slot_shot[slot] : slot;
+  int p = ps.pos[(long long)shot * ps.per_shot + i];
+  if (p < 0) return;
+  T v = vals[(long long)slot * val_slot_stride + (long long)i * val_stride];
+  T *f = field + (long long)slot * shot_stride + p;
+  *f = sign > 0 ? exact_add<T>(*f, v) : exact_sub<T>(*f, v);
+}
+
+template <typename T>
+void launch_inject(T *field, long long shot_stride, int nslots, PointSet ps, const T *vals,
+                   long long val_slot_stride, int val_stride, int sign, cudaStream_t st) {
+  if (nslots <= 0 || ps.per_shot <= 0) return;
+  dim3 g(grid_for(ps.per_shot, 128), nslots);
+  k_inject<T><<<g, 128, 0, st>>>(field, shot_stride, nslots, ps, vals, val_slot_stride, val_stride,
+                                 sign);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- record
+template <typename T>
+__global__ void k_record(T *seis, long long seis_slot_stride, const T *field, long long shot_stride,
+                         int nslots, PointSet ps) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = blockIdx.y;
+  if (i >= ps.per_shot || slot >= nslots) return;
+  int shot = ps.slot_shot ? ps.slot_shot[slot] : slot;
+  int p = ps.pos[(long long)shot * ps.per_shot + i];
+  seis[(long long)slot * seis_slot_stride + i] = p < 0 ? T(0) : field[(long long)slot * shot_stride + p];
+}
+
+template <typename T>
+void launch_record(T *seis, long long seis_slot_stride, const T *field, long long shot_stride,
+                   int nslots, PointSet ps, cudaStream_t st) {
+  if (nslots <= 0 || ps.per_shot <= 0) return;
+  dim3 g(grid_for(ps.per_shot, 128), nslots);
+  k_record<T><<<g, 128, 0, st>>>(seis, seis_slot_stride, field, shot_stride, nslots, ps);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- strips
+int strip_size(int nx, int nz, int bx0) {
+  return 6 * ((nx - 2 * (bx0 - 6)) + 2 * (nz - 6 - bx0));
+}
+
+// Strip element i -> padded field index.  Bottom: 6 rows below the
+// interior, x from bx0-6 to nx-bx0+6, stored [ix][iz]; then the left and
+// right 6-column bands over the interior depth, stored [ix][iz].
+__device__ __forceinline__ long long strip_index(int i, int nx, int nz, int bx0) {
+  const int w = 6, nxs = nx - 2 * (bx0 - w), nzs = nz - 6 - bx0;
+  if (i < w * nxs) {
+    int ix = i / w, iz = i - ix * w;
+    return (long long)(ix + bx0 - w) * nz + (nz - bx0 + iz);
+  }
+  int j = i - w * nxs;
+  int ix = j / nzs, iz = j - ix * nzs;
+  int gx = ix < w ? (bx0 - w + ix) : (nx - bx0 + ix - w);
+  return (long long)gx * nz + (6 + iz);
+}
+
+template <typename T, bool WRITE>
+__global__ void k_strip(T *bndr, long long bndr_slot_stride, T *field, long long shot_stride, int bs,
+                        int nx, int nz, int bx0) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = blockIdx.y;
+  if (i >= bs) return;
+  long long p = strip_index(i, nx, nz, bx0);
+  T *f = field + (long long)slot * shot_stride + p;
+  T *b = bndr + (long long)slot * bndr_slot_stride + i;
+  if (WRITE) *b = *f; else *f = *b;
+}
+
+template <typename T>
+void launch_strip_write(T *bndr, long long bndr_slot_stride, const T *field, long long shot_stride,
+                        int nslots, int nx, int nz, int bx0, cudaStream_t st) {
+  int bs = strip_size(nx, nz, bx0);
+  dim3 g(grid_for(bs), nslots);
+  k_strip<T, true><<<g, kThreads, 0, st>>>(bndr, bndr_slot_stride, const_cast<T *>(field), shot_stride,
+                                            bs, nx, nz, bx0);
+  note_launch();
+}
+
+template <typename T>
+void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long long shot_stride,
+                       int nslots, int nx, int nz, int bx0, cudaStream_t st) {
+  int bs = strip_size(nx, nz, bx0);
+  dim3 g(grid_for(bs), nslots);
+  k_strip<T, false><<<g, kThreads, 0, st>>>(const_cast<T *>(bndr), bndr_slot_stride, field,
+                                             shot_stride, bs, nx, nz, bx0);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- image
+template <typename T>
+__global__ void k_image(T *image, long long image_stride, const T *s, const T *r,
+                        long long shot_stride, int n, float scale) {
+  int slot = blockIdx.y;
+  T *g = image + (long long)slot * image_stride;
+  const T *a = s + (long long)slot * shot_stride;
+  const T *b = r + (long long)slot * shot_stride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if constexpr (sizeof(T) == 4) {
+      g[i] = __fsub_rn(g[i], __fmul_rn(__fmul_rn(a[i], b[i]), scale));
+    } else {
+      g[i] = g[i] - a[i] * b[i] * (double)scale;
+    }
+  }
+}
+
+template <typename T>
+void launch_image(T *image, long long image_stride, const T *s, const T *r, long long shot_stride,
+                  int nslots, int n, float scale, cudaStream_t st) {
+  unsigned gx = grid_for(n);
+  if (gx > 1184) gx = 1184;
+  dim3 g(gx, nslots);
+  k_image<T><<<g, kThreads, 0, st>>>(image, image_stride, s, r, shot_stride, n, scale);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- step
+template <int ARITH, bool DAMPED, bool RCP, int TX>
+static void step_t(const StepArgs &a, int nslots, cudaStream_t st) {
+  dim3 g((a.nz - 12 + kTZ - 1) / kTZ, (a.nx - 12 + TX - 1) / TX, nslots);
+  fd_step_tile<ARITH, DAMPED, RCP, TX><<<g, kStepThreads, 0, st>>>(a);
+  note_launch();
+}
+
+template <int ARITH, bool DAMPED, bool RCP>
+static void step_tx(int tx, const StepArgs &a, int nslots, cudaStream_t st) {
+  if (tx >= 64) step_t<ARITH, DAMPED, RCP, 64>(a, nslots, st);
+  else step_t<ARITH, DAMPED, RCP, 32>(a, nslots, st);
+}
+
+template <int ARITH>
+static void step_a(bool damped, bool rcp, int tx, const StepArgs &a, int nslots, cudaStream_t st) {
+  if (damped) {
+    if (rcp) step_tx<ARITH, true, true>(tx, a, nslots, st);
+    else step_tx<ARITH, true, false>(tx, a, nslots, st);
+  } else {
+    if (rcp) step_tx<ARITH, false, true>(tx, a, nslots, st);
+    else step_tx<ARITH, false, false>(tx, a, nslots, st);
+  }
+}
+
+void launch_step(int arith, bool damped, bool vel_is_rcp, int tx, const StepArgs &a, int nslots,
+                 cudaStream_t st) {
+  if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
+  if (arith == ARITH_REF) step_a<ARITH_REF>(damped, vel_is_rcp, tx, a, nslots, st);
+  else if (arith == ARITH_FAST) step_a<ARITH_FAST>(damped, vel_is_rcp, tx, a, nslots, st);
+  else step_a<ARITH_F64>(damped, vel_is_rcp, tx, a, nslots, st);
+}
+
+// ---------------------------------------------------------------- mute
+// One block per slot.  The velocity mean is the reference's sequential
+// float sum (damp4t10d.cpp:338-343): the block stages values in shared
+// memory and thread 0 adds them in the reference's (x, then depth) order.
+__global__ void k_mute_windows(int *win, const float *vel, int nxpad, int nzpad,
+                               const int *src_x, const int *src_z, const int *rec_x,
+                               const int *rec_z, long long rec_row_stride, int ng,
+                               const int *slot_shot, int half_len, int nt) {
+  constexpr int CH = 2048;
+  __shared__ float buf[CH];
+  __shared__ float s_avg;
+  int slot = blockIdx.x;
+  int shot = slot_shot ? slot_shot[slot] : slot;
+  int sx = src_x[shot], sz = src_z[shot];
+  const int *rx = rec_x + (long long)shot * rec_row_stride;
+  const int *rz = rec_z + (long long)shot * rec_row_stride;
+  int gz0 = rz[0];
+  int gmin = sz < gz0 ? sz : gz0, gmax = sz > gz0 ? sz : gz0;
+  int rows = gmax - gmin + 1;
+  long long total = (long long)nxpad * rows;
+  float acc = 0.0f;
+  for (long long base = 0; base < total; base += CH) {
+    int cnt = (int)((total - base) < CH ? (total - base) : CH);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      long long q = base + j;
+      int i = (int)(q / rows), k = gmin + (int)(q - (long long)i * rows);
+      buf[j] = vel[(long long)i * nzpad + k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int j = 0; j < cnt; j++) acc = __fadd_rn(acc, buf[j]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) s_avg = __fdiv_rn(acc, (float)(nxpad * rows));
+  __syncthreads();
+  float avg = s_avg;
+  for (int ig = threadIdx.x; ig < ng; ig += blockDim.x) {
+    int gx = rx[ig], gz = rz[ig];
+    int start = nt, end = nt;   // an unused receiver entry mutes nothing
+    if (gx >= 0) {
+      float dist = (float)((gx - sx) * (gx - sx) + (gz - sz) * (gz - sz));
+      int t = (int)__fsqrt_rn(__fmul_rn(dist, avg));
+      start = t;
+      end = (t + 2 * half_len) > nt ? nt : (t + 2 * half_len);
+    }
+    win[((long long)slot * ng + ig) * 2] = start;
+    win[((long long)slot * ng + ig) * 2 + 1] = end;
+  }
+}
+
+void launch_mute_windows(int *win, const float *vel, int nxpad, int nzpad, const int *src_x,
+                         const int *src_z, const int *rec_x, const int *rec_z,
+                         long long rec_row_stride, int ng, const int *slot_shot, int half_len,
+                         int nt, int nslots, cudaStream_t st) {
+  if (nslots <= 0) return;
+  k_mute_windows<<<nslots, kThreads, 0, st>>>(win, vel, nxpad, nzpad, src_x, src_z, rec_x, rec_z,
+                                              rec_row_stride, ng, slot_shot, half_len, nt);
+  note_launch();
+}
+
+__global__ void k_apply_mute(float *d, long long slot_stride, const int *win, int nt, int ng) {
+  int slot = blockIdx.y;
+  long long n = (long long)nt * ng;
+  float *x = d + (long long)slot * slot_stride;
+  const int *w = win + (long long)slot * ng * 2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    int it = (int)(q / ng), ig = (int)(q - (long long)it * ng);
+    if (it >= w[2 * ig] && it < w[2 * ig + 1]) x[q] = 0.0f;
+  }
+}
+
+void launch_apply_mute(float *d, long long slot_stride, const int *win, int nt, int ng, int nslots,
+                       cudaStream_t st) {
+  if (nslots <= 0) return;
+  unsigned gx = grid_for((long long)nt * ng);
+  if (gx > 2048) gx = 2048;
+  k_apply_mute<<<dim3(gx, nslots), kThreads, 0, st>>>(d, slot_stride, win, nt, ng);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- residual
+__global__ void k_muted_residual(float *r, const float *obs, long long obs_shot_stride,
+                                 const int *slot_shot, const float *cal, const int *win_obs,
+                                 const int *win_cal, int nt, int ng) {
+  int slot = blockIdx.y;
+  int shot = slot_shot ? slot_shot[slot] : slot;
+  long long n = (long long)nt * ng;
+  const float *o = obs + (long long)shot * obs_shot_stride;
+  const float *c = cal + (long long)slot * n;
+  const int *wo = win_obs + (long long)slot * ng * 2;
+  const int *wc = win_cal + (long long)slot * ng * 2;
+  float *y = r + (long long)slot * n;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    int it = (int)(q / ng), ig = (int)(q - (long long)it * ng);
+    float a = (it >= wo[2 * ig] && it < wo[2 * ig + 1]) ? 0.0f : o[q];
+    float b = (it >= wc[2 * ig] && it < wc[2 * ig + 1]) ? 0.0f : c[q];
+    y[q] = __fsub_rn(a, b);
+  }
+}
+
+void launch_muted_residual(float *r, const float *obs, long long obs_shot_stride,
+                           const int *slot_shot, const float *cal, const int *win_obs,
+                           const int *win_cal, int nt, int ng, int nslots, cudaStream_t st) {
+  if (nslots <= 0) return;
+  unsigned gx = grid_for((long long)nt * ng);
+  if (gx > 2048) gx = 2048;
+  k_muted_residual<<<dim3(gx, nslots), kThreads, 0, st>>>(r, obs, obs_shot_stride, slot_shot, cal,
+                                                          win_obs, win_cal, nt, ng);
+  note_launch();
+}
+
+__global__ void k_residual(float *r, const float *obs, long long obs_slot_stride, const float *cal,
+                           long long n) {
+  int slot = blockIdx.y;
+  const float *o = obs + (long long)slot * obs_slot_stride;
+  const float *c = cal + (long long)slot * n;
+  float *y = r + (long long)slot * n;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    y[q] = __fsub_rn(o[q], c[q]);
+}
+
+void launch_residual(float *r, const float *obs, long long obs_slot_stride, const float *cal,
+                     long long n_per_slot, int nslots, cudaStream_t st) {
+  if (nslots <= 0) return;
+  unsigned gx = grid_for(n_per_slot);
+  if (gx > 2048) gx = 2048;
+  k_residual<<<dim3(gx, nslots), kThreads, 0, st>>>(r, obs, obs_slot_stride, cal, n_per_slot);
+  note_launch();
+}
+
+__global__ void k_sumsq_partial(double *partials, const float *x, long long n, int pps) {
+  int slot = blockIdx.y;
+  const float *v = x + (long long)slot * n;
+  double acc = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    double a = (double)v[q];
+    acc = fma(a, a, acc);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[(long long)slot * pps + blockIdx.x] = acc;
+}
+
+__global__ void k_sum_partials(double *out, const double *partials, int pps) {
+  int slot = blockIdx.x;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < pps; i += blockDim.x) acc += partials[(long long)slot * pps + i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) out[slot] = acc;
+}
+
+void launch_sumsq_f64(double *out, const float *x, long long n_per_slot, int nslots,
+                      double *partials, int partials_per_slot, cudaStream_t st) {
+  if (nslots <= 0) return;
+  k_sumsq_partial<<<dim3(partials_per_slot, nslots), kThreads, 0, st>>>(partials, x, n_per_slot,
+                                                                       partials_per_slot);
+  note_launch();
+  k_sum_partials<<<nslots, kThreads, 0, st>>>(out, partials, partials_per_slot);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- transVsrc
+// fwiframework.cpp:90-91 in double:
+//   -1./12 r[i-2] + 4./3 r[i-1] - 2.5 r[i] + 4./3 r[i+1] - 1./12 r[i+2]
+// zero for i <= 1 and i >= nt-2.
+__global__ void k_trans_vsrc(float *out, const float *in, int nt, int ng) {
+  int slot = blockIdx.y;
+  long long n = (long long)nt * ng;
+  const float *x = in + (long long)slot * n;
+  float *y = out + (long long)slot * n;
+  const double c1 = -1. / 12, c2 = 4. / 3;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    int it = (int)(q / ng);
+    float v = 0.0f;
+    if (it > 1 && it < nt - 2) {
+      double acc = __dmul_rn(c1, (double)x[q - 2 * ng]);
+      acc = __dadd_rn(acc, __dmul_rn(c2, (double)x[q - ng]));
+      acc = __dsub_rn(acc, __dmul_rn(2.5, (double)x[q]));
+      acc = __dadd_rn(acc, __dmul_rn(c2, (double)x[q + ng]));
+      acc = __dsub_rn(acc, __dmul_rn(-c1, (double)x[q + 2 * ng]));
+      v = __double2float_rn(acc);
+    }
+    y[q] = v;
+  }
+}
+
+void launch_trans_vsrc(float *out, const float *in, int nt, int ng, int nslots, cudaStream_t st) {
+  if (nslots <= 0) return;
+  unsigned gx = grid_for((long long)nt * ng);
+  if (gx > 2048) gx = 2048;
+  k_trans_vsrc<<<dim3(gx, nslots), kThreads, 0, st>>>(out, in, nt, ng);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- gradient
+__global__ void k_finalize_gradient(float *g2, const float *gs, long long g_stride, int nslots,
+                                    int nxpad, int nzpad, int bx0, int accumulate) {
+  const int bz0 = 6, bzn = bx0, bxn = bx0;
+  int n = nxpad * nzpad;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    int ix = q / nzpad, iz = q - ix * nzpad;
+    bool inside = !(ix < bx0 || iz < bz0 || ix >= nxpad - bxn || iz >= nzpad - bzn);
+    float acc = accumulate ? g2[q] : 0.0f;
+    if (inside) {
+      int izi = iz - bz0;  // scaleGradient multiplies interior rows iz >= 1 by sqrt(iz)
+      float sc = izi >= 1 ? __fsqrt_rn((float)izi) : 1.0f;
+      for (int s = 0; s < nslots; s++) {
+        float v = gs[(long long)s * g_stride + q];
+        if (izi >= 1) v = __fmul_rn(v, sc);
+        acc = __fadd_rn(acc, v);
+      }
+    }
+    g2[q] = acc;
+  }
+}
+
+void launch_finalize_gradient(float *g2, const float *gs, long long g_stride, int nslots, int nxpad,
+                              int nzpad, int bx0, int accumulate, cudaStream_t st) {
+  unsigned gx = grid_for((long long)nxpad * nzpad);
+  k_finalize_gradient<<<gx, kThreads, 0, st>>>(g2, gs, g_stride, nslots, nxpad, nzpad, bx0,
+                                               accumulate);
+  note_launch();
+}
+
+__global__ void k_cg_dots(double *partials, const float *g, const float *g0, int n) {
+  double a = 0, b = 0, c = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    double x = g[q], y = g0[q];
+    a = fma(x, x, a);
+    b = fma(x, y, b);
+    c = fma(y, y, c);
+  }
+  a = block_sum(a);
+  b = block_sum(b);
+  c = block_sum(c);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x * 3 + 0] = a;
+    partials[blockIdx.x * 3 + 1] = b;
+    partials[blockIdx.x * 3 + 2] = c;
+  }
+}
+
+__global__ void k_cg_dots_final(double *out, const double *partials, int nb) {
+  double a = 0, b = 0, c = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    a += partials[3 * i];
+    b += partials[3 * i + 1];
+    c += partials[3 * i + 2];
+  }
+  a = block_sum(a);
+  b = block_sum(b);
+  c = block_sum(c);
+  if (threadIdx.x == 0) {
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+  }
+}
+
+void launch_cg_dots(double *out, const float *g, const float *g0, int n, double *partials,
+                    cudaStream_t st) {
+  const int nb = 256;
+  k_cg_dots<<<nb, kThreads, 0, st>>>(partials, g, g0, n);
+  note_launch();
+  k_cg_dots_final<<<1, kThreads, 0, st>>>(out, partials, nb);
+  note_launch();
+}
+
+__global__ void k_cg_update(float *d, float *g0, const float *g, float beta, int n, int first) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    float x = g[q];
+    d[q] = first ? x : __fadd_rn(x, __fmul_rn(beta, d[q]));
+    g0[q] = x;
+  }
+}
+
+void launch_cg_update(float *d, float *g0, const float *g, float beta, int n, int first,
+                      cudaStream_t st) {
+  k_cg_update<<<grid_for(n), kThreads, 0, st>>>(d, g0, g, beta, n, first);
+  note_launch();
+}
+
+// Ordered-int encoding so that atomicMin on int orders floats.
+__device__ __forceinline__ int float_to_ordered(float f) {
+  int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ordered_to_float(int i) {
+  return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+}
+
+__global__ void k_max_alpha(int *out, const float *vel, const float *grad, int n, float dt, float dx,
+                            float maxdv) {
+  float best = 3.402823466e+38f;  // FLT_MAX, the reference's initial value
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    float v = vel[q];
+    float tmpv = __fdiv_rn(dx, __fmul_rn(dt, __fsqrt_rn(v)));
+    tmpv = __fsub_rn(tmpv, maxdv);
+    float t = __fdiv_rn(dx, __fmul_rn(dt, tmpv));
+    tmpv = __fmul_rn(t, t);
+    float ag = fabsf(grad[q]);
+    if ((double)ag < 1e-10) continue;
+    float cand = __fdiv_rn(__fsub_rn(tmpv, v), ag);
+    if (best > cand) best = cand;
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_down_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMin(out, float_to_ordered(best));
+}
+
+__global__ void k_init_ordered(int *out) { *out = float_to_ordered(3.402823466e+38f); }
+__global__ void k_decode_ordered(float *out, const int *in) { *out = ordered_to_float(*in); }
+
+void launch_max_alpha(float *out_alpha2, const float *vel, const float *grad, int n, float dt,
+                      float dx, float maxdv, cudaStream_t st) {
+  int *tmp = reinterpret_cast<int *>(out_alpha2);
+  k_init_ordered<<<1, 1, 0, st>>>(tmp);
+  note_launch();
+  k_max_alpha<<<592, kThreads, 0, st>>>(tmp, vel, grad, n, dt, dx, maxdv);
+  note_launch();
+  k_decode_ordered<<<1, 1, 0, st>>>(out_alpha2, tmp);
+  note_launch();
+}
+
+__global__ void k_update_vel(float *newv, const float *v, const float *g, int n, float steplen,
+                             float vmin, float vmax) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    float x = __fadd_rn(v[q], __fmul_rn(steplen, g[q]));
+    if (x > vmax) x = vmax;
+    if (x < vmin) x = vmin;
+    newv[q] = x;
+  }
+}
+
+void launch_update_vel(float *newv, const float *v, const float *g, int n, float steplen,
+                       float vmin, float vmax, cudaStream_t st) {
+  k_update_vel<<<grid_for(n), kThreads, 0, st>>>(newv, v, g, n, steplen, vmin, vmax);
+  note_launch();
+}
+
+// Two phases as the reference's loops: top/bottom rows per column first,
+// then whole left/right columns.
+__global__ void k_refill_z(float *v, int nxpad, int nzpad, int bz0, int bzn) {
+  int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= nxpad) return;
+  float *col = v + (long long)ix * nzpad;
+  float top = col[bz0], bot = col[nzpad - bzn - 1];
+  for (int iz = 0; iz < bz0; iz++) col[iz] = top;
+  for (int iz = nzpad - bzn; iz < nzpad; iz++) col[iz] = bot;
+}
+
+__global__ void k_refill_x(float *v, int nxpad, int nzpad, int bx0, int bxn) {
+  int iz = blockIdx.x * blockDim.x + threadIdx.x;
+  int ix = blockIdx.y;
+  if (iz >= nzpad) return;
+  if (ix < bx0) v[(long long)ix * nzpad + iz] = v[(long long)bx0 * nzpad + iz];
+  else if (ix >= nxpad - bxn) v[(long long)ix * nzpad + iz] = v[(long long)(nxpad - bxn - 1) * nzpad + iz];
+}
+
+void launch_refill_boundary(float *v, int nxpad, int nzpad, int bz0, int bzn, int bx0, int bxn,
+                            cudaStream_t st) {
+  k_refill_z<<<grid_for(nxpad), kThreads, 0, st>>>(v, nxpad, nzpad, bz0, bzn);
+  note_launch();
+  k_refill_x<<<dim3(grid_for(nzpad), nxpad), kThreads, 0, st>>>(v, nxpad, nzpad, bx0, bxn);
+  note_launch();
+}
+
+__global__ void k_reciprocal(float *out, const float *in, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = __fdiv_rn(1.0f, in[q]);
+}
+
+void launch_reciprocal(float *out, const float *in, long long n, cudaStream_t st) {
+  unsigned g = grid_for(n);
+  if (g > 4096) g = 4096;
+  k_reciprocal<<<g, kThreads, 0, st>>>(out, in, n);
+  note_launch();
+}
+
+__global__ void k_to_f64_rcp(double *out, const float *in, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = 1.0 / (double)in[q];
+}
+
+void launch_to_f64_reciprocal(double *out, const float *in, long long n, cudaStream_t st) {
+  unsigned g = grid_for(n);
+  if (g > 4096) g = 4096;
+  k_to_f64_rcp<<<g, kThreads, 0, st>>>(out, in, n);
+  note_launch();
+}
+
+__global__ void k_encode_source(float *encsrc, const float *wlt, const int *codes, int nt, int ns) {
+  long long n = (long long)nt * ns;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    int it = (int)(q / ns), is = (int)(q - (long long)it * ns);
+    encsrc[q] = __fmul_rn(wlt[it], (float)codes[is]);
+  }
+}
+
+void launch_encode_source(float *encsrc, const float *wlt, const int *codes, int nt, int ns,
+                          cudaStream_t st) {
+  k_encode_source<<<grid_for((long long)nt * ns), kThreads, 0, st>>>(encsrc, wlt, codes, nt, ns);
+  note_launch();
+}
+
+__global__ void k_encode_obs(float *encobs, const float *dobs, const int *codes, long long n, int ns) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    float acc = 0.0f;
+    for (int is = 0; is < ns; is++)
+      acc = __fadd_rn(acc, __fmul_rn(dobs[(long long)is * n + q], (float)codes[is]));
+    encobs[q] = acc;
+  }
+}
+
+void launch_encode_obs(float *encobs, const float *dobs, const int *codes, long long n, int ns,
+                       cudaStream_t st) {
+  unsigned g = grid_for(n);
+  if (g > 8192) g = 8192;
+  k_encode_obs<<<g, kThreads, 0, st>>>(encobs, dobs, codes, n, ns);
+  note_launch();
+}
+
+__global__ void k_f32_to_f64(double *out, const float *in, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = in[q];
+}
+__global__ void k_f64_to_f32(float *out, const double *in, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x)
+    out[q] = (float)in[q];
+}
+void launch_f32_to_f64(double *out, const float *in, long long n, cudaStream_t st) {
+  unsigned g = grid_for(n);
+  if (g > 4096) g = 4096;
+  k_f32_to_f64<<<g, kThreads, 0, st>>>(out, in, n);
+  note_launch();
+}
+void launch_f64_to_f32(float *out, const double *in, long long n, cudaStream_t st) {
+  unsigned g = grid_for(n);
+  if (g > 4096) g = 4096;
+  k_f64_to_f32<<<g, kThreads, 0, st>>>(out, in, n);
+  note_launch();
+}
+
+// explicit instantiations
+template void launch_inject<float>(float *, long long, int, PointSet, const float *, long long, int,
+                                   int, cudaStream_t);
+template void launch_inject<double>(double *, long long, int, PointSet, const double *, long long,
+                                    int, int, cudaStream_t);
+template void launch_record<float>(float *, long long, const float *, long long, int, PointSet,
+                                   cudaStream_t);
+template void launch_record<double>(double *, long long, const double *, long long, int, PointSet,
+                                    cudaStream_t);
+template void launch_strip_write<float>(float *, long long, const float *, long long, int, int, int,
+                                        int, cudaStream_t);
+template void launch_strip_write<double>(double *, long long, const double *, long long, int, int,
+                                         int, int, cudaStream_t);
+template void launch_strip_read<float>(const float *, long long, float *, long long, int, int, int,
+                                       int, cudaStream_t);
+template void launch_strip_read<double>(const double *, long long, double *, long long, int, int,
+                                        int, int, cudaStream_t);
+template void launch_image<float>(float *, long long, const float *, const float *, long long, int,
+                                  int, float, cudaStream_t);
+template void launch_image<double>(double *, long long, const double *, const double *, long long,
+                                   int, int, float, cudaStream_t);
+
+}  // namespace swfwi

@@ -1,0 +1,120 @@
+// Device kernels around the stencil: source injection, receiver sampling,
+// boundary strips, imaging, and the per-iteration FWI arithmetic.
+// Every launcher is a host function taking a cudaStream_t; none allocates.
+#pragma once
+#include <atomic>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "stencil.cuh"
+
+namespace swfwi {
+
+// Kernel launches issued by this library (all launchers count).
+extern std::atomic<long long> g_kernel_launches;
+
+// ---- wavefield point operations (batched over shot slots) --------------
+// A "slot" is one wavefield in a batch; slot_shot maps it to a shot id
+// (NULL = identity).  Positions are padded linear indices x*nzpad + z, -1
+// for an unused entry (uneven receiver spreads).
+struct PointSet {
+  const int *pos;        // [shot][per_shot]
+  int per_shot;
+  const int *slot_shot;  // [nslots] or NULL
+};
+
+// field[slot][pos] += sign * vals[slot*val_slot_stride + i*val_stride]
+// (Damp4t10d::manipSource, damp4t10d.cpp:193-214: float add or subtract).
+template <typename T>
+void launch_inject(T *field, long long shot_stride, int nslots, PointSet ps, const T *vals,
+                   long long val_slot_stride, int val_stride, int sign, cudaStream_t st);
+
+// seis[slot*seis_slot_stride + i] = field[slot][pos]  (recordSeis, :163-180)
+template <typename T>
+void launch_record(T *seis, long long seis_slot_stride, const T *field, long long shot_stride,
+                   int nslots, PointSet ps, cudaStream_t st);
+
+// Boundary strips (writeBndry/readBndry, damp4t10d.cpp:478-536) for all
+// slots at one time step.  bndr layout [slot][bndr_slot_stride], one step's
+// strip of strip_size(nx,nz,bx0) values at offset it*strip_size.
+int strip_size(int nx, int nz, int bx0);
+template <typename T>
+void launch_strip_write(T *bndr, long long bndr_slot_stride, const T *field, long long shot_stride,
+                        int nslots, int nx, int nz, int bx0, cudaStream_t st);
+template <typename T>
+void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long long shot_stride,
+                       int nslots, int nx, int nz, int bx0, cudaStream_t st);
+
+// image[slot] -= s[slot] * r[slot] * scale  (cross_correlation,
+// fwiframework.cpp:107-112)
+template <typename T>
+void launch_image(T *image, long long image_stride, const T *s, const T *r, long long shot_stride,
+                  int nslots, int n, float scale, cudaStream_t st);
+
+// One FD step for all slots.
+void launch_step(int arith, bool damped, bool vel_is_rcp, int tx, const StepArgs &a, int nslots,
+                 cudaStream_t st);
+
+// ---- per-iteration arithmetic --------------------------------------------
+// Mute windows of removeDirectArrival (damp4t10d.cpp:321-365) for one
+// source position and a receiver list: win[2*i] = start, win[2*i+1] = end.
+// The velocity mean over rows [min(sz,gz), max(sz,gz)] is summed in float
+// in the reference's order by one thread.
+// shot = slot_shot ? slot_shot[slot] : slot; source (src_x[shot],
+// src_z[shot]); receivers rec_x/rec_z[shot*rec_row_stride + ig], -1 unused.
+void launch_mute_windows(int *win, const float *vel, int nxpad, int nzpad, const int *src_x,
+                         const int *src_z, const int *rec_x, const int *rec_z,
+                         long long rec_row_stride, int ng, const int *slot_shot, int half_len,
+                         int nt, int nslots, cudaStream_t st);
+// d[slot][it][ig] = 0 for it in [start, end) of trace ig.
+void launch_apply_mute(float *d, long long slot_stride, const int *win, int nt, int ng, int nslots,
+                       cudaStream_t st);
+// Muted residual in one pass: r = mute(obs) - mute(cal) where obs of slot
+// s is obs[slot_shot[s]] (NULL: s), win_obs / win_cal are the mute windows
+// of each (the same array when both use one velocity).  Zeroing both inside
+// the window and subtracting (removeDirectArrival then vectorMinus) gives
+// +0 there, as here.
+void launch_muted_residual(float *r, const float *obs, long long obs_shot_stride,
+                           const int *slot_shot, const float *cal, const int *win_obs,
+                           const int *win_cal, int nt, int ng, int nslots, cudaStream_t st);
+// r = obs - cal (vectorMinus, common.h:16-19) and its squared sum in FP64,
+// per slot: obj[slot] (FP64, one partial per block, then reduced).
+void launch_residual(float *r, const float *obs, long long obs_slot_stride, const float *cal,
+                     long long n_per_slot, int nslots, cudaStream_t st);
+void launch_sumsq_f64(double *out, const float *x, long long n_per_slot, int nslots,
+                      double *partials, int partials_per_slot, cudaStream_t st);
+// Time second derivative of fwiframework.cpp:75-105 on [slot][nt][ng].
+void launch_trans_vsrc(float *out, const float *in, int nt, int ng, int nslots, cudaStream_t st);
+// g2 = sum over slots, in slot order, of mask(scale(g[slot]))
+// (scaleGradient :309-319, maskGradient :216-226, std::transform plus).
+// accumulate = 1 continues a sum already in g2 (shots processed in chunks).
+void launch_finalize_gradient(float *g2, const float *gs, long long g_stride, int nslots, int nxpad,
+                              int nzpad, int bx0, int accumulate, cudaStream_t st);
+// Dot products for PR+ CG in FP64: out[0]=g.g out[1]=g.g0 out[2]=g0.g0
+void launch_cg_dots(double *out, const float *g, const float *g0, int n, double *partials,
+                    cudaStream_t st);
+// d = g + beta*d; g0 = g  (updateGrad, fwiframework.cpp:42-72)
+void launch_cg_update(float *d, float *g0, const float *g, float beta, int n, int first,
+                      cudaStream_t st);
+// calMaxAlpha2_3 (updatesteplenop.cpp:25-47): min over cells, written as an
+// order-independent float min.
+void launch_max_alpha(float *out_alpha2, const float *vel, const float *grad, int n, float dt,
+                      float dx, float maxdv, cudaStream_t st);
+// update_vel (updatevelop.cpp:11-21): new = clamp(v + steplen*g, vmin, vmax)
+void launch_update_vel(float *newv, const float *v, const float *g, int n, float steplen,
+                       float vmin, float vmax, cudaStream_t st);
+// refillBoundary (damp4t10d.cpp:228-252)
+void launch_refill_boundary(float *v, int nxpad, int nzpad, int bz0, int bzn, int bx0, int bxn,
+                            cudaStream_t st);
+// 1/vt, correctly rounded (the reference's 1.0f/curvel, computed once)
+void launch_reciprocal(float *out, const float *in, long long n, cudaStream_t st);
+void launch_to_f64_reciprocal(double *out, const float *in, long long n, cudaStream_t st);
+// Encoder (encoder.cpp:14-42)
+void launch_encode_source(float *encsrc, const float *wlt, const int *codes, int nt, int ns,
+                          cudaStream_t st);
+void launch_encode_obs(float *encobs, const float *dobs, const int *codes, long long n, int ns,
+                       cudaStream_t st);
+// float <-> double copies for the FP64 path
+void launch_f32_to_f64(double *out, const float *in, long long n, cudaStream_t st);
+void launch_f64_to_f32(float *out, const double *in, long long n, cudaStream_t st);
+
+}  // namespace swfwi

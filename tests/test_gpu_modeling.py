@@ -1,0 +1,171 @@
+"""Forward modelling, sources, receivers, strips and the data-side
+operations on the GPU against the reference."""
+import numpy as np
+import pytest
+
+from tests.conftest import golden, rel_l2
+from tests.golden.make_golden import small_survey
+from tests.gpu_helpers import small_method, t
+
+pytestmark = pytest.mark.gpu
+
+
+def test_forward_modeling_bit_exact(cuda):
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    wlt = t(torch, g["wlt"])
+    for shot in range(s.ns):
+        d = torch.zeros((s.nt, s.ng), device="cuda")
+        m.FwiForwardModeling(wlt, d, shot)
+        np.testing.assert_array_equal(d.cpu().numpy(), g["dcal"][shot])
+
+
+def test_forward_batch_bit_exact(cuda):
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    d = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
+    m.forward_batch(t(torch, g["wlt"]), d, [2, 0, 1])
+    np.testing.assert_array_equal(d.cpu().numpy(), g["dcal"][[2, 0, 1]])
+
+
+def test_step_by_step_api_composes_forward(cuda):
+    # FwiForwardModeling written out with the propagator's own calls
+    # (damp4t10d.cpp:272-289): addSource, stepForward, swap, recordSeis.
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    nxpad, nzpad = m.dims()[:2]
+    wlt = t(torch, g["wlt"])
+    p0 = torch.zeros((nxpad, nzpad), device="cuda")
+    p1 = torch.zeros((nxpad, nzpad), device="cuda")
+    d = torch.zeros((s.nt, s.ng), device="cuda")
+    for it in range(s.nt):
+        m.addSource(p1, wlt[it:], 1)
+        m.stepForward(p0, p1)
+        p0, p1 = p1, p0
+        m.recordSeis(d[it], p0)
+    np.testing.assert_array_equal(d.cpu().numpy(), g["dcal"][1])
+
+
+def test_fast_forward_within_tolerance(cuda, fdo):
+    import swfwi_b200 as S
+    torch = cuda
+    s, m, g, vel = small_method(torch, arith=S.ARITH_FAST)
+    d = torch.zeros((s.nt, s.ng), device="cuda")
+    m.FwiForwardModeling(t(torch, g["wlt"]), d, 1)
+    err_ref = rel_l2(d.cpu().numpy(), g["dcal"][1])
+    assert err_ref < 1e-5, err_ref
+    # FP64 GPU oracle run of the same scheme
+    d64 = torch.zeros((s.nt, s.ng), dtype=torch.float64, device="cuda")
+    m.FwiForwardModeling_f64(vel, t(torch, g["wlt"], torch.float64), d64, 1)
+    d64 = d64.cpu().numpy()
+    bx0 = s.nb + 6
+    nzpad = s.nz + s.nb + 12
+    src = (s.sxbeg + 1 * s.jsx + bx0) * nzpad + s.szbeg + 6
+    rec = (np.arange(s.ng) + bx0) * nzpad + s.gzbeg + 6
+    cpu64 = fdo.forward_f64(g["exvel_init"].astype(np.float64), bx0, s.nt, g["wlt"].astype(np.float64), src, rec)
+    assert rel_l2(d64, cpu64) < 1e-12
+    print(f"seismogram rel-L2 vs FP64: REF {rel_l2(g['dcal'][1], d64):.2e}  FAST {rel_l2(d.cpu().numpy(), d64):.2e}")
+
+
+def test_remove_direct_arrival_exact(cuda):
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    for shot in range(s.ns):
+        d = t(torch, g["dcal"][shot]).clone()
+        m.fwiRemoveDirectArrival(d, shot)
+        np.testing.assert_array_equal(d.cpu().numpy(), g["muted"][shot])
+    d = t(torch, g["dcal"][0]).clone()
+    m.removeDirectArrival(d)
+    np.testing.assert_array_equal(d.cpu().numpy(), g["muted_ess"])
+
+
+def test_trans_vsrc_exact(cuda):
+    import swfwi_b200 as S
+    torch = cuda
+    g = golden("small_survey")
+    out = torch.zeros(g["res"].shape, device="cuda")
+    S.trans_vsrc(out, t(torch, g["res"]))
+    np.testing.assert_array_equal(out.cpu().numpy(), g["vsrc"])
+
+
+def test_ess_forward_bit_exact(cuda):
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    enc = (g["wlt"][:, None] * g["ess_codes"][None, :].astype(np.float32)).astype(np.float32)
+    d = torch.zeros((s.nt, s.ng), device="cuda")
+    m.EssForwardModeling(t(torch, enc), d)
+    np.testing.assert_array_equal(d.cpu().numpy(), g["ess_dcal"])
+
+
+def test_boundary_strips_exact_and_round_trip(cuda):
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    nxpad, nzpad = m.dims()[:2]
+    field = torch.arange(nxpad * nzpad, dtype=torch.float32, device="cuda").reshape(nxpad, nzpad)
+    b = m.initBndryVector(3)
+    m.writeBndry(b, field, 2)
+    bs = m.bndrySize()
+    np.testing.assert_array_equal(b[2 * bs:].cpu().numpy(), g["bndr"])
+    assert torch.count_nonzero(b[: 2 * bs]) == 0
+    other = torch.zeros_like(field)
+    m.readBndry(b, other, 2)
+    mask = other != 0
+    assert torch.equal(other[mask], field[mask]) and int(mask.sum()) >= bs - 1
+
+
+def test_gpu_vs_reference_cfg0_grid(cuda, ref):
+    # the 151 x 461 grid of the plain-FWI workload, 300 steps, one shot
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    torch = cuda
+    s = sv.config("fwi").scaled(nt=300)
+    v = sv.layered_model(s.nx, s.nz, seed=1)
+    M = ref.model(s)
+    ex = M.expand_domain(v)
+    wlt = ref.ricker(s.nt, s.fm, s.dt)
+    want = M.fwi_forward(wlt, 7)
+    m = S.Damp4t10d.from_survey(s)
+    np.testing.assert_array_equal(m.expandDomain(v), ex)
+    vel = t(torch, ex)
+    m.bindVelocity(vel)
+    d = torch.zeros((s.nt, s.ng), device="cuda")
+    m.FwiForwardModeling(t(torch, wlt), d, 7)
+    np.testing.assert_array_equal(d.cpu().numpy(), want)
+
+
+def test_linearity_full_batched_grid(cuda):
+    # size-independent property on the 301 x 921 grid: doubling the source
+    # doubles every recorded sample exactly (a power-of-two scale is exact)
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    torch = cuda
+    s = sv.config("encoded").scaled(nt=400)
+    v = sv.layered_model(s.nx, s.nz, seed=3)
+    m = S.Damp4t10d.from_survey(s)
+    vel = t(torch, m.expandDomain(v))
+    m.bindVelocity(vel)
+    w = t(torch, S.ricker_wavelet(s.nt, s.fm, s.dt))
+    d1 = torch.zeros((2, s.nt, s.ng), device="cuda")
+    d2 = torch.zeros_like(d1)
+    m.forward_batch(w, d1, [0, 95])
+    m.forward_batch(w * 2, d2, [0, 95])
+    assert torch.equal(d2, d1 * 2)
+    assert float(d1.abs().max()) > 0
+
+
+def test_errors_reported(cuda):
+    import swfwi_b200 as S
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    d = torch.zeros((s.nt, s.ng), device="cuda")
+    with pytest.raises(S.SwfwiError) as e:
+        m.FwiForwardModeling(t(torch, g["wlt"]), d, s.ns)   # shot id out of range
+    assert e.value.status == 1
+    s2, _, _ = small_survey()
+    m2 = S.Damp4t10d.from_survey(s2)
+    with pytest.raises(S.SwfwiError) as e:
+        m2.FwiForwardModeling(t(torch, g["wlt"]), d, 0)     # no velocity bound
+    assert e.value.status == 6
+    bad = s2.scaled(gxbeg=s2.nx - 3)                        # receivers beyond the grid
+    with pytest.raises(S.SwfwiError):
+        S.Damp4t10d.from_survey(bad)
