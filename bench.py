@@ -216,6 +216,41 @@ def run_reference(args):
     return 0
 
 
+def run_kernel_mode(args):
+    """Short batched forward runs on the workload's grid and shots: the
+    autotuner's table (--mode tune) or one run at the tuned shape
+    (--mode kernel, the small case for profiling)."""
+    import torch
+    import swfwi_b200 as S
+    from swfwi_b200 import autotune
+    from swfwi_b200 import survey as sv
+    arith = S.ARITH_REF if args.arith == "ref" else S.ARITH_FAST
+    s = sv.config(CONFIG)
+    vtrue = sv.layered_model(s.nx, s.nz, seed=2024)
+    m0 = S.Damp4t10d.from_survey(s)
+    ex = m0.expandDomain(vtrue)
+    if args.mode == "tune":
+        best, table = autotune.tune(s, ex, arith, nt_probe=args.nt, verbose=True)
+        pts = (s.nxpad - 12) * (s.nzpad - 12) * s.ns
+        for us, cfg in table[:5]:
+            print(json.dumps({"us_per_launch": us, "gpts": pts / us / 1e3,
+                              "gbs": pts * 12.04 / us / 1e3, **cfg}))
+        return 0
+    ss = s.scaled(nt=args.nt)
+    m = S.Damp4t10d.from_survey(ss, arith=arith)
+    m.set_tuning(**autotune.DEFAULT)
+    vel = torch.from_numpy(ex).cuda()
+    m.bindVelocity(vel)
+    wlt = torch.from_numpy(S.ricker_wavelet(ss.nt, ss.fm, ss.dt)).cuda()
+    ids = np.arange(ss.ns, dtype=np.int32)
+    dcal = torch.zeros((ss.ns, ss.nt, m.getng()), device="cuda")
+    m.forward_batch(wlt, dcal, ids)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "kernel", "shots": ss.ns, "nt": ss.nt,
+                      "checksum": float(dcal.abs().sum().item())}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -225,9 +260,16 @@ def main():
     ap.add_argument("--arith", default="ref", choices=["ref", "fast"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--mode", default="bench", choices=["bench", "kernel", "tune"],
+                    help="kernel: short 96-shot batched forward (the small case for ncu); "
+                         "tune: print the autotuner's table")
+    ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode != "bench":
+        return run_kernel_mode(args)
 
     import torch
     import swfwi_b200 as S
@@ -242,6 +284,11 @@ def main():
     arith = S.ARITH_REF if args.arith == "ref" else S.ARITH_FAST
     s, m, exi, exi_h, wlt, wlt_h, dobs, ids = setup_workload(torch, arith)
     nxpad, nzpad, ns, ngmax, nt = m.dims()
+    from swfwi_b200 import autotune
+    tuning = dict(autotune.DEFAULT)
+    if not args.no_tune:
+        tuning, _ = autotune.tune(s, exi_h, arith)
+    m.set_tuning(**tuning)
     grad = torch.zeros((nxpad, nzpad), dtype=torch.float32, device="cuda")
 
     for _ in range(max(args.warmup, 0)):
@@ -341,7 +388,7 @@ def main():
                 "config": {"workload": "batched FWI gradient, 96 shots, 301x921 grid (993x337 padded), "
                                        "nt=4000, uneven spreads 200-921",
                            "shots": int(ns), "nt": int(nt), "grid": [int(nxpad), int(nzpad)],
-                           "arith": args.arith, "strips": "f32",
+                           "arith": args.arith, "strips": "f32", "tuning": tuning,
                            "point_updates_per_step": updates_rank / args.steps,
                            "l2": "inputs larger than L2 (strips 14 GB, fields 0.5 GB): no flush",
                            "parallelism": f"replicas{world}",

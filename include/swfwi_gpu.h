@@ -15,8 +15,8 @@
  *  - Every entry point returns a status (SWFWI_OK = 0).  swfwi_last_error()
  *    gives the text of the last failure on the calling thread.
  *  - Calls on one handle are ordered on that handle's CUDA stream
- *    (swfwi_damp4t10d_set_stream); functions that return host values
- *    synchronise that stream.
+ *    (swfwi_damp4t10d_set_stream; a new handle uses the legacy default
+ *    stream 0); functions that return host values synchronise that stream.
  */
 #ifndef SWFWI_GPU_H
 #define SWFWI_GPU_H
@@ -95,11 +95,19 @@ int swfwi_damp4t10d_create(swfwi_damp4t10d **out, const swfwi_shot_position *src
                            const swfwi_shot_position *geo, float dt, float dx, float fm, int nb,
                            int nt);
 int swfwi_damp4t10d_destroy(swfwi_damp4t10d *h);
-/* Order this handle's work on a caller stream (cudaStream_t); NULL returns
- * to the handle's own stream. */
+/* Order this handle's work on a caller stream (cudaStream_t); NULL is the
+ * legacy default stream. */
 int swfwi_damp4t10d_set_stream(swfwi_damp4t10d *h, void *stream);
 int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith);
 int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
+/* Launch shape of the propagator's stencil (results do not depend on it):
+ * kernel 0 = streaming step (band depth 120 or 248 = one or two warps,
+ * rows ahead 3 or 5), kernel 1 = warp-specialised streaming step (band
+ * depth 120, 248 or 376 = 1-3 consumer warps plus a copy warp, rows ahead 2
+ * or 4); rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot
+ * together. */
+int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
+                               int rows_in_flight, int shots_slowest);
 /* Per-shot receiver lists (uneven spreads; not in the reference, whose
  * ShotPosition is one common line): shot s has receivers
  * [offsets[s], offsets[s+1]) of gx/gz (unpadded, host arrays).  The

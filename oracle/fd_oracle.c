@@ -182,9 +182,11 @@ void fdo_gradient_f64(const double *vel, int nx, int nz, int nb, int nt, double 
     for (int ig = 0; ig < ng; ig++) gp1[rec_pos[ig]] += vsrc[(size_t)it * ng + ig];
     fdo_step_f64(gp0, gp1, vel, nx, nz, nb, 1);
     t = gp0; gp0 = gp1; gp1 = t;
-    double tt = (double)(float)(dt * it), w;
+    /* the reference passes the taper as a float (cross_correlation's
+     * scale parameter): t = dt*it in float, the ramp rounded to float */
+    double tt = (double)(float)((float)dt * (float)it), w;
     if (tt > 0.4) w = 1.0;
-    else if (tt > 0.3) w = (tt - 0.3) / 0.1;
+    else if (tt > 0.3) w = (double)(float)((tt - 0.3) / 0.1);
     else break;
     for (size_t i = 0; i < n; i++) g[i] -= sp0[i] * gp0[i] * w;
   }

@@ -10,8 +10,27 @@
 extern "C" {
 
 /* Silence the reference logger (logger.h:120-123 skips output when the
- * terminal stream is NULL). */
-void ref_quiet(void) { Output2FILE::TerminalStream() = NULL; }
+ * terminal stream is NULL), and size the reference's scratch once.
+ *
+ * Damp4t10d::stepForward/stepBackward keep their u2 scratch in a
+ * function-local static vector sized by the FIRST call's grid
+ * (damp4t10d.cpp:154, 189); a later call on a larger grid writes past it.
+ * One step on a grid larger than any workload here (3200 x 1100 padded
+ * points) sizes both statics before anything else runs. */
+void ref_quiet(void) {
+  Output2FILE::TerminalStream() = NULL;
+  static bool sized = false;
+  if (sized) return;
+  sized = true;
+  const int nxp = 3200, nzp = 1100;
+  ShotPosition s(0, 0, 0, 1, 1, nzp), g(0, 0, 0, 1, 1, nzp);
+  Damp4t10d fm(s, g, 0.001f, 10.0f, 10.0f, 30, 1);
+  Velocity v(std::vector<float>((size_t)nxp * nzp, 1.0f), nxp, nzp);
+  fm.bindVelocity(v);
+  std::vector<float> p0((size_t)nxp * nzp, 0.0f), p1((size_t)nxp * nzp, 0.0f);
+  fm.stepForward(&p0[0], &p1[0]);
+  fm.stepBackward(&p0[0], &p1[0]);
+}
 
 void *ref_model_create(int nz, int nx, int nb, int nt, float dt, float dx, float fm,
                        int szbeg, int sxbeg, int jsz, int jsx, int ns,

@@ -59,6 +59,7 @@ _SIGS = {
     "swfwi_damp4t10d_set_stream": [_vp, _vp],
     "swfwi_damp4t10d_set_arith": [_vp, C.c_int],
     "swfwi_damp4t10d_set_strip_format": [_vp, C.c_int],
+    "swfwi_damp4t10d_set_tuning": [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
     "swfwi_damp4t10d_set_receivers_per_shot": [_vp, _ip, _ip, _ip],
     "swfwi_damp4t10d_dims": [_vp, _ip, _ip, _ip, _ip, _ip],
     "swfwi_damp4t10d_expand_domain": [_vp, _fp, C.c_int, C.c_int, _fp],
@@ -315,6 +316,12 @@ class Damp4t10d:
     def set_arith(self, arith: int):
         _check(lib().swfwi_damp4t10d_set_arith(self.h, arith))
         self.arith = arith
+
+    def set_tuning(self, kernel: int = 1, band_depth: int = 376, rows_per_cta: int = 128,
+                   rows_in_flight: int = 4, shots_slowest: bool = False):
+        """Launch shape of the stencil (results do not change)."""
+        _check(lib().swfwi_damp4t10d_set_tuning(self.h, kernel, band_depth, rows_per_cta, rows_in_flight,
+                                                int(shots_slowest)))
 
     def setReceiversPerShot(self, offsets, gx, gz):
         o = np.ascontiguousarray(offsets, np.int32)

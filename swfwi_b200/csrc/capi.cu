@@ -55,6 +55,7 @@ StepArgs drop_in_args(float *prev, const float *curr, const float *vel, int nx, 
   a.vel = vel;
   a.nx = nx;
   a.nz = nz;
+  a.pitch = nz;
   a.bx0 = nb;
   a.shot_stride = stride;
   a.vel_stride = 0;
@@ -133,6 +134,7 @@ int swfwi_fd4t10s_step_f64(double *prev, const double *curr, const double *vel, 
     a.vel = vel;
     a.nx = nx;
     a.nz = nz;
+    a.pitch = nz;
     a.bx0 = nb;
     a.shot_stride = 0;
     a.vel_stride = 0;
@@ -177,6 +179,27 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format) {
   return guarded([&] {
     SWFWI_REQUIRE(format == SWFWI_STRIP_F32, "only FP32 strips are available");
     P(h).strip_format = format;
+  });
+}
+
+int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
+                               int rows_in_flight, int shots_slowest) {
+  return guarded([&] {
+    SWFWI_REQUIRE(kernel == 0 || kernel == 1, "kernel must be 0 or 1");
+    if (kernel == 0) {
+      SWFWI_REQUIRE(band_depth == 120 || band_depth == 248, "band depth must be 120 or 248");
+      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 5, "rows in flight must be 3 or 5");
+    } else {
+      SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,
+                    "band depth must be 120, 248 or 376");
+      SWFWI_REQUIRE(rows_in_flight == 2 || rows_in_flight == 4, "rows in flight must be 2 or 4");
+    }
+    SWFWI_REQUIRE(rows_per_cta >= 1, "rows per CTA must be positive");
+    P(h).stream_kernel = kernel;
+    P(h).stream_bz = band_depth;
+    P(h).stream_xchunk = rows_per_cta;
+    P(h).stream_depth = rows_in_flight;
+    P(h).stream_shot_major = shots_slowest ? 1 : 0;
   });
 }
 

@@ -41,38 +41,30 @@ void StepTimer::read(double &ms, long long &n, double &pts, double &b) {
   b = bytes;
 }
 
-// One FD step for n slots; when timing is on, brackets it with events on
-// the launching stream and books its algorithmic work: every interior point
-// of every slot is updated (12 B: read current and previous, write next),
-// and the velocity shared by the slots is read once (4 B a point).
-void timed_step(int arith, bool damped, int tx, const StepArgs &a, int n, cudaStream_t st) {
-  StepTimer &t = step_timer();
-  bool on = t.enabled.load(std::memory_order_relaxed);
-  std::pair<cudaEvent_t, cudaEvent_t> ev{};
-  if (on) {
-    std::lock_guard<std::mutex> g(t.mu);
-    if (t.used == t.pool.size()) {
-      cudaEvent_t x, y;
-      SWFWI_CUDA(cudaEventCreate(&x));
-      SWFWI_CUDA(cudaEventCreate(&y));
-      t.pool.emplace_back(x, y);
-    }
-    ev = t.pool[t.used++];
-    double pts = (double)(a.nx - 12) * (a.nz - 12);
-    size_t el = arith == ARITH_F64 ? 8 : 4;
-    t.launches++;
-    t.points += pts * n;
-    t.bytes += pts * n * 3 * el + pts * el * ((n + a.shots_per_vel - 1) / a.shots_per_vel);
-    SWFWI_CUDA(cudaEventRecord(ev.first, st));
+// Algorithmic work of one step launch: every interior point of every field
+// is updated (read current and previous, write next: 3 elements), and each
+// velocity model the launch uses is read once.
+cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el) {
+  if (!enabled.load(std::memory_order_relaxed)) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  if (used == pool.size()) {
+    cudaEvent_t x, y;
+    SWFWI_CUDA(cudaEventCreate(&x));
+    SWFWI_CUDA(cudaEventCreate(&y));
+    pool.emplace_back(x, y);
   }
-  launch_step(arith, damped, true, tx, a, n, st);
-  if (on) SWFWI_CUDA(cudaEventRecord(ev.second, st));
+  auto ev = pool[used++];
+  launches++;
+  points += pts * n;
+  bytes += pts * n * 3 * el + pts * el * nvel;
+  SWFWI_CUDA(cudaEventRecord(ev.first, st));
+  return ev.second;
 }
 
 Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, float fm_, int nb_,
                        int nt_)
     : nx(0), nz(0), nb(nb_), nt(nt_), ns(src.n), ng(geo.n), ngmax(geo.n), dt(dt_), dx(dx_),
-      fm(fm_), nxpad(0), nzpad(0), fstride(0), bsize(0) {
+      fm(fm_), nxpad(0), nzpad(0), pitch(0), fstride(0), bsize(0) {
   SWFWI_REQUIRE(nb_ >= 0 && nt_ > 0 && src.n > 0 && geo.n > 0, "bad propagator sizes");
   SWFWI_REQUIRE(dt_ > 0 && dx_ > 0 && fm_ > 0, "dt, dx, fm must be positive");
   // Damp4t10d::Damp4t10d (damp4t10d.cpp:367-376)
@@ -82,8 +74,6 @@ Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, f
   // half_len = t_width / dt truncated (damp4t10d.cpp:322, 391).
   float t_width = (float)(1.5 / (double)fm_);
   half_len = (int)(t_width / dt_);
-  SWFWI_CUDA(cudaStreamCreateWithFlags(&own_st_, cudaStreamNonBlocking));
-  st_ = own_st_;
   h_src_x.resize(ns);
   h_src_z.resize(ns);
   for (int i = 0; i < ns; i++) {
@@ -104,13 +94,14 @@ Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, f
       h_rec_x[(size_t)s * ng + i] = h_geo_x[i];
       h_rec_z[(size_t)s * ng + i] = h_geo_z[i];
     }
+  d_err_.resize(1);
+  SWFWI_CUDA(cudaMemset(d_err_.get(), 0, sizeof(int)));
 }
 
-Propagator::~Propagator() {
-  if (own_st_) cudaStreamDestroy(own_st_);
-}
+// the handle owns no stream: work goes to the caller's (default: legacy stream 0)
+Propagator::~Propagator() {}
 
-void Propagator::set_stream(cudaStream_t s) { st_ = s ? s : own_st_; }
+void Propagator::set_stream(cudaStream_t s) { st_ = s; }
 
 void Propagator::set_receivers_per_shot(const int *offsets, const int *gx, const int *gz) {
   SWFWI_REQUIRE(offsets && gx && gz, "null receiver arrays");
@@ -170,55 +161,79 @@ void Propagator::expand_domain(const float *v, float *out) const {
 }
 
 void Propagator::upload_geometry() {
-  std::vector<int> sp(ns), sx(ns), sz(ns), gp(ng), gxp(ng), gzp(ng);
+  std::vector<int> sp(ns), spp(ns), sx(ns), sz(ns), gp(ng), gpp(ng), gxp(ng), gzp(ng);
+  auto inside = [&](int x, int z) { return x >= 6 && x < nxpad - 6 && z >= 6 && z < nzpad - 6; };
   for (int i = 0; i < ns; i++) {
     sx[i] = h_src_x[i] + bx0;
     sz[i] = h_src_z[i] + bz0;
-    SWFWI_REQUIRE(sx[i] >= 6 && sx[i] < nxpad - 6 && sz[i] >= 6 && sz[i] < nzpad - 6,
-                  "source outside the computing zone");
+    SWFWI_REQUIRE(inside(sx[i], sz[i]), "source outside the computing zone");
     sp[i] = sx[i] * nzpad + sz[i];
+    spp[i] = sx[i] * pitch + sz[i];
   }
   for (int i = 0; i < ng; i++) {
     gxp[i] = h_geo_x[i] + bx0;
     gzp[i] = h_geo_z[i] + bz0;
-    SWFWI_REQUIRE(gxp[i] >= 6 && gxp[i] < nxpad - 6 && gzp[i] >= 6 && gzp[i] < nzpad - 6,
-                  "receiver outside the computing zone");
+    SWFWI_REQUIRE(inside(gxp[i], gzp[i]), "receiver outside the computing zone");
     gp[i] = gxp[i] * nzpad + gzp[i];
+    gpp[i] = gxp[i] * pitch + gzp[i];
   }
-  std::vector<int> rp((size_t)ns * ngmax, -1), rx((size_t)ns * ngmax, -1), rz((size_t)ns * ngmax, -1);
-  for (int s = 0; s < ns; s++)
-    for (int i = 0; i < ngmax; i++) {
-      size_t k = (size_t)s * ngmax + i;
-      if (h_rec_x[k] < 0) continue;
-      rx[k] = h_rec_x[k] + bx0;
-      rz[k] = h_rec_z[k] + bz0;
-      SWFWI_REQUIRE(rx[k] >= 6 && rx[k] < nxpad - 6 && rz[k] >= 6 && rz[k] < nzpad - 6,
-                    "receiver outside the computing zone");
-      rp[k] = rx[k] * nzpad + rz[k];
-    }
+  size_t nr = (size_t)ns * ngmax;
+  std::vector<int> rpp(nr, -1), rx(nr, -1), rz(nr, -1);
+  for (size_t k = 0; k < nr; k++) {
+    if (h_rec_x[k] < 0) continue;
+    rx[k] = h_rec_x[k] + bx0;
+    rz[k] = h_rec_z[k] + bz0;
+    SWFWI_REQUIRE(inside(rx[k], rz[k]), "receiver outside the computing zone");
+    rpp[k] = rx[k] * pitch + rz[k];
+  }
   // Positions within one injection set must be distinct (the reference adds
   // sequentially; the device adds in parallel).
   {
     std::vector<int> t = sp;
     std::sort(t.begin(), t.end());
     SWFWI_REQUIRE(std::adjacent_find(t.begin(), t.end()) == t.end(), "duplicate source positions");
+    t = gp;
+    std::sort(t.begin(), t.end());
+    SWFWI_REQUIRE(std::adjacent_find(t.begin(), t.end()) == t.end(), "duplicate receiver positions");
     for (int s = 0; s < ns; s++) {
-      std::vector<int> r(rp.begin() + (size_t)s * ngmax, rp.begin() + (size_t)(s + 1) * ngmax);
+      std::vector<int> r(rpp.begin() + (size_t)s * ngmax, rpp.begin() + (size_t)(s + 1) * ngmax);
       r.erase(std::remove(r.begin(), r.end(), -1), r.end());
       std::sort(r.begin(), r.end());
       SWFWI_REQUIRE(std::adjacent_find(r.begin(), r.end()) == r.end(), "duplicate receiver positions");
     }
   }
   d_src_pos_.upload(sp, st_);
+  d_src_pos_p_.upload(spp, st_);
   d_src_x_.upload(sx, st_);
   d_src_z_.upload(sz, st_);
   d_geo_pos_.upload(gp, st_);
+  d_geo_pos_p_.upload(gpp, st_);
   d_geo_x_.upload(gxp, st_);
   d_geo_z_.upload(gzp, st_);
-  d_rec_pos_.upload(rp, st_);
+  d_rec_pos_p_.upload(rpp, st_);
   d_rec_x_.upload(rx, st_);
   d_rec_z_.upload(rz, st_);
   SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+// Called once the padded size is known (from expandDomain or a bind).
+void Propagator::set_dims(int nxpad_, int nzpad_) {
+  SWFWI_REQUIRE(nxpad_ > 2 * bx0 && nzpad_ > bz0 + bzn, "grid smaller than its padding");
+  if (nxpad == nxpad_ && nzpad == nzpad_) return;
+  nxpad = nxpad_;
+  nzpad = nzpad_;
+  nx = nxpad - 2 * nb - 12;
+  nz = nzpad - nb - 12;
+  // rows keep 8 spare floats before depth 0 (the origin offset) and end on a
+  // 32-byte boundary; slots hold the origin offset plus all rows
+  pitch = (int)round_up(nzpad + kStreamCoff, 8);
+  fstride = round_up((long long)nxpad * pitch + 2 * kStreamCoff, 64);
+  damp_x_.resize(nxpad);
+  damp_z_.resize(nzpad);
+  launch_damp_tables(damp_x_.get(), damp_z_.get(), nxpad, nzpad, bx0, st_);
+  bsize = strip_size(nxpad, nzpad, bx0);
+  rcp_for_ = nullptr;
+  upload_geometry();
 }
 
 void Propagator::bind_velocity(const float *exvel) {
@@ -230,54 +245,112 @@ void Propagator::bind_velocity(const float *exvel) {
 
 const float *Propagator::rcp_of(const float *vel) {
   SWFWI_REQUIRE(vel != nullptr, "no velocity bound");
-  long long n = (long long)nxpad * nzpad;
+  size_t n = (size_t)nxpad * pitch;
   if (vel == vel_) {
     if (rcp_for_ != vel_) {
-      rcp_.resize(n);
-      launch_reciprocal(rcp_.get(), vel_, n, st_);
+      rcp_.resize(n + 2 * kStreamCoff);
+      launch_pitched_reciprocal(rcp_.get() + kStreamCoff, vel_, nxpad, nzpad, pitch, st_);
       rcp_for_ = vel_;
     }
-    return rcp_.get();
+    return rcp_.get() + kStreamCoff;
   }
-  trial_rcp_.resize(n);
-  launch_reciprocal(trial_rcp_.get(), vel, n, st_);
-  return trial_rcp_.get();
+  trial_rcp_.resize(n + 2 * kStreamCoff);
+  launch_pitched_reciprocal(trial_rcp_.get() + kStreamCoff, vel, nxpad, nzpad, pitch, st_);
+  return trial_rcp_.get() + kStreamCoff;
 }
 
-StepArgs Propagator::step_args(void *prev, const void *curr, const void *velrcp, int n) const {
-  StepArgs a;
-  a.prev = prev;
-  a.curr = curr;
-  a.vel = velrcp;
+void Propagator::check_device_error() {
+  int e = 0;
+  SWFWI_CUDA(cudaMemcpyAsync(&e, d_err_.get(), sizeof(int), cudaMemcpyDeviceToHost, st_));
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+  if (e) {
+    SWFWI_CUDA(cudaMemsetAsync(d_err_.get(), 0, sizeof(int), st_));
+    throw Error(SWFWI_ERR_TIMEOUT, "a stencil kernel's bounded wait on its row pipeline gave up");
+  }
+}
+
+// One FD step for n propagator-owned fields (pitched rows, fstride apart,
+// one velocity model): the streaming TMA kernel for float arithmetics, the
+// shared-memory tile kernel for FP64.
+void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp,
+                             int n) {
+  double pts = (double)(nxpad - 12) * (nzpad - 12);
+  if (ar == ARITH_F64) {
+    cudaEvent_t done = step_timer().open(st_, pts, n, 1, 8);
+    StepArgs a;
+    a.prev = prev;
+    a.curr = curr;
+    a.vel = velrcp;
+    a.nx = nxpad;
+    a.nz = nzpad;
+    a.pitch = pitch;
+    a.bx0 = bx0;
+    a.shot_stride = fstride;
+    a.vel_stride = 0;
+    a.shots_per_vel = std::max(n, 1);
+    launch_step(ARITH_F64, damped, true, 32, a, n, st_);
+    if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
+    return;
+  }
+  cudaEvent_t done = step_timer().open(st_, pts, n, 1, 4);
+  StreamArgs a;
+  a.prev = static_cast<float *>(prev);
+  a.curr = static_cast<const float *>(curr);
+  a.rcp = static_cast<const float *>(velrcp);
+  a.damp_x = damp_x_.get();
+  a.damp_z = damp_z_.get();
   a.nx = nxpad;
   a.nz = nzpad;
-  a.bx0 = bx0;
+  a.pitch = pitch;
   a.shot_stride = fstride;
   a.vel_stride = 0;
   a.shots_per_vel = std::max(n, 1);
-  return a;
+  a.xchunk = stream_xchunk;
+  a.shot_major = stream_shot_major;
+  a.err = d_err_.get();
+  if (stream_kernel == 1) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  else launch_stream_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
 }
 
-// ---- single-field operations ------------------------------------------
+// ---- single-field operations on caller arrays ([nxpad][nzpad]) ---------
+namespace {
+StepArgs caller_args(float *p0, const float *p1, const float *vel, int nxpad, int nzpad, int bx0) {
+  StepArgs a;
+  a.prev = p0;
+  a.curr = p1;
+  a.vel = vel;
+  a.nx = nxpad;
+  a.nz = nzpad;
+  a.pitch = nzpad;
+  a.bx0 = bx0;
+  a.shot_stride = 0;
+  a.vel_stride = 0;
+  a.shots_per_vel = 1;
+  return a;
+}
+}  // namespace
+
 void Propagator::step_forward(float *p0, float *p1) {
-  SWFWI_REQUIRE(p0 && p1, "null field");
-  timed_step(arith, true, tile_tx, step_args(p0, p1, rcp_of(vel_), 1), 1, st_);
+  SWFWI_REQUIRE(p0 && p1 && vel_, "null field or no velocity");
+  cudaEvent_t done = step_timer().open(st_, (double)(nxpad - 12) * (nzpad - 12), 1, 1, 4);
+  launch_step(arith, true, false, 32, caller_args(p0, p1, vel_, nxpad, nzpad, bx0), 1, st_);
+  if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
 }
 
 void Propagator::step_backward(float *p0, float *p1) {
-  SWFWI_REQUIRE(p0 && p1, "null field");
-  timed_step(arith, false, tile_tx, step_args(p0, p1, rcp_of(vel_), 1), 1, st_);
+  SWFWI_REQUIRE(p0 && p1 && vel_, "null field or no velocity");
+  cudaEvent_t done = step_timer().open(st_, (double)(nxpad - 12) * (nzpad - 12), 1, 1, 4);
+  launch_step(arith, false, false, 32, caller_args(p0, p1, vel_, nxpad, nzpad, bx0), 1, st_);
+  if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
 }
 
 void Propagator::manip_source(float *p, const float *src, int shot_id, int sign) {
   SWFWI_REQUIRE(p && src, "null pointer");
   SWFWI_REQUIRE(shot_id >= -1 && shot_id < ns, "shot id out of range");
   PointSet ps;
-  if (shot_id >= 0) {
-    ps = {d_src_pos_.get() + shot_id, 1, nullptr};
-  } else {
-    ps = {d_src_pos_.get(), ns, nullptr};
-  }
+  if (shot_id >= 0) ps = {d_src_pos_.get() + shot_id, 1, nullptr};
+  else ps = {d_src_pos_.get(), ns, nullptr};
   launch_inject<float>(p, 0, 1, ps, src, 0, 1, sign, st_);
 }
 
@@ -293,12 +366,12 @@ void Propagator::record_seis(float *seis, const float *p) {
 
 void Propagator::write_bndry(float *bndr, const float *p, int it) {
   SWFWI_REQUIRE(bndr && p && it >= 0, "bad strip arguments");
-  launch_strip_write<float>(bndr + (long long)it * bsize, 0, p, 0, 1, nxpad, nzpad, bx0, st_);
+  launch_strip_write<float>(bndr + (long long)it * bsize, 0, p, 0, 1, nxpad, nzpad, bx0, nzpad, st_);
 }
 
 void Propagator::read_bndry(const float *bndr, float *p, int it) {
   SWFWI_REQUIRE(bndr && p && it >= 0, "bad strip arguments");
-  launch_strip_read<float>(bndr + (long long)it * bsize, 0, p, 0, 1, nxpad, nzpad, bx0, st_);
+  launch_strip_read<float>(bndr + (long long)it * bsize, 0, p, 0, 1, nxpad, nzpad, bx0, nzpad, st_);
 }
 
 namespace {
@@ -351,42 +424,42 @@ void Propagator::remove_direct_arrival(float *data, int shot_id, const float *ve
   launch_apply_mute(data, 0, d_win1_.get(), nt, ng, 1, st_);
 }
 
+// ---- time loops ----------------------------------------------------------
 template <typename T>
-void Propagator::ensure_work(Work<T> &w, int n, bool strips, int ngrec) {
+void Propagator::ensure_work(Work<T> &w, int n, bool strips) {
   size_t f = (size_t)n * fstride;
   w.p0.resize(f);
   w.p1.resize(f);
   if (strips) w.strips.resize((size_t)n * nt * bsize);
   w.partials.resize((size_t)n * kPartials);
   w.obj.resize(n);
-  (void)ngrec;
 }
 
 template <typename T>
 void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                              long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
                              bool save_strips, const void *velrcp) {
-  ensure_work(w, n, save_strips, ngrec);
-  T *p0 = w.p0.get(), *p1 = w.p1.get();
+  ensure_work(w, n, save_strips);
+  T *p0 = w.p0.get() + kStreamCoff, *p1 = w.p1.get() + kStreamCoff;
   w.p0.zero(st_);
   w.p1.zero(st_);
-  int ar = sizeof(T) == 8 ? ARITH_F64 : arith;
+  int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
   for (int it = 0; it < nt; it++) {
     // addSource -> stepForward -> swap -> recordSeis / writeBndry
     // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
     launch_inject<T>(p1, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
                      +1, st_);
-    timed_step(ar, true, tile_tx, step_args(p0, p1, velrcp, n), n, st_);
+    step_fields(ar, true, p0, p1, velrcp, n);
     std::swap(p0, p1);
     if (dcal)
       launch_record<T>(dcal + (long long)it * ngrec, (long long)nt * ngrec, p0, fstride, n, rec, st_);
     if (save_strips)
       launch_strip_write<T>(w.strips.get() + (long long)it * bsize, bstride, p0, fstride, n, nxpad,
-                            nzpad, bx0, st_);
+                            nzpad, bx0, pitch, st_);
   }
   // leave the final (current, next) pair for a backward sweep
-  if (p0 != w.p0.get()) std::swap(w.p0, w.p1);
+  if (p0 != w.p0.get() + kStreamCoff) std::swap(w.p0, w.p1);
 }
 
 template <typename T>
@@ -398,57 +471,70 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   w.g1.resize(f);
   w.g0.zero(st_);
   w.g1.zero(st_);
-  T *sp0 = w.p0.get(), *sp1 = w.p1.get(), *gp0 = w.g0.get(), *gp1 = w.g1.get();
-  int ar = sizeof(T) == 8 ? ARITH_F64 : arith;
+  T *sp0 = w.p0.get() + kStreamCoff, *sp1 = w.p1.get() + kStreamCoff;
+  T *gp0 = w.g0.get() + kStreamCoff, *gp1 = w.g1.get() + kStreamCoff;
+  int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
-  int npts = nxpad * nzpad;
+  int npts = (int)fstride;
   for (int it = nt - 1; it >= 0; it--) {
     // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
     // subSource; receiver addSource -> stepForward -> swap; image.
     launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad,
-                         nzpad, bx0, st_);
+                         nzpad, bx0, pitch, st_);
     std::swap(sp0, sp1);
-    timed_step(ar, false, tile_tx, step_args(sp0, sp1, velrcp, n), n, st_);
+    step_fields(ar, false, sp0, sp1, velrcp, n);
     launch_inject<T>(sp0, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
                      -1, st_);
     launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1,
                      +1, st_);
-    timed_step(ar, true, tile_tx, step_args(gp0, gp1, velrcp, n), n, st_);
+    step_fields(ar, true, gp0, gp1, velrcp, n);
     std::swap(gp0, gp1);
     float t = dt * (float)it;
     float scale;
     if ((double)t > 0.4) scale = 1.0f;
     else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
     else break;
-    launch_image<T>(w.image.get(), fstride, sp0, gp0, fstride, n, npts, scale, st_);
+    launch_image<T>(w.image.get() + kStreamCoff, fstride, sp0, gp0, fstride, n, npts, scale, st_);
   }
+}
+
+template <typename T>
+void Propagator::to_pitched(T *dst, const T *src) {
+  SWFWI_CUDA(cudaMemcpy2DAsync(dst, sizeof(T) * pitch, src, sizeof(T) * nzpad, sizeof(T) * nzpad,
+                               nxpad, cudaMemcpyDeviceToDevice, st_));
+}
+
+template <typename T>
+void Propagator::from_pitched(T *dst, const T *src) {
+  SWFWI_CUDA(cudaMemcpy2DAsync(dst, sizeof(T) * nzpad, src, sizeof(T) * pitch, sizeof(T) * nzpad,
+                               nxpad, cudaMemcpyDeviceToDevice, st_));
 }
 
 void Propagator::fwi_forward(const float *wlt, float *dcal, int shot_id) {
   SWFWI_REQUIRE(wlt && dcal, "null pointer");
   SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
-  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
-  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  PointSet src{d_src_pos_p_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
   run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, rcp_of(vel_));
 }
 
 void Propagator::ess_forward(const float *encsrc, float *dcal, const float *vel) {
   SWFWI_REQUIRE(encsrc && dcal, "null pointer");
-  PointSet src{d_src_pos_.get(), ns, nullptr};
-  PointSet rec{d_geo_pos_.get(), ng, nullptr};
-  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false,
-                     rcp_of(vel ? vel : vel_));
+  PointSet src{d_src_pos_p_.get(), ns, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false, rcp_of(vel ? vel : vel_));
 }
 
 int Propagator::max_batch() const {
   size_t freeb = 0, total = 0;
   if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) return 1;
-  // per slot: p0,p1,g0,g1,image fields; strips; dcal,res,vsrc data
+  // per slot: p0, p1, g0, g1, image fields; strips; dcal, res, vsrc data
   double per = 5.0 * fstride * 4 + (double)nt * bsize * 4 + 3.0 * nt * ngmax * 4 + 4096;
   double budget = 0.85 * (double)freeb;
   // memory already held by this propagator's work space counts as free
-  budget += (double)(w_.p0.size() + w_.p1.size() + w_.g0.size() + w_.g1.size() + w_.image.size() +
-                     w_.strips.size() + w_.dcal.size() + w_.res.size() + w_.vsrc.size()) * 4;
+  budget += (double)(w_.p0.capacity() + w_.p1.capacity() + w_.g0.capacity() + w_.g1.capacity() +
+                     w_.image.capacity() + w_.strips.capacity() + w_.dcal.capacity() +
+                     w_.res.capacity() + w_.vsrc.capacity()) * 4;
   int m = (int)(budget / per);
   return std::max(1, std::min(m, ns));
 }
@@ -462,8 +548,8 @@ void Propagator::forward_batch(const float *wlt, float *dcal, const int *ids, in
   for (int c0 = 0; c0 < n; c0 += mb) {
     int k = std::min(mb, n - c0);
     w_.slot_shot.upload(ids + c0, k, st_);
-    PointSet src{d_src_pos_.get(), 1, w_.slot_shot.get()};
-    PointSet rec{d_rec_pos_.get(), ngmax, w_.slot_shot.get()};
+    PointSet src{d_src_pos_p_.get(), 1, w_.slot_shot.get()};
+    PointSet rec{d_rec_pos_p_.get(), ngmax, w_.slot_shot.get()};
     run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, dcal + (long long)c0 * nt * ngmax,
                        false, rcp);
   }
@@ -485,8 +571,8 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
       w_.slot_row.upload(rows + c0, k, st_);
       rr = w_.slot_row.get();
     }
-    PointSet src{d_src_pos_.get(), 1, ss};
-    PointSet rec{d_rec_pos_.get(), ngmax, ss};
+    PointSet src{d_src_pos_p_.get(), 1, ss};
+    PointSet rec{d_rec_pos_p_.get(), ngmax, ss};
     w_.dcal.resize((size_t)k * dn);
     w_.res.resize((size_t)k * dn);
     w_.vsrc.resize((size_t)k * dn);
@@ -503,14 +589,14 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
     launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);
     launch_trans_vsrc(w_.vsrc.get(), w_.res.get(), nt, ngmax, k, st_);
     run_backward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.vsrc.get(), rcp);
-    launch_finalize_gradient(grad, w_.image.get(), fstride, k, nxpad, nzpad, bx0,
+    launch_finalize_gradient(grad, w_.image.get() + kStreamCoff, fstride, k, nxpad, nzpad, bx0, pitch,
                              (accumulate || c0 > 0) ? 1 : 0, st_);
     if (obj) {
       SWFWI_CUDA(cudaMemcpyAsync(obj + c0, w_.obj.get(), sizeof(double) * k, cudaMemcpyDeviceToHost,
                                  st_));
     }
   }
-  if (obj) SWFWI_CUDA(cudaStreamSynchronize(st_));
+  if (obj) check_device_error();
 }
 
 double Propagator::trial_objective_fwi(const float *wlt, const float *dobs, const int *ids, int n,
@@ -521,30 +607,29 @@ double Propagator::trial_objective_fwi(const float *wlt, const float *dobs, cons
   long long dn = (long long)nt * ngmax;
   std::vector<double> h;
   double total = 0.0;
-  DevBuf<int> win_obs;
   for (int c0 = 0; c0 < n; c0 += mb) {
     int k = std::min(mb, n - c0);
     w_.slot_shot.upload(ids + c0, k, st_);
     const int *ss = w_.slot_shot.get();
-    PointSet src{d_src_pos_.get(), 1, ss};
-    PointSet rec{d_rec_pos_.get(), ngmax, ss};
+    PointSet src{d_src_pos_p_.get(), 1, ss};
+    PointSet rec{d_rec_pos_p_.get(), ngmax, ss};
     w_.dcal.resize((size_t)k * dn);
     w_.res.resize((size_t)k * dn);
     w_.win.resize((size_t)k * ngmax * 2);
-    win_obs.resize((size_t)k * ngmax * 2);
+    w_.win2.resize((size_t)k * ngmax * 2);
     run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), false, rcp);
     // modelled data muted with the trial velocity, observed data with the
     // current one (updatesteplenop.cpp:77 and essfwiframework.cpp:205)
     launch_mute_windows(w_.win.get(), trial_vel, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
                         d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
-    launch_mute_windows(win_obs.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
+    launch_mute_windows(w_.win2.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
                         d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
-    launch_muted_residual(w_.res.get(), dobs, dn, ss, w_.dcal.get(), win_obs.get(), w_.win.get(),
-                          nt, ngmax, k, st_);
+    launch_muted_residual(w_.res.get(), dobs, dn, ss, w_.dcal.get(), w_.win2.get(), w_.win.get(), nt,
+                          ngmax, k, st_);
     launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);
     h.resize(k);
     SWFWI_CUDA(cudaMemcpyAsync(h.data(), w_.obj.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, st_));
-    SWFWI_CUDA(cudaStreamSynchronize(st_));
+    check_device_error();
     for (int i = 0; i < k; i++) total += h[i];
   }
   return total;
@@ -553,72 +638,56 @@ double Propagator::trial_objective_fwi(const float *wlt, const float *dobs, cons
 void Propagator::calgradient_ess(const float *encsrc, const float *vsrc, float *grad) {
   SWFWI_REQUIRE(encsrc && vsrc && grad, "null pointer");
   const float *rcp = rcp_of(vel_);
-  PointSet src{d_src_pos_.get(), ns, nullptr};
-  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  PointSet src{d_src_pos_p_.get(), ns, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
   w_.image.resize((size_t)fstride);
-  SWFWI_CUDA(cudaMemcpyAsync(w_.image.get(), grad, sizeof(float) * nxpad * nzpad,
-                             cudaMemcpyDeviceToDevice, st_));
+  w_.image.zero(st_);
+  to_pitched(w_.image.get() + kStreamCoff, grad);
   run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp);
   run_backward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, rcp);
-  SWFWI_CUDA(cudaMemcpyAsync(grad, w_.image.get(), sizeof(float) * nxpad * nzpad,
-                             cudaMemcpyDeviceToDevice, st_));
+  from_pitched(grad, w_.image.get() + kStreamCoff);
 }
 
 void Propagator::calgradient_fwi(const float *wlt, const float *vsrc, float *grad, int shot_id) {
   SWFWI_REQUIRE(wlt && vsrc && grad, "null pointer");
   SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
   const float *rcp = rcp_of(vel_);
-  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
-  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  PointSet src{d_src_pos_p_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
   w_.image.resize((size_t)fstride);
-  SWFWI_CUDA(cudaMemcpyAsync(w_.image.get(), grad, sizeof(float) * nxpad * nzpad,
-                             cudaMemcpyDeviceToDevice, st_));
+  w_.image.zero(st_);
+  to_pitched(w_.image.get() + kStreamCoff, grad);
   run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp);
   run_backward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, rcp);
-  SWFWI_CUDA(cudaMemcpyAsync(grad, w_.image.get(), sizeof(float) * nxpad * nzpad,
-                             cudaMemcpyDeviceToDevice, st_));
+  from_pitched(grad, w_.image.get() + kStreamCoff);
 }
 
 void Propagator::calgradient_fwi_f64(const float *vel, const double *wlt, const double *vsrc,
                                      double *grad, int shot_id) {
   SWFWI_REQUIRE(vel && wlt && vsrc && grad, "null pointer");
   SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
-  long long np = (long long)nxpad * nzpad;
-  DevBuf<double> r64(np);
-  launch_to_f64_reciprocal(r64.get(), vel, np, st_);
-  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
-  PointSet rec{d_geo_pos_.get(), ng, nullptr};
+  DevBuf<double> r64((size_t)nxpad * pitch + 2 * kStreamCoff);
+  launch_to_f64_reciprocal(r64.get() + kStreamCoff, vel, nxpad, nzpad, pitch, st_);
+  PointSet src{d_src_pos_p_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
   wd_.image.resize((size_t)fstride);
-  SWFWI_CUDA(cudaMemcpyAsync(wd_.image.get(), grad, sizeof(double) * np, cudaMemcpyDeviceToDevice, st_));
-  run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, r64.get());
-  run_backward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, r64.get());
-  SWFWI_CUDA(cudaMemcpyAsync(grad, wd_.image.get(), sizeof(double) * np, cudaMemcpyDeviceToDevice, st_));
+  wd_.image.zero(st_);
+  to_pitched(wd_.image.get() + kStreamCoff, grad);
+  run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, r64.get() + kStreamCoff);
+  run_backward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, r64.get() + kStreamCoff);
+  from_pitched(grad, wd_.image.get() + kStreamCoff);
   SWFWI_CUDA(cudaStreamSynchronize(st_));
 }
 
 void Propagator::fwi_forward_f64(const float *vel, const double *wlt, double *dcal, int shot_id) {
   SWFWI_REQUIRE(vel && wlt && dcal, "null pointer");
   SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
-  long long np = (long long)nxpad * nzpad;
-  DevBuf<double> r64(np);
-  launch_to_f64_reciprocal(r64.get(), vel, np, st_);
-  PointSet src{d_src_pos_.get() + shot_id, 1, nullptr};
-  PointSet rec{d_geo_pos_.get(), ng, nullptr};
-  run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, r64.get());
+  DevBuf<double> r64((size_t)nxpad * pitch + 2 * kStreamCoff);
+  launch_to_f64_reciprocal(r64.get() + kStreamCoff, vel, nxpad, nzpad, pitch, st_);
+  PointSet src{d_src_pos_p_.get() + shot_id, 1, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
+  run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, r64.get() + kStreamCoff);
   SWFWI_CUDA(cudaStreamSynchronize(st_));
-}
-
-// Called once the padded size is known (from expandDomain or a bind).
-void Propagator::set_dims(int nxpad_, int nzpad_) {
-  SWFWI_REQUIRE(nxpad_ > 2 * bx0 && nzpad_ > bz0 + bzn, "grid smaller than its padding");
-  if (nxpad == nxpad_ && nzpad == nzpad_) return;
-  nxpad = nxpad_;
-  nzpad = nzpad_;
-  nx = nxpad - 2 * nb - 12;
-  nz = nzpad - nb - 12;
-  fstride = round_up((long long)nxpad * nzpad, 64);
-  bsize = strip_size(nxpad, nzpad, bx0);
-  upload_geometry();
 }
 
 }  // namespace swfwi

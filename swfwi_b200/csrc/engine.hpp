@@ -1,6 +1,13 @@
 // The propagator: swfwi's Damp4t10d on the GPU, plus batched whole-shot
 // forward modelling and gradients.  Host C++ over the kernels in
-// kernels.cu / stencil.cuh.
+// kernels.cu / stencil.cuh / stream.cuh.
+//
+// Wavefields the propagator owns are stored with rows of `pitch` floats
+// (nzpad + 8 rounded up to 8) behind an 8-float origin offset, so every row
+// and every 4-depth group starts on a 16-byte boundary and the streaming step
+// can move rows with TMA bulk copies; pointers to them passed to kernels are
+// origins (slot start + 8).  Arrays the caller owns keep the reference's
+// [nxpad][nzpad] layout.
 #pragma once
 #include <atomic>
 #include <mutex>
@@ -21,9 +28,12 @@ struct StepTimer {
   double points = 0, bytes = 0;
   void reset();
   void read(double &ms, long long &n, double &pts, double &b);
+  // Opens the timing of one launch over n fields of pts interior points
+  // reading nvel velocity models, el bytes an element; returns the event to
+  // record after the launch (null when timing is off).
+  cudaEvent_t open(cudaStream_t st, double pts, int n, int nvel, int el);
 };
 StepTimer &step_timer();
-void timed_step(int arith, bool damped, int tx, const StepArgs &a, int n, cudaStream_t st);
 
 // A regular line of points (src/common/shot-position.cpp:11-41).
 struct Line {
@@ -36,8 +46,8 @@ struct Line {
 template <typename T>
 struct Work {
   DevBuf<T> p0, p1, g0, g1, image, strips;
-  DevBuf<float> dcal, obs, res, vsrc;   // [slot][nt][ng]
-  DevBuf<int> win, slot_shot, slot_row;
+  DevBuf<float> dcal, res, vsrc;   // [slot][nt][ngmax]
+  DevBuf<int> win, win2, slot_shot, slot_row;
   DevBuf<double> partials, obj;
 };
 
@@ -51,7 +61,8 @@ class Propagator {
   float dt, dx, fm;
   int bx0, bxn, bz0, bzn;
   int nxpad, nzpad;
-  long long fstride;   // floats between batched fields (aligned)
+  int pitch;           // floats per row of propagator-owned fields
+  long long fstride;   // floats between batched fields (multiple of 64)
   int bsize;           // strip floats per step
   int half_len;        // direct-arrival mute half window (samples)
 
@@ -59,7 +70,11 @@ class Propagator {
   cudaStream_t stream() const { return st_; }
   int arith = ARITH_REF;
   int strip_format = SWFWI_STRIP_F32;
-  int tile_tx = 32;
+  int stream_kernel = 1;      // 0: streaming step, 1: warp-specialised streaming step
+  int stream_bz = 376;        // output depths per CTA (120, 248; 376 warp-specialised only)
+  int stream_xchunk = 128;    // rows per CTA
+  int stream_depth = 4;       // rows ahead (3 or 5; warp-specialised 2 or 4)
+  int stream_shot_major = 0;  // launch order: 0 = shots fastest
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);
   void set_dims(int nxpad, int nzpad);   // padded grid; uploads geometry
@@ -67,7 +82,8 @@ class Propagator {
   void bind_velocity(const float *exvel_dev);
   const float *velocity() const { return vel_; }
 
-  // ---- reference-compatible single-field operations (device pointers) ----
+  // ---- reference-compatible single-field operations (device pointers,
+  // caller layout [nxpad][nzpad]) ----
   void step_forward(float *p0, float *p1);
   void step_backward(float *p0, float *p1);
   void manip_source(float *p, const float *src, int shot_id, int sign);
@@ -83,20 +99,18 @@ class Propagator {
   void ess_forward(const float *encsrc, float *dcal, const float *vel = nullptr);
 
   // ---- batched ----
-  // dcal [n][nt][ng] for shots ids[0..n) (host list).
+  // dcal [n][nt][ngmax] for shots ids[0..n) (host list).
   void forward_batch(const float *wlt, float *dcal, const int *ids, int n,
                      const float *vel = nullptr);
   // Gradient loop of FwiFramework::epoch for the listed shots; grad
-  // overwritten (or accumulated if accumulate); obj[n] host.
-  // rows (host, optional): the dobs row of each listed shot (default: the
-  // shot id itself).
+  // overwritten (or accumulated); obj[n] host.  rows (host, optional): the
+  // dobs row of each listed shot (default: the shot id).
   void gradient_batch(const float *wlt, const float *dobs, const int *ids, int n, float *grad,
                       double *obj, bool accumulate = false, const int *rows = nullptr);
-  // Trial objective: sum over listed shots of |mute_obs - mute_cal(vel)|^2
-  // with the observed data muted with the bound velocity (host result).
+  // Trial objective: sum over listed shots of |mute(obs) - mute(cal(vel))|^2,
+  // the observed data muted with the bound velocity (host result).
   double trial_objective_fwi(const float *wlt, const float *dobs, const int *ids, int n,
                              const float *trial_vel);
-  // Encoded supershot pieces.
   void calgradient_ess(const float *encsrc, const float *vsrc, float *grad);
   void calgradient_fwi(const float *wlt, const float *vsrc, float *grad, int shot_id);
   void calgradient_fwi_f64(const float *vel, const double *wlt, const double *vsrc, double *grad,
@@ -105,43 +119,54 @@ class Propagator {
 
   // Max shots per batch that fit the device memory budget.
   int max_batch() const;
+  // Raises SWFWI_ERR_TIMEOUT if a kernel's bounded wait gave up (syncs).
+  void check_device_error();
 
-  // host mirrors of geometry (padded coordinates)
+  // host mirrors of geometry (unpadded coordinates)
   std::vector<int> h_src_x, h_src_z, h_geo_x, h_geo_z;
   std::vector<int> h_rec_x, h_rec_z;   // [ns][ngmax], -1 padded
   std::vector<int> h_rec_count;
 
  private:
-  cudaStream_t st_ = nullptr, own_st_ = nullptr;
+  cudaStream_t st_ = nullptr;   // 0 = the legacy default stream
   const float *vel_ = nullptr;
-  DevBuf<float> rcp_;
+  DevBuf<float> rcp_;           // pitched 1/vt of the bound velocity
   const float *rcp_for_ = nullptr;
-  DevBuf<int> d_src_pos_, d_src_x_, d_src_z_;
-  DevBuf<int> d_geo_pos_, d_geo_x_, d_geo_z_;
-  DevBuf<int> d_rec_pos_, d_rec_x_, d_rec_z_;
-  DevBuf<int> d_win1_;
-  DevBuf<double> d_scalar_;
   DevBuf<float> trial_rcp_;
+  DevBuf<int> d_err_;
+  DevBuf<float> damp_x_, damp_z_;   // per-axis sponge ramps (streaming step)
+  // positions in the caller's layout (x*nzpad + z) ...
+  DevBuf<int> d_src_pos_, d_geo_pos_;
+  // ... and in the propagator's pitched layout (x*pitch + z)
+  DevBuf<int> d_src_pos_p_, d_geo_pos_p_, d_rec_pos_p_;
+  // padded coordinates for the mute windows
+  DevBuf<int> d_src_x_, d_src_z_, d_geo_x_, d_geo_z_, d_rec_x_, d_rec_z_;
+  DevBuf<int> d_win1_;
   Work<float> w_;
   Work<double> wd_;
 
   void upload_geometry();
   const float *rcp_of(const float *vel);
-  StepArgs step_args(void *prev, const void *curr, const void *velrcp, int n) const;
+  void step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp, int n);
 
-  // Runs the forward time loop for n slots already described by src/rec
-  // point sets.  Source values: vals + it*it_stride + slot*slot_stride +
-  // i*i_stride.
+  // Forward time loop for n slots.  Source values:
+  // vals + it*it_stride + slot*slot_stride + i*i_stride.
   template <typename T>
   void run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                    long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
                    bool save_strips, const void *velrcp);
+  // Backward sweep with imaging into w.image (not cleared here).
   template <typename T>
   void run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                     long long slot_stride, int i_stride, PointSet rec, int ngrec, const T *vsrc,
-                    const void *velrcp_damped);
+                    const void *velrcp);
   template <typename T>
-  void ensure_work(Work<T> &w, int n, bool strips, int ngrec);
+  void ensure_work(Work<T> &w, int n, bool strips);
+  // copies between the caller's [nxpad][nzpad] layout and pitched rows
+  template <typename T>
+  void to_pitched(T *dst, const T *src);
+  template <typename T>
+  void from_pitched(T *dst, const T *src);
 };
 
 }  // namespace swfwi

@@ -96,25 +96,25 @@ int strip_size(int nx, int nz, int bx0) {
 // Strip element i -> padded field index.  Bottom: 6 rows below the
 // interior, x from bx0-6 to nx-bx0+6, stored [ix][iz]; then the left and
 // right 6-column bands over the interior depth, stored [ix][iz].
-__device__ __forceinline__ long long strip_index(int i, int nx, int nz, int bx0) {
+__device__ __forceinline__ long long strip_index(int i, int nx, int nz, int bx0, int pitch) {
   const int w = 6, nxs = nx - 2 * (bx0 - w), nzs = nz - 6 - bx0;
   if (i < w * nxs) {
     int ix = i / w, iz = i - ix * w;
-    return (long long)(ix + bx0 - w) * nz + (nz - bx0 + iz);
+    return (long long)(ix + bx0 - w) * pitch + (nz - bx0 + iz);
   }
   int j = i - w * nxs;
   int ix = j / nzs, iz = j - ix * nzs;
   int gx = ix < w ? (bx0 - w + ix) : (nx - bx0 + ix - w);
-  return (long long)gx * nz + (6 + iz);
+  return (long long)gx * pitch + (6 + iz);
 }
 
 template <typename T, bool WRITE>
 __global__ void k_strip(T *bndr, long long bndr_slot_stride, T *field, long long shot_stride, int bs,
-                        int nx, int nz, int bx0) {
+                        int nx, int nz, int bx0, int pitch) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int slot = blockIdx.y;
   if (i >= bs) return;
-  long long p = strip_index(i, nx, nz, bx0);
+  long long p = strip_index(i, nx, nz, bx0, pitch);
   T *f = field + (long long)slot * shot_stride + p;
   T *b = bndr + (long long)slot * bndr_slot_stride + i;
   if (WRITE) *b = *f; else *f = *b;
@@ -122,21 +122,21 @@ __global__ void k_strip(T *bndr, long long bndr_slot_stride, T *field, long long
 
 template <typename T>
 void launch_strip_write(T *bndr, long long bndr_slot_stride, const T *field, long long shot_stride,
-                        int nslots, int nx, int nz, int bx0, cudaStream_t st) {
+                        int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st) {
   int bs = strip_size(nx, nz, bx0);
   dim3 g(grid_for(bs), nslots);
   k_strip<T, true><<<g, kThreads, 0, st>>>(bndr, bndr_slot_stride, const_cast<T *>(field), shot_stride,
-                                            bs, nx, nz, bx0);
+                                            bs, nx, nz, bx0, pitch);
   note_launch();
 }
 
 template <typename T>
 void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long long shot_stride,
-                       int nslots, int nx, int nz, int bx0, cudaStream_t st) {
+                       int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st) {
   int bs = strip_size(nx, nz, bx0);
   dim3 g(grid_for(bs), nslots);
   k_strip<T, false><<<g, kThreads, 0, st>>>(const_cast<T *>(bndr), bndr_slot_stride, field,
-                                             shot_stride, bs, nx, nz, bx0);
+                                             shot_stride, bs, nx, nz, bx0, pitch);
   note_launch();
 }
 
@@ -400,18 +400,19 @@ void launch_trans_vsrc(float *out, const float *in, int nt, int ng, int nslots, 
 
 // ---------------------------------------------------------------- gradient
 __global__ void k_finalize_gradient(float *g2, const float *gs, long long g_stride, int nslots,
-                                    int nxpad, int nzpad, int bx0, int accumulate) {
+                                    int nxpad, int nzpad, int bx0, int pitch, int accumulate) {
   const int bz0 = 6, bzn = bx0, bxn = bx0;
   int n = nxpad * nzpad;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     int ix = q / nzpad, iz = q - ix * nzpad;
+    long long qp = (long long)ix * pitch + iz;
     bool inside = !(ix < bx0 || iz < bz0 || ix >= nxpad - bxn || iz >= nzpad - bzn);
     float acc = accumulate ? g2[q] : 0.0f;
     if (inside) {
       int izi = iz - bz0;  // scaleGradient multiplies interior rows iz >= 1 by sqrt(iz)
       float sc = izi >= 1 ? __fsqrt_rn((float)izi) : 1.0f;
       for (int s = 0; s < nslots; s++) {
-        float v = gs[(long long)s * g_stride + q];
+        float v = gs[(long long)s * g_stride + qp];
         if (izi >= 1) v = __fmul_rn(v, sc);
         acc = __fadd_rn(acc, v);
       }
@@ -421,9 +422,9 @@ __global__ void k_finalize_gradient(float *g2, const float *gs, long long g_stri
 }
 
 void launch_finalize_gradient(float *g2, const float *gs, long long g_stride, int nslots, int nxpad,
-                              int nzpad, int bx0, int accumulate, cudaStream_t st) {
+                              int nzpad, int bx0, int pitch, int accumulate, cudaStream_t st) {
   unsigned gx = grid_for((long long)nxpad * nzpad);
-  k_finalize_gradient<<<gx, kThreads, 0, st>>>(g2, gs, g_stride, nslots, nxpad, nzpad, bx0,
+  k_finalize_gradient<<<gx, kThreads, 0, st>>>(g2, gs, g_stride, nslots, nxpad, nzpad, bx0, pitch,
                                                accumulate);
   note_launch();
 }
@@ -583,16 +584,134 @@ void launch_reciprocal(float *out, const float *in, long long n, cudaStream_t st
   note_launch();
 }
 
-__global__ void k_to_f64_rcp(double *out, const float *in, long long n) {
+// out[x*pitch + z] = 1/in[x*nz + z] (padding columns set to 1).
+template <typename T>
+__global__ void k_pitched_rcp(T *out, const float *in, int nx, int nz, int pitch) {
+  long long n = (long long)nx * pitch;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
-       q += (long long)gridDim.x * blockDim.x)
-    out[q] = 1.0 / (double)in[q];
+       q += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(q / pitch), z = (int)(q - (long long)x * pitch);
+    if (z < nz) {
+      float v = in[(long long)x * nz + z];
+      if constexpr (sizeof(T) == 4) out[q] = __fdiv_rn(1.0f, v);
+      else out[q] = 1.0 / (double)v;
+    } else {
+      out[q] = T(1);
+    }
+  }
 }
 
-void launch_to_f64_reciprocal(double *out, const float *in, long long n, cudaStream_t st) {
-  unsigned g = grid_for(n);
+void launch_pitched_reciprocal(float *out, const float *in, int nx, int nz, int pitch,
+                               cudaStream_t st) {
+  unsigned g = grid_for((long long)nx * pitch);
   if (g > 4096) g = 4096;
-  k_to_f64_rcp<<<g, kThreads, 0, st>>>(out, in, n);
+  k_pitched_rcp<float><<<g, kThreads, 0, st>>>(out, in, nx, nz, pitch);
+  note_launch();
+}
+
+void launch_to_f64_reciprocal(double *out, const float *in, int nx, int nz, int pitch,
+                              cudaStream_t st) {
+  unsigned g = grid_for((long long)nx * pitch);
+  if (g > 4096) g = 4096;
+  k_pitched_rcp<double><<<g, kThreads, 0, st>>>(out, in, nx, nz, pitch);
+  note_launch();
+}
+
+// Sponge ramps of fd4t10s-damp-zjh.c:64-80 split by axis: dist_x[ix] is the
+// left/right ramp (0 inside), dist_z[iz] the bottom ramp (-1 above it, where
+// the left/right one applies).
+__global__ void k_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nx) {
+    float d = 0.0f;
+    if (i < nb) d = __fdiv_rn((float)(nb - i), (float)nb);
+    if (i >= nx - nb) d = __fdiv_rn((float)(i - (nx - nb) + 1), (float)nb);
+    dist_x[i] = d;
+  }
+  if (i < nz) dist_z[i] = i >= nz - nb ? __fdiv_rn((float)(i - (nz - nb) + 1), (float)nb) : -1.0f;
+}
+
+void launch_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb, cudaStream_t st) {
+  int n = nx > nz ? nx : nz;
+  k_damp_tables<<<grid_for(n), kThreads, 0, st>>>(dist_x, dist_z, nx, nz, nb);
+  note_launch();
+}
+
+// ---------------------------------------------------------------- streaming step
+template <int ARITH, bool DAMPED, int NW, int D>
+static void stream_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+  constexpr int BZ = 128 * NW - 8;
+  int nbands = (a.nz - 10 + BZ - 1) / BZ;
+  int nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
+  dim3 g = a.shot_major ? dim3(nbands, nchunks, nslots) : dim3(nslots, nbands, nchunks);
+  fd_step_stream<ARITH, DAMPED, NW, D><<<g, NW * 32, 0, st>>>(a);
+}
+
+template <int ARITH, bool DAMPED, int D>
+static void stream_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (bz >= 248) stream_t<ARITH, DAMPED, 2, D>(a, nslots, st);
+  else stream_t<ARITH, DAMPED, 1, D>(a, nslots, st);
+}
+
+template <int ARITH, bool DAMPED>
+static void stream_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (depth >= 5) stream_nw<ARITH, DAMPED, 5>(bz, a, nslots, st);
+  else stream_nw<ARITH, DAMPED, 3>(bz, a, nslots, st);
+}
+
+// ---------------------------------------------------------------- warp-specialised step
+template <int ARITH, bool DAMPED, int NW, int D>
+static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+  constexpr int BZ = 128 * NW - 8;
+  constexpr size_t smem = ws_smem_bytes<NW, D>();
+  static bool attr_set = false;   // raise the dynamic shared memory limit once
+  if (!attr_set) {
+    cudaFuncSetAttribute(fd_step_ws<ARITH, DAMPED, NW, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_set = true;
+  }
+  int nbands = (a.nz - 10 + BZ - 1) / BZ;
+  int nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
+  dim3 g = a.shot_major ? dim3(nbands, nchunks, nslots) : dim3(nslots, nbands, nchunks);
+  fd_step_ws<ARITH, DAMPED, NW, D><<<g, (NW + 1) * 32, smem, st>>>(a);
+}
+
+template <int ARITH, bool DAMPED, int D>
+static void ws_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (bz >= 376) ws_t<ARITH, DAMPED, 3, D>(a, nslots, st);
+  else if (bz >= 248) ws_t<ARITH, DAMPED, 2, D>(a, nslots, st);
+  else ws_t<ARITH, DAMPED, 1, D>(a, nslots, st);
+}
+
+template <int ARITH, bool DAMPED>
+static void ws_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (depth >= 4) ws_nw<ARITH, DAMPED, 4>(bz, a, nslots, st);
+  else ws_nw<ARITH, DAMPED, 2>(bz, a, nslots, st);
+}
+
+void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
+                    cudaStream_t st) {
+  if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
+  if (arith == ARITH_REF) {
+    if (damped) ws_d<ARITH_REF, true>(depth, bz, a, nslots, st);
+    else ws_d<ARITH_REF, false>(depth, bz, a, nslots, st);
+  } else {
+    if (damped) ws_d<ARITH_FAST, true>(depth, bz, a, nslots, st);
+    else ws_d<ARITH_FAST, false>(depth, bz, a, nslots, st);
+  }
+  note_launch();
+}
+
+void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamArgs &a,
+                        int nslots, cudaStream_t st) {
+  if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
+  if (arith == ARITH_REF) {
+    if (damped) stream_d<ARITH_REF, true>(depth, bz, a, nslots, st);
+    else stream_d<ARITH_REF, false>(depth, bz, a, nslots, st);
+  } else {
+    if (damped) stream_d<ARITH_FAST, true>(depth, bz, a, nslots, st);
+    else stream_d<ARITH_FAST, false>(depth, bz, a, nslots, st);
+  }
   note_launch();
 }
 
@@ -662,13 +781,13 @@ template void launch_record<float>(float *, long long, const float *, long long,
 template void launch_record<double>(double *, long long, const double *, long long, int, PointSet,
                                     cudaStream_t);
 template void launch_strip_write<float>(float *, long long, const float *, long long, int, int, int,
-                                        int, cudaStream_t);
-template void launch_strip_write<double>(double *, long long, const double *, long long, int, int,
-                                         int, int, cudaStream_t);
-template void launch_strip_read<float>(const float *, long long, float *, long long, int, int, int,
-                                       int, cudaStream_t);
-template void launch_strip_read<double>(const double *, long long, double *, long long, int, int,
                                         int, int, cudaStream_t);
+template void launch_strip_write<double>(double *, long long, const double *, long long, int, int,
+                                         int, int, int, cudaStream_t);
+template void launch_strip_read<float>(const float *, long long, float *, long long, int, int, int,
+                                       int, int, cudaStream_t);
+template void launch_strip_read<double>(const double *, long long, double *, long long, int, int,
+                                        int, int, int, cudaStream_t);
 template void launch_image<float>(float *, long long, const float *, const float *, long long, int,
                                   int, float, cudaStream_t);
 template void launch_image<double>(double *, long long, const double *, const double *, long long,

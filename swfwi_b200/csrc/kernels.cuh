@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "stencil.cuh"
+#include "stream.cuh"
+#include "stream_ws.cuh"
 
 namespace swfwi {
 
@@ -39,10 +41,10 @@ void launch_record(T *seis, long long seis_slot_stride, const T *field, long lon
 int strip_size(int nx, int nz, int bx0);
 template <typename T>
 void launch_strip_write(T *bndr, long long bndr_slot_stride, const T *field, long long shot_stride,
-                        int nslots, int nx, int nz, int bx0, cudaStream_t st);
+                        int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st);
 template <typename T>
 void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long long shot_stride,
-                       int nslots, int nx, int nz, int bx0, cudaStream_t st);
+                       int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st);
 
 // image[slot] -= s[slot] * r[slot] * scale  (cross_correlation,
 // fwiframework.cpp:107-112)
@@ -50,9 +52,19 @@ template <typename T>
 void launch_image(T *image, long long image_stride, const T *s, const T *r, long long shot_stride,
                   int nslots, int n, float scale, cudaStream_t st);
 
-// One FD step for all slots.
+// One FD step for all slots: shared-memory tile form (any pitch, any
+// arithmetic) and streaming TMA form (float, 16-byte aligned pitched rows;
+// bz = 120 or 248 output depths per CTA, depth = 3 or 5 rows in flight).
 void launch_step(int arith, bool damped, bool vel_is_rcp, int tx, const StepArgs &a, int nslots,
                  cudaStream_t st);
+void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamArgs &a,
+                        int nslots, cudaStream_t st);
+// Warp-specialised streaming step (stream_ws.cuh): bz = 120, 248 or 376
+// output depths per CTA (1-3 consumer warps), depth = 2 or 4 rows ahead.
+void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
+                    cudaStream_t st);
+// Per-axis sponge ramps for the streaming step (see stream.cuh).
+void launch_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb, cudaStream_t st);
 
 // ---- per-iteration arithmetic --------------------------------------------
 // Mute windows of removeDirectArrival (damp4t10d.cpp:321-365) for one
@@ -87,8 +99,9 @@ void launch_trans_vsrc(float *out, const float *in, int nt, int ng, int nslots, 
 // g2 = sum over slots, in slot order, of mask(scale(g[slot]))
 // (scaleGradient :309-319, maskGradient :216-226, std::transform plus).
 // accumulate = 1 continues a sum already in g2 (shots processed in chunks).
+// gs rows have pitch floats; g2 is [nxpad][nzpad].
 void launch_finalize_gradient(float *g2, const float *gs, long long g_stride, int nslots, int nxpad,
-                              int nzpad, int bx0, int accumulate, cudaStream_t st);
+                              int nzpad, int bx0, int pitch, int accumulate, cudaStream_t st);
 // Dot products for PR+ CG in FP64: out[0]=g.g out[1]=g.g0 out[2]=g0.g0
 void launch_cg_dots(double *out, const float *g, const float *g0, int n, double *partials,
                     cudaStream_t st);
@@ -105,9 +118,13 @@ void launch_update_vel(float *newv, const float *v, const float *g, int n, float
 // refillBoundary (damp4t10d.cpp:228-252)
 void launch_refill_boundary(float *v, int nxpad, int nzpad, int bz0, int bzn, int bx0, int bxn,
                             cudaStream_t st);
-// 1/vt, correctly rounded (the reference's 1.0f/curvel, computed once)
+// 1/vt, correctly rounded (the reference's 1.0f/curvel, computed once),
+// from [nx][nz] into rows of pitch floats (padding columns 1).
 void launch_reciprocal(float *out, const float *in, long long n, cudaStream_t st);
-void launch_to_f64_reciprocal(double *out, const float *in, long long n, cudaStream_t st);
+void launch_pitched_reciprocal(float *out, const float *in, int nx, int nz, int pitch,
+                               cudaStream_t st);
+void launch_to_f64_reciprocal(double *out, const float *in, int nx, int nz, int pitch,
+                              cudaStream_t st);
 // Encoder (encoder.cpp:14-42)
 void launch_encode_source(float *encsrc, const float *wlt, const int *codes, int nt, int ns,
                           cudaStream_t st);

@@ -45,6 +45,7 @@ struct StepArgs {
   const void *curr;     // same
   const void *vel;      // vt, or 1/vt when VEL_IS_RCP
   int nx, nz;           // padded grid
+  int pitch;            // elements between rows (>= nz)
   int bx0;              // sponge width + 6 (damping ramp length)
   long long shot_stride;   // elements between the fields of consecutive shots
   long long vel_stride;    // elements between velocity models
@@ -180,7 +181,7 @@ fd_step_tile(StepArgs a) {
   __shared__ T sc[CX * CZ];
   __shared__ T su[UX * UZ];
 
-  const int nx = a.nx, nz = a.nz;
+  const int nx = a.nx, nz = a.nz, pitch = a.pitch;
   const int shot = blockIdx.z;
   const int x0 = H + blockIdx.y * TX;
   const int z0 = H + blockIdx.x * kTZ;
@@ -200,7 +201,7 @@ fd_step_tile(StepArgs a) {
     pv[k] = 0;
     rv[k] = 1;
     if (gx < nx - H && gz < nz - H) {
-      long long idx = (long long)gx * nz + gz;
+      long long idx = (long long)gx * pitch + gz;
       pv[k] = prev[idx];
       rv[k] = vel[idx];
     }
@@ -211,7 +212,7 @@ fd_step_tile(StepArgs a) {
     int lx = i / CZ, lz = i - lx * CZ;
     int gx = x0 - H + lx, gzz = z0 - H + lz;
     T v = 0;
-    if (gx < nx && gzz < nz) v = curr[(long long)gx * nz + gzz];
+    if (gx < nx && gzz < nz) v = curr[(long long)gx * pitch + gzz];
     sc[i] = v;
   }
   __syncthreads();
@@ -239,7 +240,7 @@ fd_step_tile(StepArgs a) {
       float delta = 0.0f;
       if constexpr (DAMPED) delta = damp_delta(gx, gz, nx, nz, a.bx0);
       T c = sc[(lx + H) * CZ + (tz + H)];
-      prev[(long long)gx * nz + gz] =
+      prev[(long long)gx * pitch + gz] =
           update_point<ARITH, UZ, T>(c, pv[k], r, &su[(lx + 1) * UZ + (tz + 1)], delta);
     }
   }

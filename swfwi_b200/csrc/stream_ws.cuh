@@ -1,0 +1,267 @@
+// Warp-specialised streaming step for sm_100a (same scheme, arithmetics and
+// layout as stream.cuh).
+//
+// CTA = NW consumer warps + 1 producer warp.  The producer's lane 0 walks
+// the chunk's rows and issues TMA bulk copies into the rings, throttled by
+// "empty" mbarriers the consumers release; the consumers wait on "full"
+// mbarriers and never touch the copy engine:
+//   current-field ring: 16 rows; stage k (row xa-6+k) lands in slot k & 15,
+//     is read by u2 at steps k..k+10 and released after step k+10;
+//   prev / velocity ring: D+1 rows; stage k >= 12 (row xa-12+k) is read by
+//     the output at step k and released after step k+1.
+// The consumers of one CTA share every staged row: with 3 consumer warps a
+// band is 376 deep.  Warm-up rows (no output yet) are peeled out of the main
+// loop, and rows and depths outside the sponge take an undamped fast path.
+// Every wait is bounded; on timeout the CTA raises the error flag and the
+// producer stops issuing.
+#pragma once
+#include "stream.cuh"
+
+namespace swfwi {
+
+namespace ws_detail {
+using namespace stream_detail;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <int NT>
+__device__ __forceinline__ void consumer_sync() {
+  if constexpr (NT == 32) __syncwarp();
+  else asm volatile("bar.sync 1, %0;" ::"r"(NT) : "memory");
+}
+
+template <int NT, int NP>
+struct Smem {
+  static constexpr int BZ = 4 * NT - 8, WC = BZ + 24, WP = BZ + 8, NC = 16;
+  static constexpr size_t c_off = 0;
+  static constexpr size_t p_off = c_off + sizeof(float) * NC * WC;
+  static constexpr size_t v_off = p_off + sizeof(float) * NP * WP;
+  static constexpr size_t u_off = v_off + sizeof(float) * NP * WP;
+  static constexpr size_t b_off = u_off + sizeof(float) * 4 * 4 * NT;
+  static constexpr size_t bytes = b_off + sizeof(uint64_t) * (2 * NC + NP) + 16;
+};
+
+}  // namespace ws_detail
+
+template <int NW, int D>
+constexpr size_t ws_smem_bytes() {
+  return ws_detail::Smem<NW * 32, D + 1>::bytes;
+}
+
+template <int ARITH, bool DAMPED, int NW, int D>
+__global__ void __launch_bounds__((NW + 1) * 32)
+fd_step_ws(StreamArgs a) {
+  using namespace ws_detail;
+  constexpr int NT = NW * 32;      // consumer threads
+  constexpr int NP = D + 1;
+  using L = Smem<NT, NP>;
+  constexpr int BZ = L::BZ, WC = L::WC, WP = L::WP, NC = L::NC;
+  extern __shared__ __align__(128) unsigned char smem[];
+  float(*cring)[WC] = reinterpret_cast<float(*)[WC]>(smem + L::c_off);
+  float(*pring)[WP] = reinterpret_cast<float(*)[WP]>(smem + L::p_off);
+  float(*vring)[WP] = reinterpret_cast<float(*)[WP]>(smem + L::v_off);
+  float(*u2r)[4 * NT] = reinterpret_cast<float(*)[4 * NT]>(smem + L::u_off);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::b_off);
+  uint64_t *emptyc = full + NC;
+  uint64_t *emptyp = emptyc + NC;
+  int *s_fail = reinterpret_cast<int *>(emptyp + NP);
+
+  const int tid = threadIdx.x;
+  const int shot = a.shot_major ? blockIdx.z : blockIdx.x;
+  const int band = a.shot_major ? blockIdx.x : blockIdx.y;
+  const int chunk = a.shot_major ? blockIdx.y : blockIdx.z;
+  const int nx = a.nx, nz = a.nz, P = a.pitch;
+  const int z0 = 4 + band * BZ;
+  const int xa = 6 + chunk * a.xchunk;
+  const int xb = min(xa + a.xchunk, nx - 6);
+  if (xa >= xb) return;
+  const int K = xb - xa + 12;
+
+  if (tid == 0) {
+    for (int i = 0; i < NC; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&emptyc[i], 1);
+    }
+    for (int i = 0; i < NP; i++) mbar_init(&emptyp[i], 1);
+    fence_mbar_init();
+    *s_fail = 0;
+  }
+  __syncthreads();
+
+  // ---------------------------------------------------------------- producer
+  if (tid >= NT) {
+    if (tid != NT) return;
+    const int cz = z0 - 12, pz = z0 - 4;
+    const int clen = min(WC, P - kStreamCoff - cz), plen = min(WP, P - kStreamCoff - pz);
+    const uint32_t cbytes = (uint32_t)clen * 4u, pbytes = (uint32_t)plen * 4u;
+    const float *curr = a.curr + (long long)shot * a.shot_stride + cz;
+    const float *prevw = a.prev + (long long)shot * a.shot_stride + pz;
+    const float *rcpw = a.rcp + (long long)(shot / a.shots_per_vel) * a.vel_stride + pz;
+    for (int k = 0; k < K; k++) {
+      if (*(volatile int *)s_fail) break;
+      if (k >= NC && !mbar_wait(&emptyc[k & (NC - 1)], (uint32_t)(((k >> 4) + 1) & 1))) {
+        atomicExch(a.err, 1);
+        *(volatile int *)s_fail = 1;
+        break;
+      }
+      const bool pv = k >= 12;
+      const int ps = pv ? (k - 12) % NP : 0;
+      if (pv && k - 12 >= NP &&
+          !mbar_wait(&emptyp[ps], (uint32_t)(((k - 12) / NP + 1) & 1))) {
+        atomicExch(a.err, 1);
+        *(volatile int *)s_fail = 1;
+        break;
+      }
+      uint64_t *fb = &full[k & (NC - 1)];
+      mbar_expect_tx(fb, cbytes + (pv ? 2u * pbytes : 0u));
+      bulk_g2s(&cring[k & (NC - 1)][0], curr + (long long)(xa - 6 + k) * P, cbytes, fb);
+      if (pv) {
+        long long off = (long long)(xa - 12 + k) * P;
+        bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
+        bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
+      }
+    }
+    return;
+  }
+
+  // ---------------------------------------------------------------- consumers
+  const int t = tid;
+  const int zg = z0 - 4 + 4 * t;
+  float *prev = a.prev + (long long)shot * a.shot_stride;
+  float dz[4] = {-1.f, -1.f, -1.f, -1.f};
+  bool zok[4];
+  bool coldamp = false;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    int z = zg + i;
+    zok[i] = z >= 6 && z < nz - 6;
+    if constexpr (DAMPED) {
+      dz[i] = (z >= 0 && z < nz) ? a.damp_z[z] : -1.f;
+      coldamp = coldamp || dz[i] >= 0.f;
+    }
+  }
+  const bool outgroup = t >= 1 && t < NT - 1 && zg < nz - 6 && zg + 3 >= 6;
+  const bool fullgroup = zok[0] && zok[1] && zok[2] && zok[3];
+
+  auto wait_full = [&](int k) -> bool {
+    if (mbar_wait(&full[k & (NC - 1)], (uint32_t)((k >> 4) & 1))) return true;
+    atomicExch(a.err, 1);
+    *(volatile int *)s_fail = 1;
+    return false;
+  };
+
+  // u2 of row r = xa - 11 + k from stages k-10 .. k into u2r[k & 3]
+  auto do_u2 = [&](int k) {
+    const float *rowc = &cring[(k - 5) & (NC - 1)][0];
+    float zn[20];
+    {
+      float4 v0 = ld4(rowc + 4 * t), v1 = ld4(rowc + 4 * t + 4), v2 = ld4(rowc + 4 * t + 8),
+             v3 = ld4(rowc + 4 * t + 12), v4 = ld4(rowc + 4 * t + 16);
+      zn[0] = v0.x; zn[1] = v0.y; zn[2] = v0.z; zn[3] = v0.w;
+      zn[4] = v1.x; zn[5] = v1.y; zn[6] = v1.z; zn[7] = v1.w;
+      zn[8] = v2.x; zn[9] = v2.y; zn[10] = v2.z; zn[11] = v2.w;
+      zn[12] = v3.x; zn[13] = v3.y; zn[14] = v3.z; zn[15] = v3.w;
+      zn[16] = v4.x; zn[17] = v4.y; zn[18] = v4.z; zn[19] = v4.w;
+    }
+    float4 xm4[6], xp4[6];
+#pragma unroll
+    for (int d = 1; d <= 5; d++) {
+      xm4[d] = ld4(&cring[(k - 5 - d) & (NC - 1)][8 + 4 * t]);
+      xp4[d] = ld4(&cring[(k - 5 + d) & (NC - 1)][8 + 4 * t]);
+    }
+    float u[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      float xm[6], xp[6];
+#pragma unroll
+      for (int d = 1; d <= 5; d++) {
+        xm[d] = get(xm4[d], i);
+        xp[d] = get(xp4[d], i);
+      }
+      xm[0] = xp[0] = 0.f;
+      u[i] = lap_pt<ARITH>(zn, i, xm, xp);
+    }
+    st4(&u2r[k & 3][4 * t], make_float4(u[0], u[1], u[2], u[3]));
+  };
+
+  auto release = [&](int k) {
+    // after the consumer barrier of step k: stage k-10's current row and
+    // stage k-1's prev/vel rows have been read by every consumer
+    if (t == 0) {
+      if (k >= 10) mbar_arrive(&emptyc[(k - 10) & (NC - 1)]);
+      if (k - 1 >= 12) mbar_arrive(&emptyp[(k - 13) % NP]);
+    }
+  };
+
+  int k = 0;
+  // warm-up: stages 0..11, u2 from stage 10 on, no output yet
+  for (; k < 12 && k < K; k++) {
+    if (!wait_full(k)) break;
+    if (k >= 10) do_u2(k);
+    consumer_sync<NT>();
+    release(k);
+  }
+  if (!*(volatile int *)s_fail) {
+    for (; k < K; k++) {
+      if (!wait_full(k)) break;
+      do_u2(k);
+      consumer_sync<NT>();
+      if (*(volatile int *)s_fail) break;
+      release(k);
+      if (outgroup) {
+        const int j = xa - 12 + k;
+        const int ps = (k - 12) % NP;
+        const float *um = &u2r[(k - 2) & 3][4 * t];
+        const float *uc = &u2r[(k - 1) & 3][4 * t];
+        const float *up = &u2r[k & 3][4 * t];
+        float4 c4 = ld4(&cring[(k - 6) & (NC - 1)][8 + 4 * t]);
+        float4 p4 = ld4(&pring[ps][4 * t]);
+        float4 r4 = ld4(&vring[ps][4 * t]);
+        float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
+        float ucl = uc[-1], ucr = uc[4];
+        float o[4];
+        bool damp = false;
+        float dxr = 0.f;
+        if constexpr (DAMPED) {
+          dxr = a.damp_x[j];
+          damp = coldamp || dxr != 0.f;
+        }
+        if (!damp) {
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            float uzm = i == 0 ? ucl : get(uc4, i - 1);
+            float uzp = i == 3 ? ucr : get(uc4, i + 1);
+            o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
+                                    get(um4, i), get(up4, i), 0.0f);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            float dist = dz[i] >= 0.f ? dz[i] : dxr;
+            float delta = __fmul_rn(__fmul_rn(0.05f, dist), dist);
+            float uzm = i == 0 ? ucl : get(uc4, i - 1);
+            float uzp = i == 3 ? ucr : get(uc4, i + 1);
+            o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
+                                    get(um4, i), get(up4, i), delta);
+          }
+        }
+        float *dst = prev + (long long)j * P + zg;
+        if (fullgroup) {
+          st4(dst, make_float4(o[0], o[1], o[2], o[3]));
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+            if (zok[i]) dst[i] = o[i];
+        }
+      }
+    }
+  }
+  if (*(volatile int *)s_fail && t == 0) {
+    // wait (bounded) for copies the producer already issued
+    for (int i = k; i < K && i < k + NC; i++) mbar_wait(&full[i & (NC - 1)], (uint32_t)((i >> 4) & 1));
+  }
+}
+
+}  // namespace swfwi
