@@ -103,8 +103,8 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
 /* Launch shape of the propagator's stencil (results do not depend on it):
  * kernel 0 = streaming step (band depth 120 or 248 = one or two warps,
  * rows ahead 3 or 5), kernel 1 = warp-specialised streaming step (band
- * depth 120, 248 or 376 = 1-3 consumer warps plus a copy warp, rows ahead 2
- * or 4); rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot
+ * depth 120, 248 or 376 = 1-3 consumer warps plus a copy warp, rows ahead 3
+ * or 7); rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot
  * together. */
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest);

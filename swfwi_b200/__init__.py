@@ -317,8 +317,8 @@ class Damp4t10d:
         _check(lib().swfwi_damp4t10d_set_arith(self.h, arith))
         self.arith = arith
 
-    def set_tuning(self, kernel: int = 1, band_depth: int = 376, rows_per_cta: int = 128,
-                   rows_in_flight: int = 4, shots_slowest: bool = False):
+    def set_tuning(self, kernel: int = 1, band_depth: int = 376, rows_per_cta: int = 64,
+                   rows_in_flight: int = 3, shots_slowest: bool = False):
         """Launch shape of the stencil (results do not change)."""
         _check(lib().swfwi_damp4t10d_set_tuning(self.h, kernel, band_depth, rows_per_cta, rows_in_flight,
                                                 int(shots_slowest)))

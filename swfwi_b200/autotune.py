@@ -13,14 +13,14 @@ import itertools
 
 import numpy as np
 
-DEFAULT = {"kernel": 1, "band_depth": 376, "rows_per_cta": 128, "rows_in_flight": 4,
+DEFAULT = {"kernel": 1, "band_depth": 376, "rows_per_cta": 64, "rows_in_flight": 3,
            "shots_slowest": False}
 
 
 def candidates(nz: int):
     """Both kernels' band depths crossed with chunk lengths, prefetch depths
     and launch orders."""
-    for bz, rows, depth, order in itertools.product((120, 248, 376), (64, 128, 256), (2, 4), (False, True)):
+    for bz, rows, depth, order in itertools.product((120, 248, 376), (48, 64, 128), (3, 7), (False, True)):
         yield {"kernel": 1, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": order}
     for bz, rows in itertools.product((120, 248), (64, 128)):

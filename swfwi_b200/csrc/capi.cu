@@ -192,7 +192,7 @@ int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, i
     } else {
       SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,
                     "band depth must be 120, 248 or 376");
-      SWFWI_REQUIRE(rows_in_flight == 2 || rows_in_flight == 4, "rows in flight must be 2 or 4");
+      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
     }
     SWFWI_REQUIRE(rows_per_cta >= 1, "rows per CTA must be positive");
     P(h).stream_kernel = kernel;

@@ -72,8 +72,8 @@ class Propagator {
   int strip_format = SWFWI_STRIP_F32;
   int stream_kernel = 1;      // 0: streaming step, 1: warp-specialised streaming step
   int stream_bz = 376;        // output depths per CTA (120, 248; 376 warp-specialised only)
-  int stream_xchunk = 128;    // rows per CTA
-  int stream_depth = 4;       // rows ahead (3 or 5; warp-specialised 2 or 4)
+  int stream_xchunk = 64;     // rows per CTA
+  int stream_depth = 3;       // rows ahead (3 or 5; warp-specialised 3 or 7)
   int stream_shot_major = 0;  // launch order: 0 = shots fastest
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);

@@ -685,8 +685,8 @@ static void ws_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
 
 template <int ARITH, bool DAMPED>
 static void ws_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
-  if (depth >= 4) ws_nw<ARITH, DAMPED, 4>(bz, a, nslots, st);
-  else ws_nw<ARITH, DAMPED, 2>(bz, a, nslots, st);
+  if (depth >= 7) ws_nw<ARITH, DAMPED, 7>(bz, a, nslots, st);
+  else ws_nw<ARITH, DAMPED, 3>(bz, a, nslots, st);
 }
 
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,

@@ -60,7 +60,7 @@ void launch_step(int arith, bool damped, bool vel_is_rcp, int tx, const StepArgs
 void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamArgs &a,
                         int nslots, cudaStream_t st);
 // Warp-specialised streaming step (stream_ws.cuh): bz = 120, 248 or 376
-// output depths per CTA (1-3 consumer warps), depth = 2 or 4 rows ahead.
+// output depths per CTA (1-3 consumer warps), depth = 3 or 7 rows ahead.
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
                     cudaStream_t st);
 // Per-axis sponge ramps for the streaming step (see stream.cuh).

@@ -7,14 +7,17 @@
 // mbarriers and never touch the copy engine:
 //   current-field ring: 16 rows; stage k (row xa-6+k) lands in slot k & 15,
 //     is read by u2 at steps k..k+10 and released after step k+10;
-//   prev / velocity ring: D+1 rows; stage k >= 12 (row xa-12+k) is read by
-//     the output at step k and released after step k+1.
+//   prev / velocity ring: NP rows (a power of two); stage k >= 12 (row
+//     xa-12+k) lands in slot (k-12) & (NP-1), is read by the output at step
+//     k and released after step k+1.
 // The consumers of one CTA share every staged row: with 3 consumer warps a
-// band is 376 deep.  Warm-up rows (no output yet) are peeled out of the main
-// loop, and rows and depths outside the sponge take an undamped fast path.
-// Every wait is bounded; on timeout the CTA raises the error flag and the
-// producer stops issuing.
+// band is 376 deep.  Warm-up rows (no output yet) are peeled off; the main
+// loop is unrolled by the ring length from a fixed phase (step 12), so every
+// ring slot, barrier and u2-row index is a compile-time constant; rows and
+// depths outside the sponge take an undamped fast path.  Every wait is
+// bounded; on timeout the CTA raises the error flag and the producer stops.
 #pragma once
+#include <utility>
 #include "stream.cuh"
 
 namespace swfwi {
@@ -32,6 +35,11 @@ __device__ __forceinline__ void consumer_sync() {
   else asm volatile("bar.sync 1, %0;" ::"r"(NT) : "memory");
 }
 
+template <typename F, int... I>
+__device__ __forceinline__ void static_for(F &&f, std::integer_sequence<int, I...>) {
+  (f(std::integral_constant<int, I>{}), ...);
+}
+
 template <int NT, int NP>
 struct Smem {
   static constexpr int BZ = 4 * NT - 8, WC = BZ + 24, WP = BZ + 8, NC = 16;
@@ -45,6 +53,7 @@ struct Smem {
 
 }  // namespace ws_detail
 
+// D rows ahead: the prev/velocity ring has D + 1 slots (D = 3 or 7).
 template <int NW, int D>
 constexpr size_t ws_smem_bytes() {
   return ws_detail::Smem<NW * 32, D + 1>::bytes;
@@ -56,6 +65,7 @@ fd_step_ws(StreamArgs a) {
   using namespace ws_detail;
   constexpr int NT = NW * 32;      // consumer threads
   constexpr int NP = D + 1;
+  static_assert(NP == 4 || NP == 8, "the prev/vel ring must divide the current ring");
   using L = Smem<NT, NP>;
   constexpr int BZ = L::BZ, WC = L::WC, WP = L::WP, NC = L::NC;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -107,9 +117,9 @@ fd_step_ws(StreamArgs a) {
         break;
       }
       const bool pv = k >= 12;
-      const int ps = pv ? (k - 12) % NP : 0;
+      const int ps = (k - 12) & (NP - 1);
       if (pv && k - 12 >= NP &&
-          !mbar_wait(&emptyp[ps], (uint32_t)(((k - 12) / NP + 1) & 1))) {
+          !mbar_wait(&emptyp[ps], (uint32_t)((((k - 12) / NP) + 1) & 1))) {
         atomicExch(a.err, 1);
         *(volatile int *)s_fail = 1;
         break;
@@ -129,7 +139,7 @@ fd_step_ws(StreamArgs a) {
   // ---------------------------------------------------------------- consumers
   const int t = tid;
   const int zg = z0 - 4 + 4 * t;
-  float *prev = a.prev + (long long)shot * a.shot_stride;
+  float *prevg = a.prev + (long long)shot * a.shot_stride + (long long)xa * P + zg;   // output row xa
   float dz[4] = {-1.f, -1.f, -1.f, -1.f};
   bool zok[4];
   bool coldamp = false;
@@ -144,121 +154,135 @@ fd_step_ws(StreamArgs a) {
   }
   const bool outgroup = t >= 1 && t < NT - 1 && zg < nz - 6 && zg + 3 >= 6;
   const bool fullgroup = zok[0] && zok[1] && zok[2] && zok[3];
+  const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
 
-  auto wait_full = [&](int k) -> bool {
-    if (mbar_wait(&full[k & (NC - 1)], (uint32_t)((k >> 4) & 1))) return true;
-    atomicExch(a.err, 1);
-    *(volatile int *)s_fail = 1;
-    return false;
-  };
-
-  // u2 of row r = xa - 11 + k from stages k-10 .. k into u2r[k & 3]
-  auto do_u2 = [&](int k) {
-    const float *rowc = &cring[(k - 5) & (NC - 1)][0];
-    float zn[20];
-    {
-      float4 v0 = ld4(rowc + 4 * t), v1 = ld4(rowc + 4 * t + 4), v2 = ld4(rowc + 4 * t + 8),
-             v3 = ld4(rowc + 4 * t + 12), v4 = ld4(rowc + 4 * t + 16);
-      zn[0] = v0.x; zn[1] = v0.y; zn[2] = v0.z; zn[3] = v0.w;
-      zn[4] = v1.x; zn[5] = v1.y; zn[6] = v1.z; zn[7] = v1.w;
-      zn[8] = v2.x; zn[9] = v2.y; zn[10] = v2.z; zn[11] = v2.w;
-      zn[12] = v3.x; zn[13] = v3.y; zn[14] = v3.z; zn[15] = v3.w;
-      zn[16] = v4.x; zn[17] = v4.y; zn[18] = v4.z; zn[19] = v4.w;
+  // One step.  PH is k & 15 when known at compile time, else -1.
+  auto step = [&](auto ph, int k) -> bool {
+    constexpr int PH = decltype(ph)::value;
+    auto cs = [&](int off) -> int {
+      if constexpr (PH >= 0) return (PH + off) & (NC - 1);
+      else return (k + off) & (NC - 1);
+    };
+    auto us = [&](int off) -> int {
+      if constexpr (PH >= 0) return (PH + off) & 3;
+      else return (k + off) & 3;
+    };
+    const int fs = cs(0);
+    if (!mbar_wait(&full[fs], (uint32_t)((k >> 4) & 1))) {
+      atomicExch(a.err, 1);
+      *(volatile int *)s_fail = 1;
+      return false;
     }
-    float4 xm4[6], xp4[6];
-#pragma unroll
-    for (int d = 1; d <= 5; d++) {
-      xm4[d] = ld4(&cring[(k - 5 - d) & (NC - 1)][8 + 4 * t]);
-      xp4[d] = ld4(&cring[(k - 5 + d) & (NC - 1)][8 + 4 * t]);
-    }
-    float u[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      float xm[6], xp[6];
+    const bool has_u2 = PH >= 0 || k >= 10;
+    const bool has_out = PH >= 0 || k >= 12;
+    if (has_u2) {
+      // u2 of row r = xa - 11 + k from stages k-10 .. k
+      const float *rowc = &cring[cs(-5)][0];
+      float zn[20];
+      {
+        float4 v0 = ld4(rowc + 4 * t), v1 = ld4(rowc + 4 * t + 4), v2 = ld4(rowc + 4 * t + 8),
+               v3 = ld4(rowc + 4 * t + 12), v4 = ld4(rowc + 4 * t + 16);
+        zn[0] = v0.x; zn[1] = v0.y; zn[2] = v0.z; zn[3] = v0.w;
+        zn[4] = v1.x; zn[5] = v1.y; zn[6] = v1.z; zn[7] = v1.w;
+        zn[8] = v2.x; zn[9] = v2.y; zn[10] = v2.z; zn[11] = v2.w;
+        zn[12] = v3.x; zn[13] = v3.y; zn[14] = v3.z; zn[15] = v3.w;
+        zn[16] = v4.x; zn[17] = v4.y; zn[18] = v4.z; zn[19] = v4.w;
+      }
+      float4 xm4[6], xp4[6];
 #pragma unroll
       for (int d = 1; d <= 5; d++) {
-        xm[d] = get(xm4[d], i);
-        xp[d] = get(xp4[d], i);
+        xm4[d] = ld4(&cring[cs(-5 - d)][8 + 4 * t]);
+        xp4[d] = ld4(&cring[cs(-5 + d)][8 + 4 * t]);
       }
-      xm[0] = xp[0] = 0.f;
-      u[i] = lap_pt<ARITH>(zn, i, xm, xp);
+      float u[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        float xm[6], xp[6];
+#pragma unroll
+        for (int d = 1; d <= 5; d++) {
+          xm[d] = get(xm4[d], i);
+          xp[d] = get(xp4[d], i);
+        }
+        xm[0] = xp[0] = 0.f;
+        u[i] = lap_pt<ARITH>(zn, i, xm, xp);
+      }
+      st4(&u2r[us(0)][4 * t], make_float4(u[0], u[1], u[2], u[3]));
     }
-    st4(&u2r[k & 3][4 * t], make_float4(u[0], u[1], u[2], u[3]));
-  };
-
-  auto release = [&](int k) {
-    // after the consumer barrier of step k: stage k-10's current row and
-    // stage k-1's prev/vel rows have been read by every consumer
+    consumer_sync<NT>();
+    if (*(volatile int *)s_fail) return false;
+    // release stage k-10's current row and stage k-1's prev/vel rows
     if (t == 0) {
-      if (k >= 10) mbar_arrive(&emptyc[(k - 10) & (NC - 1)]);
-      if (k - 1 >= 12) mbar_arrive(&emptyp[(k - 13) % NP]);
+      if (has_u2) mbar_arrive(&emptyc[cs(-10)]);
+      // (stage 11 carries no prev/vel rows: the first release is at step 13)
+      if (k >= 13) {
+        if constexpr (PH >= 0) mbar_arrive(&emptyp[(PH - 13) & (NP - 1)]);
+        else mbar_arrive(&emptyp[(k - 13) & (NP - 1)]);
+      }
     }
+    if (has_out && outgroup) {
+      const int ps = (PH >= 0) ? ((PH - 12) & (NP - 1)) : ((k - 12) & (NP - 1));
+      const float *um = &u2r[us(-2)][4 * t];
+      const float *uc = &u2r[us(-1)][4 * t];
+      const float *up = &u2r[us(0)][4 * t];
+      float4 c4 = ld4(&cring[cs(-6)][8 + 4 * t]);
+      float4 p4 = ld4(&pring[ps][4 * t]);
+      float4 r4 = ld4(&vring[ps][4 * t]);
+      float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
+      float ucl = uc[-1], ucr = uc[4];
+      float o[4];
+      bool damp = false;
+      float dxr = 0.f;
+      if constexpr (DAMPED) {
+        dxr = damp_row[k];
+        damp = coldamp || dxr != 0.f;
+      }
+      if (!damp) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          float uzm = i == 0 ? ucl : get(uc4, i - 1);
+          float uzp = i == 3 ? ucr : get(uc4, i + 1);
+          o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
+                                  get(um4, i), get(up4, i), 0.0f);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          float dist = dz[i] >= 0.f ? dz[i] : dxr;
+          float delta = __fmul_rn(__fmul_rn(0.05f, dist), dist);
+          float uzm = i == 0 ? ucl : get(uc4, i - 1);
+          float uzp = i == 3 ? ucr : get(uc4, i + 1);
+          o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
+                                  get(um4, i), get(up4, i), delta);
+        }
+      }
+      float *dst = prevg + (long long)(k - 12) * P;
+      if (fullgroup) {
+        st4(dst, make_float4(o[0], o[1], o[2], o[3]));
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          if (zok[i]) dst[i] = o[i];
+      }
+    }
+    return true;
   };
 
   int k = 0;
-  // warm-up: stages 0..11, u2 from stage 10 on, no output yet
-  for (; k < 12 && k < K; k++) {
-    if (!wait_full(k)) break;
-    if (k >= 10) do_u2(k);
-    consumer_sync<NT>();
-    release(k);
+  bool ok = true;
+  // warm-up: stages 0..11 (u2 from stage 10 on, no output yet)
+  for (; ok && k < 12 && k < K; k++) ok = step(std::integral_constant<int, -1>{}, k);
+  // main loop: from step 12 in blocks of 16, every ring index is a constant
+  for (; ok && k + 16 <= K; k += 16) {
+    static_for(
+        [&](auto u) {
+          constexpr int U = decltype(u)::value;
+          if (ok) ok = step(std::integral_constant<int, (12 + U) & 15>{}, k + U);
+        },
+        std::make_integer_sequence<int, 16>{});
   }
-  if (!*(volatile int *)s_fail) {
-    for (; k < K; k++) {
-      if (!wait_full(k)) break;
-      do_u2(k);
-      consumer_sync<NT>();
-      if (*(volatile int *)s_fail) break;
-      release(k);
-      if (outgroup) {
-        const int j = xa - 12 + k;
-        const int ps = (k - 12) % NP;
-        const float *um = &u2r[(k - 2) & 3][4 * t];
-        const float *uc = &u2r[(k - 1) & 3][4 * t];
-        const float *up = &u2r[k & 3][4 * t];
-        float4 c4 = ld4(&cring[(k - 6) & (NC - 1)][8 + 4 * t]);
-        float4 p4 = ld4(&pring[ps][4 * t]);
-        float4 r4 = ld4(&vring[ps][4 * t]);
-        float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
-        float ucl = uc[-1], ucr = uc[4];
-        float o[4];
-        bool damp = false;
-        float dxr = 0.f;
-        if constexpr (DAMPED) {
-          dxr = a.damp_x[j];
-          damp = coldamp || dxr != 0.f;
-        }
-        if (!damp) {
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            float uzm = i == 0 ? ucl : get(uc4, i - 1);
-            float uzp = i == 3 ? ucr : get(uc4, i + 1);
-            o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
-                                    get(um4, i), get(up4, i), 0.0f);
-          }
-        } else {
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            float dist = dz[i] >= 0.f ? dz[i] : dxr;
-            float delta = __fmul_rn(__fmul_rn(0.05f, dist), dist);
-            float uzm = i == 0 ? ucl : get(uc4, i - 1);
-            float uzp = i == 3 ? ucr : get(uc4, i + 1);
-            o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
-                                    get(um4, i), get(up4, i), delta);
-          }
-        }
-        float *dst = prev + (long long)j * P + zg;
-        if (fullgroup) {
-          st4(dst, make_float4(o[0], o[1], o[2], o[3]));
-        } else {
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-            if (zok[i]) dst[i] = o[i];
-        }
-      }
-    }
-  }
-  if (*(volatile int *)s_fail && t == 0) {
+  for (; ok && k < K; k++) ok = step(std::integral_constant<int, -1>{}, k);
+
+  if (!ok && t == 0) {
     // wait (bounded) for copies the producer already issued
     for (int i = k; i < K && i < k + NC; i++) mbar_wait(&full[i & (NC - 1)], (uint32_t)((i >> 4) & 1));
   }

@@ -175,7 +175,8 @@ def test_errors_reported(cuda):
 
 @pytest.mark.parametrize("kern,bz,rows,depth,order", [
     (0, 120, 1, 3, 1), (0, 248, 7, 5, 0), (0, 120, 64, 5, 0),
-    (1, 120, 1, 2, 1), (1, 248, 9, 4, 0), (1, 376, 64, 4, 0), (1, 376, 3, 2, 1), (1, 120, 200, 4, 0)])
+    (1, 120, 1, 3, 1), (1, 248, 9, 7, 0), (1, 376, 64, 7, 0), (1, 376, 3, 3, 1), (1, 120, 200, 7, 0),
+    (1, 376, 16, 3, 0), (1, 248, 33, 3, 1)])
 def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     # every band depth / chunk length of the streaming stencil gives the
     # reference's seismogram bit for bit
@@ -187,7 +188,8 @@ def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     np.testing.assert_array_equal(d.cpu().numpy(), g["dcal"][2])
 
 
-@pytest.mark.parametrize("kern,bz,depth", [(0, 120, 5), (0, 248, 3), (1, 120, 4), (1, 248, 2), (1, 376, 4)])
+@pytest.mark.parametrize("kern,bz,depth", [(0, 120, 5), (0, 248, 3), (1, 120, 7), (1, 248, 3), (1, 376, 3),
+                                           (1, 376, 7)])
 def test_stream_matches_reference_large_grid(cuda, ref, kern, bz, depth):
     # 921 x 301 (993 x 343 padded, pitch 344): several bands, a short last
     # band, many chunks
