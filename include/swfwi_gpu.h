@@ -216,6 +216,17 @@ int swfwi_update_vel(float *new_vel, const float *vel, const float *grad, int n,
 int swfwi_trans_vsrc(float *out, const float *in, int nt, int ng, void *stream);
 /* sum of squares of n floats in FP64 (cal_objective, common.cpp:231-241). */
 int swfwi_cal_objective(const float *r, long long n, double *obj, void *stream);
+/* The sum of squares above for nslots consecutive arrays of n_per_slot
+ * floats, written to obj[0..nslots) (DEVICE), without allocating: no
+ * counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (allocation forbidden inside their callbacks or owned by their own
+ * allocator).  Scratch is a static device array of 32 slots x 256 FP64
+ * partials (64 KB, held by every GPU that loads the library); nslots > 32
+ * is rejected.  The first call on a device looks up that array's address
+ * and should come before any stream capture; calls that overlap on the GPU
+ * race on the array.  Same results as swfwi_cal_objective per slot. */
+int swfwi_cal_objective_static(const float *r, long long n_per_slot, int nslots, double *obj,
+                               void *stream);
 /* parabolaVertex (parabola-vertex.cpp:12-33), host. */
 int swfwi_parabola_vertex(float x1, float y1, float x2, float y2, float x3, float y3,
                           float max_alpha3, float *xv, float *yv);

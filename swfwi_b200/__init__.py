@@ -93,6 +93,7 @@ _SIGS = {
                          C.c_float, _vp],
     "swfwi_trans_vsrc": [_vp, _vp, C.c_int, C.c_int, _vp],
     "swfwi_cal_objective": [_vp, C.c_longlong, _dp, _vp],
+    "swfwi_cal_objective_static": [_vp, C.c_longlong, C.c_int, _vp, _vp],
     "swfwi_parabola_vertex": [C.c_float] * 7 + [_fp, _fp],
     "swfwi_ricker_wavelet": [_fp, C.c_int, C.c_float, C.c_float, C.c_float],
     "swfwi_random_codes": [C.c_int, C.c_int, C.c_int, _ip],
@@ -255,6 +256,13 @@ def cal_objective(r, stream=None) -> float:
     o = C.c_double()
     _check(lib().swfwi_cal_objective(_ptr(r), r.numel(), C.byref(o), _stream(stream)))
     return o.value
+
+
+def cal_objective_static(r, out, stream=None) -> None:
+    """Sums of squares of each row of r ([nslots][n] float32, CUDA) into out
+    ([nslots] float64, CUDA) without allocating device memory."""
+    nslots, n = r.shape
+    _check(lib().swfwi_cal_objective_static(_ptr(r), n, nslots, _ptr(out), _stream(stream)))
 
 
 # ---------------------------------------------------------------- propagator
