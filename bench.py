@@ -130,10 +130,12 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def setup_workload(torch, arith):
+def setup_workload(torch, arith, nt=0):
     import swfwi_b200 as S
     from swfwi_b200 import survey as sv
     s = sv.config(CONFIG)
+    if nt > 0:
+        s = s.scaled(nt=nt)
     vtrue = sv.layered_model(s.nx, s.nz, seed=2024)
     vinit = sv.smooth(vtrue, 15.0).astype(np.float32)
     m = S.Damp4t10d.from_survey(s, arith=arith)
@@ -238,7 +240,7 @@ def run_kernel_mode(args):
         return 0
     ss = s.scaled(nt=args.nt)
     m = S.Damp4t10d.from_survey(ss, arith=arith)
-    m.set_tuning(**autotune.DEFAULT)
+    m.set_tuning(**(json.loads(args.tuning) if args.tuning else autotune.DEFAULT))
     vel = torch.from_numpy(ex).cuda()
     m.bindVelocity(vel)
     wlt = torch.from_numpy(S.ricker_wavelet(ss.nt, ss.fm, ss.dt)).cuda()
@@ -265,6 +267,10 @@ def main():
                     help="kernel: short 96-shot batched forward (the small case for ncu); "
                          "tune: print the autotuner's table")
     ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")
+    ap.add_argument("--tuning", default="", help="stencil launch shape as JSON (skips the autotuner)")
+    ap.add_argument("--workload-nt", type=int, default=0,
+                    help="cut the time axis to this many steps (a short run for the ncu launch list; "
+                         "not the benchmark workload)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -282,11 +288,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     arith = S.ARITH_REF if args.arith == "ref" else S.ARITH_FAST
-    s, m, exi, exi_h, wlt, wlt_h, dobs, ids = setup_workload(torch, arith)
+    s, m, exi, exi_h, wlt, wlt_h, dobs, ids = setup_workload(torch, arith, args.workload_nt)
     nxpad, nzpad, ns, ngmax, nt = m.dims()
     from swfwi_b200 import autotune
     tuning = dict(autotune.DEFAULT)
-    if not args.no_tune:
+    if args.tuning:
+        tuning = json.loads(args.tuning)
+    elif not args.no_tune:
         tuning, _ = autotune.tune(s, exi_h, arith)
     m.set_tuning(**tuning)
     grad = torch.zeros((nxpad, nzpad), dtype=torch.float32, device="cuda")
@@ -308,12 +316,14 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    torch.cuda.profiler.start()       # ncu --profile-from-start off sees the timed steps only
     ev0.record(stream)
     objs = None
     for _ in range(args.steps):
         objs = m.gradient_batch(wlt, dobs, ids, grad)
     ev1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     barrier()
     clocks = clk.stop()
     ms = ev0.elapsed_time(ev1)
@@ -335,7 +345,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                 "frac": step_gbs / peak, "peak_basis": peak_kind,
                 "traffic": (tpp * per_launch_pts) if tpp else None,
-                "kernel": "fd_step_tile", "launches": st["step_launches"],
+                "kernel": {0: "fd_step_stream", 1: "fd_step_ws", 2: "fd_step_wi"}.get(tuning.get("kernel", 1)),
+                "launches": st["step_launches"],
                 "avg_launch_us": st["step_ms"] * 1e3 / max(st["step_launches"], 1),
                 "bytes_per_launch": st["step_bytes"] / max(st["step_launches"], 1),
                 "stencil_share_of_step": st["step_ms"] / ms if ms > 0 else None}
@@ -386,7 +397,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "batched FWI gradient, 96 shots, 301x921 grid (993x337 padded), "
-                                       "nt=4000, uneven spreads 200-921",
+                                       f"nt={nt}, uneven spreads 200-921"
+                                       + (" (REDUCED time axis: not the benchmark)" if args.workload_nt else ""),
                            "shots": int(ns), "nt": int(nt), "grid": [int(nxpad), int(nzpad)],
                            "arith": args.arith, "strips": "f32", "tuning": tuning,
                            "point_updates_per_step": updates_rank / args.steps,
