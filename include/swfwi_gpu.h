@@ -104,6 +104,8 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
  * kernel 0 = streaming step (band depth 120 or 248 = one or two warps,
  * rows ahead 3 or 5), kernel 1 = warp-specialised streaming step (band
  * depth 120, 248 or 376 = 1-3 consumer warps plus a copy warp, rows ahead 3
+ * or 7), kernel 2 = streaming step with independent consumer warps (band
+ * depth 240, 360 or 480 = 2-4 consumer warps plus a copy warp, rows ahead 3
  * or 7); rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot
  * together. */
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,

@@ -308,7 +308,8 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.xchunk = stream_xchunk;
   a.shot_major = stream_shot_major;
   a.err = d_err_.get();
-  if (stream_kernel == 1) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  if (stream_kernel == 2) launch_wi_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  else if (stream_kernel == 1) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   else launch_stream_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
 }

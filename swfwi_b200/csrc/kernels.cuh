@@ -63,6 +63,11 @@ void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamA
 // output depths per CTA (1-3 consumer warps), depth = 3 or 7 rows ahead.
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
                     cudaStream_t st);
+// Streaming step with independent consumer warps (stream_wi.cuh): bz = 240,
+// 360 or 480 output depths per CTA (2-4 consumer warps of 120), depth = 3
+// or 7 rows ahead.
+void launch_wi_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
+                    cudaStream_t st);
 // Per-axis sponge ramps for the streaming step (see stream.cuh).
 void launch_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb, cudaStream_t st);
 

@@ -28,11 +28,15 @@ def test_calgradient_ess_bit_exact(cuda):
     np.testing.assert_array_equal(gr.cpu().numpy(), g["grad_ess"])
 
 
-def test_gradient_batch_matches_reference_loop(cuda):
+@pytest.mark.parametrize("tuning", [None, (1, 248, 7, 3, 1), (2, 360, 64, 3, 0), (2, 240, 5, 7, 1)])
+def test_gradient_batch_matches_reference_loop(cuda, tuning):
     # the per-shot loop of FwiFramework::epoch: gradient bit-exact, the
-    # objective summed in FP64 (the reference sums in float)
+    # objective summed in FP64 (the reference sums in float); with the
+    # default and other stencil launch shapes
     torch = cuda
     s, m, g, _ = small_method(torch)
+    if tuning is not None:
+        m.set_tuning(*tuning)
     gr = torch.zeros(g["grad_sum"].shape, device="cuda")
     obj = m.gradient_batch(t(torch, g["wlt"]), t(torch, g["dobs"]), [0, 1, 2], gr)
     np.testing.assert_array_equal(gr.cpu().numpy(), g["grad_sum"])

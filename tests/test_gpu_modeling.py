@@ -67,6 +67,21 @@ def test_fast_forward_within_tolerance(cuda, fdo):
     print(f"seismogram rel-L2 vs FP64: REF {rel_l2(g['dcal'][1], d64):.2e}  FAST {rel_l2(d.cpu().numpy(), d64):.2e}")
 
 
+@pytest.mark.parametrize("kern,bz,rows,depth", [(0, 248, 7, 5), (1, 376, 64, 3), (2, 360, 64, 3),
+                                                (2, 240, 9, 7)])
+def test_fast_forward_every_kernel_within_tolerance(cuda, kern, bz, rows, depth):
+    # FAST arithmetic in every stencil kernel: seismogram within 1e-5
+    # relative L2 of the reference's
+    import swfwi_b200 as S
+    torch = cuda
+    s, m, g, vel = small_method(torch, arith=S.ARITH_FAST)
+    m.set_tuning(kern, bz, rows, depth, 0)
+    d = torch.zeros((s.nt, s.ng), device="cuda")
+    m.FwiForwardModeling(t(torch, g["wlt"]), d, 1)
+    err = rel_l2(d.cpu().numpy(), g["dcal"][1])
+    assert err < 1e-5, err
+
+
 def test_remove_direct_arrival_exact(cuda):
     torch = cuda
     s, m, g, _ = small_method(torch)
@@ -176,7 +191,8 @@ def test_errors_reported(cuda):
 @pytest.mark.parametrize("kern,bz,rows,depth,order", [
     (0, 120, 1, 3, 1), (0, 248, 7, 5, 0), (0, 120, 64, 5, 0),
     (1, 120, 1, 3, 1), (1, 248, 9, 7, 0), (1, 376, 64, 7, 0), (1, 376, 3, 3, 1), (1, 120, 200, 7, 0),
-    (1, 376, 16, 3, 0), (1, 248, 33, 3, 1)])
+    (1, 376, 16, 3, 0), (1, 248, 33, 3, 1),
+    (2, 240, 1, 3, 1), (2, 360, 64, 7, 0), (2, 480, 9, 3, 0), (2, 240, 33, 7, 0), (2, 360, 16, 3, 1)])
 def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     # every band depth / chunk length of the streaming stencil gives the
     # reference's seismogram bit for bit
@@ -189,7 +205,7 @@ def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
 
 
 @pytest.mark.parametrize("kern,bz,depth", [(0, 120, 5), (0, 248, 3), (1, 120, 7), (1, 248, 3), (1, 376, 3),
-                                           (1, 376, 7)])
+                                           (1, 376, 7), (2, 240, 3), (2, 360, 7), (2, 480, 3)])
 def test_stream_matches_reference_large_grid(cuda, ref, kern, bz, depth):
     # 921 x 301 (993 x 343 padded, pitch 344): several bands, a short last
     # band, many chunks
