@@ -268,6 +268,8 @@ def main():
                          "tune: print the autotuner's table")
     ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")
     ap.add_argument("--tuning", default="", help="stencil launch shape as JSON (skips the autotuner)")
+    ap.add_argument("--strips", default="f32", choices=["f32", "f16", "bf16"],
+                    help="storage of the boundary strips the gradient saves")
     ap.add_argument("--workload-nt", type=int, default=0,
                     help="cut the time axis to this many steps (a short run for the ncu launch list; "
                          "not the benchmark workload)")
@@ -297,6 +299,7 @@ def main():
     elif not args.no_tune:
         tuning, _ = autotune.tune(s, exi_h, arith)
     m.set_tuning(**tuning)
+    m.set_strip_format({"f32": S.STRIP_F32, "f16": S.STRIP_F16, "bf16": S.STRIP_BF16}[args.strips])
     grad = torch.zeros((nxpad, nzpad), dtype=torch.float32, device="cuda")
 
     for _ in range(max(args.warmup, 0)):
@@ -400,7 +403,7 @@ def main():
                                        f"nt={nt}, uneven spreads 200-921"
                                        + (" (REDUCED time axis: not the benchmark)" if args.workload_nt else ""),
                            "shots": int(ns), "nt": int(nt), "grid": [int(nxpad), int(nzpad)],
-                           "arith": args.arith, "strips": "f32", "tuning": tuning,
+                           "arith": args.arith, "strips": args.strips, "tuning": tuning,
                            "point_updates_per_step": updates_rank / args.steps,
                            "l2": "inputs larger than L2 (strips 14 GB, fields 0.5 GB): no flush",
                            "parallelism": f"replicas{world}",

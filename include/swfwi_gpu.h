@@ -99,6 +99,11 @@ int swfwi_damp4t10d_destroy(swfwi_damp4t10d *h);
  * legacy default stream. */
 int swfwi_damp4t10d_set_stream(swfwi_damp4t10d *h, void *stream);
 int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith);
+/* Storage of the boundary strips the batched gradients save in the forward
+ * sweep and restore in the backward one (SWFWI_STRIP_F32 = the reference's
+ * writeBndry/readBndry, bit-exact; F16/BF16 = half the memory, one
+ * power-of-two scale per shot and step).  The single-field
+ * write_bndry/read_bndry calls always use FP32. */
 int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
 /* Launch shape of the propagator's stencil (results do not depend on it):
  * kernel 0 = streaming step (band depth 120 or 248 = one or two warps,

@@ -325,6 +325,11 @@ class Damp4t10d:
         _check(lib().swfwi_damp4t10d_set_arith(self.h, arith))
         self.arith = arith
 
+    def set_strip_format(self, fmt: int):
+        """Boundary strips of the gradients: STRIP_F32 (exact), STRIP_F16 or
+        STRIP_BF16 (scaled 16-bit)."""
+        _check(lib().swfwi_damp4t10d_set_strip_format(self.h, fmt))
+
     def set_tuning(self, kernel: int = 1, band_depth: int = 376, rows_per_cta: int = 64,
                    rows_in_flight: int = 3, shots_slowest: bool = False):
         """Launch shape of the stencil (results do not change)."""

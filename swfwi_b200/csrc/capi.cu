@@ -177,7 +177,8 @@ int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith) {
 
 int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format) {
   return guarded([&] {
-    SWFWI_REQUIRE(format == SWFWI_STRIP_F32, "only FP32 strips are available");
+    SWFWI_REQUIRE(format == SWFWI_STRIP_F32 || format == SWFWI_STRIP_F16 || format == SWFWI_STRIP_BF16,
+                  "strip format must be SWFWI_STRIP_F32, _F16 or _BF16");
     P(h).strip_format = format;
   });
 }

@@ -431,7 +431,14 @@ void Propagator::ensure_work(Work<T> &w, int n, bool strips) {
   size_t f = (size_t)n * fstride;
   w.p0.resize(f);
   w.p1.resize(f);
-  if (strips) w.strips.resize((size_t)n * nt * bsize);
+  if (strips) {
+    if (sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32) {
+      w.qstrips.resize((size_t)n * nt * bsize);
+      w.qscale.resize((size_t)n * nt);
+    } else {
+      w.strips.resize((size_t)n * nt * bsize);
+    }
+  }
   w.partials.resize((size_t)n * kPartials);
   w.obj.resize(n);
 }
@@ -455,9 +462,15 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
     std::swap(p0, p1);
     if (dcal)
       launch_record<T>(dcal + (long long)it * ngrec, (long long)nt * ngrec, p0, fstride, n, rec, st_);
-    if (save_strips)
-      launch_strip_write<T>(w.strips.get() + (long long)it * bsize, bstride, p0, fstride, n, nxpad,
-                            nzpad, bx0, pitch, st_);
+    if (save_strips) {
+      if (sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32)
+        launch_strip_write_q(strip_format, w.qstrips.get() + (long long)it * bsize, bstride,
+                             w.qscale.get() + it, nt, reinterpret_cast<const float *>(p0), fstride, n,
+                             nxpad, nzpad, bx0, pitch, st_);
+      else
+        launch_strip_write<T>(w.strips.get() + (long long)it * bsize, bstride, p0, fstride, n, nxpad,
+                              nzpad, bx0, pitch, st_);
+    }
   }
   // leave the final (current, next) pair for a backward sweep
   if (p0 != w.p0.get() + kStreamCoff) std::swap(w.p0, w.p1);
@@ -480,8 +493,13 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   for (int it = nt - 1; it >= 0; it--) {
     // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
     // subSource; receiver addSource -> stepForward -> swap; image.
-    launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad,
-                         nzpad, bx0, pitch, st_);
+    if (sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32)
+      launch_strip_read_q(strip_format, w.qstrips.get() + (long long)it * bsize, bstride,
+                          w.qscale.get() + it, nt, reinterpret_cast<float *>(sp0), fstride, n, nxpad,
+                          nzpad, bx0, pitch, st_);
+    else
+      launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad,
+                           nzpad, bx0, pitch, st_);
     std::swap(sp0, sp1);
     step_fields(ar, false, sp0, sp1, velrcp, n);
     launch_inject<T>(sp0, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
@@ -530,12 +548,14 @@ int Propagator::max_batch() const {
   size_t freeb = 0, total = 0;
   if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) return 1;
   // per slot: p0, p1, g0, g1, image fields; strips; dcal, res, vsrc data
-  double per = 5.0 * fstride * 4 + (double)nt * bsize * 4 + 3.0 * nt * ngmax * 4 + 4096;
+  const double strip_bytes = strip_format == SWFWI_STRIP_F32 ? 4.0 : 2.0;
+  double per = 5.0 * fstride * 4 + (double)nt * bsize * strip_bytes + 3.0 * nt * ngmax * 4 + 4096;
   double budget = 0.85 * (double)freeb;
   // memory already held by this propagator's work space counts as free
   budget += (double)(w_.p0.capacity() + w_.p1.capacity() + w_.g0.capacity() + w_.g1.capacity() +
                      w_.image.capacity() + w_.strips.capacity() + w_.dcal.capacity() +
-                     w_.res.capacity() + w_.vsrc.capacity()) * 4;
+                     w_.res.capacity() + w_.vsrc.capacity()) * 4 +
+            (double)w_.qstrips.capacity() * 2;
   int m = (int)(budget / per);
   return std::max(1, std::min(m, ns));
 }

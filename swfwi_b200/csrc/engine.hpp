@@ -46,6 +46,8 @@ struct Line {
 template <typename T>
 struct Work {
   DevBuf<T> p0, p1, g0, g1, image, strips;
+  DevBuf<uint16_t> qstrips;   // 16-bit strips [slot][nt][bsize] (FP32 fields, F16/BF16 format)
+  DevBuf<float> qscale;       // their scales [slot][nt]
   DevBuf<float> dcal, res, vsrc;   // [slot][nt][ngmax]
   DevBuf<int> win, win2, slot_shot, slot_row;
   DevBuf<double> partials, obj;

@@ -1,7 +1,10 @@
 // Kernels around the stencil; see kernels.cuh for the reference citations.
 #include <atomic>
 #include <cmath>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include "kernels.cuh"
+#include "swfwi_gpu.h"
 
 namespace swfwi {
 
@@ -780,6 +783,84 @@ template void launch_record<float>(float *, long long, const float *, long long,
                                    cudaStream_t);
 template void launch_record<double>(double *, long long, const double *, long long, int, PointSet,
                                     cudaStream_t);
+// ---------------------------------------------------------------- 16-bit strips
+namespace {
+template <int FMT>
+__device__ __forceinline__ uint16_t q_encode(float v) {
+  if constexpr (FMT == SWFWI_STRIP_F16) return __half_as_ushort(__float2half_rn(v));
+  else return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+template <int FMT>
+__device__ __forceinline__ float q_decode(uint16_t h) {
+  if constexpr (FMT == SWFWI_STRIP_F16) return __half2float(__ushort_as_half(h));
+  else return __bfloat162float(__ushort_as_bfloat16(h));
+}
+
+// One CTA per slot: the step's largest |value|, its power-of-two scale,
+// then the scaled 16-bit values.
+template <int FMT>
+__global__ void __launch_bounds__(1024)
+k_strip_write_q(uint16_t *q, long long q_slot_stride, float *scale, long long scale_slot_stride,
+                const float *field, long long shot_stride, int bs, int nx, int nz, int bx0, int pitch) {
+  __shared__ float wmax[32];
+  const int slot = blockIdx.x;
+  const float *f = field + (long long)slot * shot_stride;
+  float m = 0.f;
+  for (int i = threadIdx.x; i < bs; i += blockDim.x)
+    m = fmaxf(m, fabsf(f[strip_index(i, nx, nz, bx0, pitch)]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  m = 0.f;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wmax[w]);
+  int e = 0;
+  if (m > 0.f && m <= 3.0e38f) frexpf(m, &e);   // m < 2^e
+  const float s = ldexpf(1.0f, e - 14), inv = ldexpf(1.0f, 14 - e);
+  if (threadIdx.x == 0) scale[(long long)slot * scale_slot_stride] = s;
+  uint16_t *qs = q + (long long)slot * q_slot_stride;
+  for (int i = threadIdx.x; i < bs; i += blockDim.x)
+    qs[i] = q_encode<FMT>(f[strip_index(i, nx, nz, bx0, pitch)] * inv);
+}
+
+template <int FMT>
+__global__ void k_strip_read_q(const uint16_t *q, long long q_slot_stride, const float *scale,
+                               long long scale_slot_stride, float *field, long long shot_stride, int bs,
+                               int nx, int nz, int bx0, int pitch) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, slot = blockIdx.y;
+  if (i >= bs) return;
+  const float s = scale[(long long)slot * scale_slot_stride];
+  field[(long long)slot * shot_stride + strip_index(i, nx, nz, bx0, pitch)] =
+      q_decode<FMT>(q[(long long)slot * q_slot_stride + i]) * s;
+}
+}  // namespace
+
+void launch_strip_write_q(int format, uint16_t *q, long long q_slot_stride, float *scale,
+                          long long scale_slot_stride, const float *field, long long shot_stride,
+                          int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st) {
+  int bs = strip_size(nx, nz, bx0);
+  if (format == SWFWI_STRIP_F16)
+    k_strip_write_q<SWFWI_STRIP_F16><<<nslots, 1024, 0, st>>>(q, q_slot_stride, scale, scale_slot_stride,
+                                                              field, shot_stride, bs, nx, nz, bx0, pitch);
+  else
+    k_strip_write_q<SWFWI_STRIP_BF16><<<nslots, 1024, 0, st>>>(q, q_slot_stride, scale, scale_slot_stride,
+                                                               field, shot_stride, bs, nx, nz, bx0, pitch);
+  note_launch();
+}
+
+void launch_strip_read_q(int format, const uint16_t *q, long long q_slot_stride, const float *scale,
+                         long long scale_slot_stride, float *field, long long shot_stride, int nslots,
+                         int nx, int nz, int bx0, int pitch, cudaStream_t st) {
+  int bs = strip_size(nx, nz, bx0);
+  dim3 g(grid_for(bs), nslots);
+  if (format == SWFWI_STRIP_F16)
+    k_strip_read_q<SWFWI_STRIP_F16><<<g, kThreads, 0, st>>>(q, q_slot_stride, scale, scale_slot_stride,
+                                                            field, shot_stride, bs, nx, nz, bx0, pitch);
+  else
+    k_strip_read_q<SWFWI_STRIP_BF16><<<g, kThreads, 0, st>>>(q, q_slot_stride, scale, scale_slot_stride,
+                                                             field, shot_stride, bs, nx, nz, bx0, pitch);
+  note_launch();
+}
+
 template void launch_strip_write<float>(float *, long long, const float *, long long, int, int, int,
                                         int, int, cudaStream_t);
 template void launch_strip_write<double>(double *, long long, const double *, long long, int, int,

@@ -45,6 +45,16 @@ void launch_strip_write(T *bndr, long long bndr_slot_stride, const T *field, lon
 template <typename T>
 void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long long shot_stride,
                        int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st);
+// The same strips stored as 16-bit values (format SWFWI_STRIP_F16 or
+// SWFWI_STRIP_BF16) with one power-of-two scale per slot and step: value =
+// decode(q) * scale, scale chosen so the step's largest |value| / scale is
+// below 2^14.  q layout as bndr; scale[slot * scale_slot_stride].
+void launch_strip_write_q(int format, uint16_t *q, long long q_slot_stride, float *scale,
+                          long long scale_slot_stride, const float *field, long long shot_stride,
+                          int nslots, int nx, int nz, int bx0, int pitch, cudaStream_t st);
+void launch_strip_read_q(int format, const uint16_t *q, long long q_slot_stride, const float *scale,
+                         long long scale_slot_stride, float *field, long long shot_stride, int nslots,
+                         int nx, int nz, int bx0, int pitch, cudaStream_t st);
 
 // image[slot] -= s[slot] * r[slot] * scale  (cross_correlation,
 // fwiframework.cpp:107-112)

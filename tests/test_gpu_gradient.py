@@ -74,6 +74,43 @@ def test_fast_gradient_within_tolerance_and_f64(cuda, fdo):
     print(f"gradient rel-L2 vs FP64: REF {rel_l2(g['grad_shot1'], g64):.2e}  FAST {rel_l2(fast, g64):.2e}")
 
 
+@pytest.mark.parametrize("fmt,bound", [(1, 2e-3), (2, 2e-2)])
+def test_16bit_strips_gradient_error_vs_f64(cuda, fmt, bound):
+    # scaled FP16 / BF16 boundary strips: the gradient's error against the
+    # FP64 run of the same scheme, beside the FP32-strip gradient's
+    import swfwi_b200 as S
+    torch = cuda
+    s, m, g, vel = small_method(torch)
+    g64 = torch.zeros(g["grad_shot1"].shape, dtype=torch.float64, device="cuda")
+    m.calgradient_fwi_f64(vel, t(torch, g["wlt"], torch.float64), t(torch, g["vsrc"], torch.float64), g64, 1)
+    g64 = g64.cpu().numpy()
+    m.set_strip_format(fmt)
+    gr = torch.zeros(g["grad_shot1"].shape, device="cuda")
+    m.calgradient_fwi(t(torch, g["wlt"]), t(torch, g["vsrc"]), gr, 1)
+    q = gr.cpu().numpy()
+    e32, eq = rel_l2(g["grad_shot1"], g64), rel_l2(q, g64)
+    print(f"gradient rel-L2 vs FP64: F32 strips {e32:.2e}  {('F16', 'BF16')[fmt - 1]} strips {eq:.2e}")
+    assert np.isfinite(q).all() and eq < bound, eq
+    # back to FP32 strips: bit-exact again
+    m.set_strip_format(S.STRIP_F32)
+    gr.zero_()
+    m.calgradient_fwi(t(torch, g["wlt"]), t(torch, g["vsrc"]), gr, 1)
+    np.testing.assert_array_equal(gr.cpu().numpy(), g["grad_shot1"])
+
+
+def test_16bit_strips_batched_gradient(cuda):
+    # the batched gradient loop with FP16 strips stays within the FP16
+    # bound of the exact (FP32-strip) result
+    import swfwi_b200 as S
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    m.set_strip_format(S.STRIP_F16)
+    gr = torch.zeros(g["grad_sum"].shape, device="cuda")
+    obj = m.gradient_batch(t(torch, g["wlt"]), t(torch, g["dobs"]), [0, 1, 2], gr)
+    assert rel_l2(gr.cpu().numpy(), g["grad_sum"]) < 2e-3
+    assert abs(obj.sum() - float(g["obj"])) / float(g["obj"]) < 1e-5
+
+
 def test_uneven_spreads_match_per_shot_reference(cuda, ref):
     # per-shot receiver spreads (not expressible in the reference's one
     # common line): each shot checked against a reference model built with
