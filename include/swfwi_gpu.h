@@ -165,6 +165,14 @@ int swfwi_damp4t10d_fwi_forward_modeling(swfwi_damp4t10d *h, const float *wlt, f
                                          int shot_id);
 /* EssForwardModeling (damp4t10d.cpp:291-307): encsrc [nt][ns]. */
 int swfwi_damp4t10d_ess_forward_modeling(swfwi_damp4t10d *h, const float *encsrc, float *dcal);
+/* The HA loop of EnkfAnalyze::calGainMatrix (enkfanalyze.cpp:207-236):
+ * EssForwardModeling of the encoded supershot (encsrc [nt][ns]) with each of
+ * n member velocities vels [n][nxpad*nzpad] (padded, transformed), run as
+ * one batch; hona [n][ng*nt] receives each seismogram transposed to the
+ * analysis matrix's column order (row ig*nt + it, matrix_transpose).  All
+ * device pointers. */
+int swfwi_damp4t10d_ess_forward_members(swfwi_damp4t10d *h, const float *encsrc, const float *vels,
+                                        int n, float *hona);
 
 /* ------------------------------------------------------------------------
  * Batched whole-shot operations (the fast path): nshots shots of
@@ -284,6 +292,48 @@ int swfwi_stats_reset(void);
 int swfwi_stats_enable_step_timing(int on);
 /* waits for the timed launches to finish */
 int swfwi_stats_read(swfwi_stats *out);
+
+/* Encoder::encodeSource (encoder.cpp:14-26): encsrc[it][is] = wlt[it] *
+ * codes[is]; codes are +-1 ints.  Device pointers. */
+int swfwi_encode_source(float *encsrc, const float *wlt, const int *codes, int nt, int ns, void *stream);
+/* Encoder::encodeObsData (encoder.cpp:28-42): encobs[j] = sum over shots in
+ * order of dobs[is][j] * codes[is] (float), j < n_per_shot = nt*ng.  Device. */
+int swfwi_encode_obs(float *encobs, const float *dobs, const int *codes, long long n_per_shot, int ns,
+                     void *stream);
+
+/* ------------------------------------------------------------------------
+ * Ensemble Kalman analysis (src/enfwi/enkfanalyze.cpp), FP64 on the GPU.
+ * n = 2..64 members; rows = nt*ng data samples in the reference's matrix
+ * order (row ig*nt + it); rows*n < 2^32.
+ * ---------------------------------------------------------------------- */
+/* EnkfAnalyze::calGainMatrix (enkfanalyze.cpp:185-341), serial form.
+ * hona [n][rows] DEVICE float: each member's modelled encoded data;
+ * dobs [rows] DEVICE float: the encoded observed data (every column of D);
+ * z [n][rows] DEVICE double: standard-normal draws, the observation
+ *   perturbation being sigma*z (the reference draws normal(0, sigma) from
+ *   Boost mt19937 seed 1); NULL draws them on the device (Philox4x32-10 with
+ *   `seed`, Box-Muller);
+ * sigma (host, in/out): <= 0 on the first call, then set to max|HA'| *
+ *   sigfac as initPerturbation does (enkfanalyze.cpp:621-635); pass it back
+ *   unchanged on later calls;
+ * t4 (host, out): the n x n gain HA'^T U SSqInv U^T (D - HA), column-major
+ *   (t4[col*n + row]) like the reference's Matrix;
+ * clip (host, out, optional): clipPosition of the singular values.
+ * The SVD is taken through the n x n cross product band^T band (cyclic
+ * Jacobi in double on the host); the three n x n products over the rows are
+ * one fused FP64 pass on the device.  Synchronises the stream. */
+int swfwi_enkf_gain_matrix(const float *hona, const float *dobs, const double *z, long long rows,
+                           int n, float sigfac, double *sigma, unsigned long long seed, double *t4,
+                           int *clip, void *stream);
+/* The update of EnkfAnalyze::analyze (enkfanalyze.cpp:57-111): vels [n]
+ * [model_size] DEVICE (padded, transformed members, updated in place):
+ * A' = members - their float mean, v_i <- velTrans(velRecover(v_i) +
+ * (A' t4)_i).  t4 host, column-major as returned above.  Synchronises. */
+int swfwi_enkf_update(float *vels, long long model_size, int n, const double *t4, float dx, float dt,
+                      void *stream);
+/* createAMean (enkfanalyze.cpp:568-580): mean [model_size] DEVICE = the
+ * members' float sum in member order / n. */
+int swfwi_enkf_mean(float *mean, const float *vels, long long model_size, int n, void *stream);
 
 #ifdef __cplusplus
 }

@@ -103,6 +103,8 @@ class RefLib:
             "ref_update_vel": [vp, _fp, _fp, _fp, C.c_float, C.c_float, C.c_float],
             "fd4t10s_damp_zjh_2d_vtrans": [_fp, _fp, _fp, _fp, C.c_int, C.c_int, C.c_int],
             "fd4t10s_zjh_2d_vtrans": [_fp, _fp, _fp, _fp, C.c_int, C.c_int],
+            "ref_clip_position": [_dp, C.c_int],
+            "ref_a_plus_b": [_dp, _dp, _dp, C.c_int],
         }
         for k, v in sig.items():
             getattr(L, k).argtypes = v
@@ -139,6 +141,18 @@ class RefLib:
         a = np.zeros(1, np.float32); b = np.zeros(1, np.float32)
         self.lib.ref_parabola_vertex(x1, y1, x2, y2, x3, y3, maxa3, fptr(a), fptr(b))
         return float(a[0]), float(b[0])
+
+    def clip_position(self, s) -> int:
+        """clipPosition (src/enfwi/Matrix.cpp:170-185), compiled."""
+        s = np.ascontiguousarray(s, np.float64)
+        return int(self.lib.ref_clip_position(s.ctypes.data_as(_dp), s.size))
+
+    def a_plus_b(self, a, b):
+        a = np.ascontiguousarray(a, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        c = np.zeros_like(a)
+        self.lib.ref_a_plus_b(a.ctypes.data_as(_dp), b.ctypes.data_as(_dp), c.ctypes.data_as(_dp), a.size)
+        return c
 
     def ricker(self, nt, fm, dt, amp=1.0):
         w = np.zeros(nt, np.float32)

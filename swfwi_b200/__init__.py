@@ -94,6 +94,13 @@ _SIGS = {
     "swfwi_trans_vsrc": [_vp, _vp, C.c_int, C.c_int, _vp],
     "swfwi_cal_objective": [_vp, C.c_longlong, _dp, _vp],
     "swfwi_cal_objective_static": [_vp, C.c_longlong, C.c_int, _vp, _vp],
+    "swfwi_encode_source": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_encode_obs": [_vp, _vp, _vp, C.c_longlong, C.c_int, _vp],
+    "swfwi_damp4t10d_ess_forward_members": [_vp, _vp, _vp, C.c_int, _vp],
+    "swfwi_enkf_gain_matrix": [_vp, _vp, _vp, C.c_longlong, C.c_int, C.c_float, _dp, C.c_ulonglong, _dp,
+                               _ip, _vp],
+    "swfwi_enkf_update": [_vp, C.c_longlong, C.c_int, _dp, C.c_float, C.c_float, _vp],
+    "swfwi_enkf_mean": [_vp, _vp, C.c_longlong, C.c_int, _vp],
     "swfwi_parabola_vertex": [C.c_float] * 7 + [_fp, _fp],
     "swfwi_ricker_wavelet": [_fp, C.c_int, C.c_float, C.c_float, C.c_float],
     "swfwi_random_codes": [C.c_int, C.c_int, C.c_int, _ip],
@@ -256,6 +263,90 @@ def cal_objective(r, stream=None) -> float:
     o = C.c_double()
     _check(lib().swfwi_cal_objective(_ptr(r), r.numel(), C.byref(o), _stream(stream)))
     return o.value
+
+
+def encode_source(encsrc, wlt, codes, stream=None) -> None:
+    """Encoder::encodeSource: encsrc [nt][ns] = wlt[it] * codes[is] (CUDA)."""
+    nt, ns = encsrc.shape
+    _check(lib().swfwi_encode_source(_ptr(encsrc), _ptr(wlt), _ptr(codes), nt, ns, _stream(stream)))
+
+
+def encode_obs(encobs, dobs, codes, stream=None) -> None:
+    """Encoder::encodeObsData: encobs [nt][ng] = sum_s codes[s] * dobs[s] (CUDA)."""
+    _check(lib().swfwi_encode_obs(_ptr(encobs), _ptr(dobs), _ptr(codes), encobs.numel(), dobs.shape[0],
+                                  _stream(stream)))
+
+
+def enkf_gain_matrix(hona, dobs, z=None, sigfac: float = 0.0, sigma: float = 0.0, seed: int = 1,
+                     stream=None):
+    """calGainMatrix on the device: hona [n][rows] float32, dobs [rows]
+    float32, z [n][rows] float64 or None (device draws).  Returns (t4 as
+    numpy [n][n] indexed [row, col], sigma, clip)."""
+    n, rows = hona.shape
+    t4 = np.zeros((n, n), np.float64)   # filled column-major: t4c[col][row]
+    sg = C.c_double(sigma)
+    clip = C.c_int(0)
+    _check(lib().swfwi_enkf_gain_matrix(_ptr(hona), _ptr(dobs), _ptr(z) if z is not None else None, rows, n,
+                                        sigfac, C.byref(sg), seed, t4.ctypes.data_as(_dp), C.byref(clip),
+                                        _stream(stream)))
+    return t4.T.copy(), sg.value, clip.value
+
+
+def enkf_update(vels, t4, dx: float, dt: float, stream=None) -> None:
+    """analyze's member update in place: vels [n][model] float32 CUDA; t4
+    numpy [n][n] indexed [row, col]."""
+    n = vels.shape[0]
+    t4c = np.ascontiguousarray(np.asarray(t4, np.float64).T)   # column-major for the C ABI
+    _check(lib().swfwi_enkf_update(_ptr(vels), vels.numel() // n, n, t4c.ctypes.data_as(_dp), dx, dt,
+                                   _stream(stream)))
+
+
+def enkf_mean(mean, vels, stream=None) -> None:
+    n = vels.shape[0]
+    _check(lib().swfwi_enkf_mean(_ptr(mean), _ptr(vels), vels.numel() // n, n, _stream(stream)))
+
+
+class EnkfAnalyze:
+    """EnkfAnalyze (src/enfwi/enkfanalyze.h): the ensemble Kalman analysis
+    of the encoded observed data, on the GPU.  fm: the propagator (geometry,
+    dt, dx); wlt [nt] and dobs [ns][nt][ng]: CUDA tensors; sigfac: the
+    perturbation factor.  sigma is fixed at the first analysis, as the
+    reference's initPerturbation does."""
+
+    def __init__(self, fm, wlt, dobs, sigfac: float):
+        self.fm, self.wlt, self.dobs, self.sigfac = fm, wlt, dobs, sigfac
+        self.sigma = 0.0
+        self.seed = 1
+
+    def calGainMatrix(self, vels, codes, z=None):
+        """vels [N][nxpad][nzpad] CUDA members; codes [ns] +-1 ints.  Returns
+        (t4 [N][N] numpy, clip)."""
+        import torch
+        nxpad, nzpad, ns, ng, nt = self.fm.dims()
+        c = torch.as_tensor(np.asarray(codes, np.int32), device=self.wlt.device)
+        encsrc = torch.empty((nt, ns), dtype=torch.float32, device=self.wlt.device)
+        encode_source(encsrc, self.wlt, c)
+        encobs = torch.empty((nt, ng), dtype=torch.float32, device=self.wlt.device)
+        encode_obs(encobs, self.dobs, c)
+        d = encobs.t().contiguous().reshape(-1)             # matrix_transpose: row ig*nt + it
+        n = vels.shape[0]
+        hona = torch.empty((n, ng * nt), dtype=torch.float32, device=self.wlt.device)
+        self.fm.ess_forward_members(encsrc, vels, hona)
+        t4, self.sigma, clip = enkf_gain_matrix(hona, d, z, self.sigfac, self.sigma, self.seed)
+        self.seed += 1
+        return t4, clip
+
+    def analyze(self, vels, codes, z=None):
+        """One analysis: gain, then every member moved in place."""
+        t4, clip = self.calGainMatrix(vels, codes, z)
+        enkf_update(vels.reshape(vels.shape[0], -1), t4, self.fm.dx, self.fm.dt)
+        return t4, clip
+
+    def createAMean(self, vels):
+        import torch
+        mean = torch.empty(vels.shape[1:], dtype=torch.float32, device=vels.device)
+        enkf_mean(mean, vels)
+        return mean
 
 
 def cal_objective_static(r, out, stream=None) -> None:
@@ -431,6 +522,12 @@ class Damp4t10d:
 
     def EssForwardModeling(self, encsrc, dcal):
         _check(lib().swfwi_damp4t10d_ess_forward_modeling(self.h, _ptr(encsrc), _ptr(dcal)))
+
+    def ess_forward_members(self, encsrc, vels, hona):
+        """EssForwardModeling with each member velocity (vels [n][nxpad][nzpad]
+        CUDA) into hona [n][ng*nt] in the analysis matrix's row order."""
+        _check(lib().swfwi_damp4t10d_ess_forward_members(self.h, _ptr(encsrc), _ptr(vels), vels.shape[0],
+                                                         _ptr(hona)))
 
     # ---- batched ----
     def forward_batch(self, wlt, dcal, shot_ids):

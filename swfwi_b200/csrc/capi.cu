@@ -357,6 +357,31 @@ int swfwi_damp4t10d_ess_forward_modeling(swfwi_damp4t10d *h, const float *encsrc
   });
 }
 
+int swfwi_encode_source(float *encsrc, const float *wlt, const int *codes, int nt, int ns, void *stream) {
+  return guarded([&] {
+    SWFWI_REQUIRE(encsrc && wlt && codes && nt > 0 && ns > 0, "bad encoder arguments");
+    launch_encode_source(encsrc, wlt, codes, nt, ns, reinterpret_cast<cudaStream_t>(stream));
+    check_launch();
+  });
+}
+
+int swfwi_encode_obs(float *encobs, const float *dobs, const int *codes, long long n_per_shot, int ns,
+                     void *stream) {
+  return guarded([&] {
+    SWFWI_REQUIRE(encobs && dobs && codes && n_per_shot > 0 && ns > 0, "bad encoder arguments");
+    launch_encode_obs(encobs, dobs, codes, n_per_shot, ns, reinterpret_cast<cudaStream_t>(stream));
+    check_launch();
+  });
+}
+
+int swfwi_damp4t10d_ess_forward_members(swfwi_damp4t10d *h, const float *encsrc, const float *vels,
+                                        int n, float *hona) {
+  return guarded([&] {
+    P(h).ess_forward_members(encsrc, vels, n, hona);
+    check_launch();
+  });
+}
+
 int swfwi_damp4t10d_forward_batch(swfwi_damp4t10d *h, const float *wlt, float *dcal,
                                   const int *shot_ids, int nshots) {
   return guarded([&] {

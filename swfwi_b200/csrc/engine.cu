@@ -292,7 +292,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
     if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
     return;
   }
-  cudaEvent_t done = step_timer().open(st_, pts, n, 1, 4);
+  cudaEvent_t done = step_timer().open(st_, pts, n, vel_stride_ ? n : 1, 4);
   StreamArgs a;
   a.prev = static_cast<float *>(prev);
   a.curr = static_cast<const float *>(curr);
@@ -303,8 +303,8 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.nz = nzpad;
   a.pitch = pitch;
   a.shot_stride = fstride;
-  a.vel_stride = 0;
-  a.shots_per_vel = std::max(n, 1);
+  a.vel_stride = vel_stride_;
+  a.shots_per_vel = vel_stride_ ? 1 : std::max(n, 1);
   a.xchunk = stream_xchunk;
   a.shot_major = stream_shot_major;
   a.err = d_err_.get();
@@ -542,6 +542,36 @@ void Propagator::ess_forward(const float *encsrc, float *dcal, const float *vel)
   PointSet src{d_src_pos_p_.get(), ns, nullptr};
   PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
   run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false, rcp_of(vel ? vel : vel_));
+}
+
+void Propagator::ess_forward_members(const float *encsrc, const float *vels, int n, float *hona) {
+  SWFWI_REQUIRE(encsrc && vels && hona && n > 0, "bad member batch arguments");
+  SWFWI_REQUIRE(nxpad > 12 && nzpad > 12, "grid size not set");
+  const long long per = (long long)nxpad * pitch;        // floats per member reciprocal
+  const long long vsz = (long long)nxpad * nzpad;
+  int mb = max_batch();
+  for (int c0 = 0; c0 < n; c0 += mb) {
+    int k = std::min(mb, n - c0);
+    members_rcp_.resize((size_t)k * per + 2 * kStreamCoff);
+    float *rcp = members_rcp_.get() + kStreamCoff;
+    for (int i = 0; i < k; i++)
+      launch_pitched_reciprocal(rcp + i * per, vels + (c0 + i) * vsz, nxpad, nzpad, pitch, st_);
+    std::vector<int> zeros(k, 0);                        // every slot: the one encoded supershot
+    w_.slot_shot.upload(zeros.data(), k, st_);
+    PointSet src{d_src_pos_p_.get(), ns, w_.slot_shot.get()};
+    PointSet rec{d_geo_pos_p_.get(), ng, w_.slot_shot.get()};
+    w_.dcal.resize((size_t)k * nt * ng);
+    struct Restore {
+      long long &v;
+      ~Restore() { v = 0; }
+    } restore{vel_stride_};
+    vel_stride_ = per;
+    run_forward<float>(w_, k, src, encsrc, ns, 0, 1, rec, ng, w_.dcal.get(), false, rcp);
+    vel_stride_ = 0;
+    // EssForwardModeling's dcal [nt][ng] -> the matrix column order [ng][nt]
+    launch_transpose_traces(hona + (long long)c0 * nt * ng, w_.dcal.get(), nt, ng, k, st_);
+  }
+  check_device_error();
 }
 
 int Propagator::max_batch() const {

@@ -99,6 +99,11 @@ class Propagator {
   void remove_direct_arrival(float *data, int shot_id, const float *vel = nullptr);
   void fwi_forward(const float *wlt, float *dcal, int shot_id);
   void ess_forward(const float *encsrc, float *dcal, const float *vel = nullptr);
+  // The HA loop of EnkfAnalyze::calGainMatrix (enkfanalyze.cpp:207-236):
+  // EssForwardModeling of the encoded supershot with each of n velocities
+  // (vels [n][nxpad*nzpad], caller layout), the seismograms transposed to
+  // the analysis matrix's column order: hona [n][ng*nt], row ig*nt + it.
+  void ess_forward_members(const float *encsrc, const float *vels, int n, float *hona);
 
   // ---- batched ----
   // dcal [n][nt][ngmax] for shots ids[0..n) (host list).
@@ -135,6 +140,8 @@ class Propagator {
   DevBuf<float> rcp_;           // pitched 1/vt of the bound velocity
   const float *rcp_for_ = nullptr;
   DevBuf<float> trial_rcp_;
+  DevBuf<float> members_rcp_;   // per-member reciprocals of ess_forward_members
+  long long vel_stride_ = 0;    // floats between slots' velocity reciprocals (0: one model)
   DevBuf<int> d_err_;
   DevBuf<float> damp_x_, damp_z_;   // per-axis sponge ramps (streaming step)
   // positions in the caller's layout (x*nzpad + z) ...

@@ -783,6 +783,29 @@ template void launch_record<float>(float *, long long, const float *, long long,
                                    cudaStream_t);
 template void launch_record<double>(double *, long long, const double *, long long, int, PointSet,
                                     cudaStream_t);
+// ---------------------------------------------------------------- trace transpose
+__global__ void k_transpose_traces(float *out, const float *in, int nt, int ng) {
+  __shared__ float tile[32][33];
+  const long long base = (long long)blockIdx.z * nt * ng;
+  const int it0 = blockIdx.y * 32, ig0 = blockIdx.x * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    int it = it0 + j, ig = ig0 + threadIdx.x;
+    if (it < nt && ig < ng) tile[j][threadIdx.x] = in[base + (long long)it * ng + ig];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    int ig = ig0 + j, it = it0 + threadIdx.x;
+    if (it < nt && ig < ng) out[base + (long long)ig * nt + it] = tile[threadIdx.x][j];
+  }
+}
+
+void launch_transpose_traces(float *out, const float *in, int nt, int ng, int nslots, cudaStream_t st) {
+  if (nt <= 0 || ng <= 0 || nslots <= 0) return;
+  dim3 g((ng + 31) / 32, (nt + 31) / 32, nslots);
+  k_transpose_traces<<<g, dim3(32, 8), 0, st>>>(out, in, nt, ng);
+  note_launch();
+}
+
 // ---------------------------------------------------------------- 16-bit strips
 namespace {
 template <int FMT>
