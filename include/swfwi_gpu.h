@@ -335,6 +335,34 @@ int swfwi_enkf_update(float *vels, long long model_size, int n, const double *t4
  * members' float sum in member order / n. */
 int swfwi_enkf_mean(float *mean, const float *vels, long long model_size, int n, void *stream);
 
+/* ------------------------------------------------------------------------
+ * RSF files (Madagascar format), the I/O of the reference's tools
+ * (sf_input / sf_output in src/tool/main-*.cpp; ShotDataReader,
+ * shotdata-reader.cpp:54-64).  Host buffers; native float32 data only;
+ * header keys are key=value tokens, the last occurrence wins; in="stdin"
+ * data embedded after the header are read too.
+ * ---------------------------------------------------------------------- */
+/* The value of one header key (as text) into value[len]. */
+int swfwi_rsf_get(const char *path, const char *key, char *value, int len);
+/* Axis lengths n[9] (1 where absent), d[9], o[9] (optional) and the number
+ * of axes longer than 1. */
+int swfwi_rsf_dims(const char *path, int *ndim, int *n, float *d, float *o);
+/* count floats starting at element `first`, axis 1 fastest (a velocity
+ * n1=nz, n2=nx reads straight into [nx][nz]). */
+int swfwi_rsf_read(const char *path, float *out, long long count, long long first);
+/* Header at path, data at data_path (NULL: path + "@"); axes n/d/o (d, o
+ * optional); extra: more header lines ("\tkey=value\n"), or NULL. */
+int swfwi_rsf_write(const char *path, const char *data_path, const float *data, int ndim, const int *n,
+                    const float *d, const float *o, const char *extra);
+/* Shots n1=nt, n2=ng, n3=ns on disk ([is][ig][it]) -> dobs [ns][nt][ng]
+ * (ShotDataReader::serialRead). */
+int swfwi_rsf_read_shots(const char *path, float *dobs, int ns, int nt, int ng);
+/* dobs [ns][nt][ng] -> a shot file as main-fm-damp.cpp:144-173 writes it
+ * (n1=nt d1=dt, n2=ng d2=dgx, n3=ns, labels and units); extra: the
+ * acquisition keys (fm, szbeg, ...) as header lines, or NULL. */
+int swfwi_rsf_write_shots(const char *path, const char *data_path, const float *dobs, int ns, int nt, int ng,
+                          float dt, float dgx, const char *extra);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,13 @@ _SIGS = {
     "swfwi_cal_objective": [_vp, C.c_longlong, _dp, _vp],
     "swfwi_cal_objective_static": [_vp, C.c_longlong, C.c_int, _vp, _vp],
     "swfwi_encode_source": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_rsf_get": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int],
+    "swfwi_rsf_dims": [C.c_char_p, _ip, _ip, _fp, _fp],
+    "swfwi_rsf_read": [C.c_char_p, _fp, C.c_longlong, C.c_longlong],
+    "swfwi_rsf_write": [C.c_char_p, C.c_char_p, _fp, C.c_int, _ip, _fp, _fp, C.c_char_p],
+    "swfwi_rsf_read_shots": [C.c_char_p, _fp, C.c_int, C.c_int, C.c_int],
+    "swfwi_rsf_write_shots": [C.c_char_p, C.c_char_p, _fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                              C.c_char_p],
     "swfwi_encode_obs": [_vp, _vp, _vp, C.c_longlong, C.c_int, _vp],
     "swfwi_damp4t10d_ess_forward_members": [_vp, _vp, _vp, C.c_int, _vp],
     "swfwi_enkf_gain_matrix": [_vp, _vp, _vp, C.c_longlong, C.c_int, C.c_float, _dp, C.c_ulonglong, _dp,
