@@ -298,6 +298,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.curr = static_cast<const float *>(curr);
   a.rcp = static_cast<const float *>(velrcp);
   a.damp_x = damp_x_.get();
+  a.ramp = bx0;   // launch_damp_tables ramp length
   a.damp_z = damp_z_.get();
   a.nx = nxpad;
   a.nz = nzpad;

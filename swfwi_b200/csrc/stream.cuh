@@ -43,6 +43,7 @@ struct StreamArgs {
   int xchunk;             // output rows per CTA
   int shot_major;         // 0: blockIdx = (shot, band, chunk); 1: (band, chunk, shot)
   int *err;               // set to 1 when a bounded wait gives up
+  int ramp;               // damp_x is 0 on rows [ramp, nx - ramp): those rows skip its load
 };
 
 constexpr int kStreamCoff = 8;   // floats between a slot's start and its origin
@@ -318,7 +319,7 @@ fd_step_stream(StreamArgs a) {
       float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
       float ucl = uc[-1], ucr = uc[4];
       float dxr = 0.f;
-      if constexpr (DAMPED) dxr = a.damp_x[j];
+      if constexpr (DAMPED) dxr = (j < a.ramp || j >= nx - a.ramp) ? a.damp_x[j] : 0.f;
       float o[4];
 #pragma unroll
       for (int i = 0; i < 4; i++) {

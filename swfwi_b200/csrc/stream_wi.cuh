@@ -144,6 +144,8 @@ fd_step_wi(StreamArgs a) {
   const bool outlane = lane >= 1 && lane <= 30 && zg < nz - 6 && zg + 3 >= 6;
   const bool fullgroup = zok[0] && zok[1] && zok[2] && zok[3];
   const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
+  // steps whose output row lies between the x ramps, where damp_x is 0
+  const int k_ramp_lo = a.ramp - xa + 12, k_ramp_hi = nx - a.ramp - xa + 12;
   // u2 of rows xa-13+k and xa-12+k at step k (the row made at step k is up)
   float4 um = make_float4(0.f, 0.f, 0.f, 0.f), uc = um;
 
@@ -212,7 +214,7 @@ fd_step_wi(StreamArgs a) {
       bool damp = false;
       float dxr = 0.f;
       if constexpr (DAMPED) {
-        dxr = damp_row[k];
+        dxr = (k < k_ramp_lo || k >= k_ramp_hi) ? damp_row[k] : 0.f;
         damp = coldamp || dxr != 0.f;
       }
       if (!damp) {

@@ -155,6 +155,8 @@ fd_step_ws(StreamArgs a) {
   const bool outgroup = t >= 1 && t < NT - 1 && zg < nz - 6 && zg + 3 >= 6;
   const bool fullgroup = zok[0] && zok[1] && zok[2] && zok[3];
   const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
+  // steps whose output row lies between the x ramps, where damp_x is 0
+  const int k_ramp_lo = a.ramp - xa + 12, k_ramp_hi = nx - a.ramp - xa + 12;
 
   // One step.  PH is k & 15 when known at compile time, else -1.
   auto step = [&](auto ph, int k) -> bool {
@@ -233,7 +235,7 @@ fd_step_ws(StreamArgs a) {
       bool damp = false;
       float dxr = 0.f;
       if constexpr (DAMPED) {
-        dxr = damp_row[k];
+        dxr = (k < k_ramp_lo || k >= k_ramp_hi) ? damp_row[k] : 0.f;
         damp = coldamp || dxr != 0.f;
       }
       if (!damp) {
