@@ -95,6 +95,7 @@ _SIGS = {
     "swfwi_cal_objective": [_vp, C.c_longlong, _dp, _vp],
     "swfwi_cal_objective_static": [_vp, C.c_longlong, C.c_int, _vp, _vp],
     "swfwi_encode_source": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_damp4t10d_set_fusion": [_vp, C.c_int],
     "swfwi_rsf_get": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int],
     "swfwi_rsf_dims": [C.c_char_p, _ip, _ip, _fp, _fp],
     "swfwi_rsf_read": [C.c_char_p, _fp, C.c_longlong, C.c_longlong],
@@ -422,6 +423,10 @@ class Damp4t10d:
     def set_arith(self, arith: int):
         _check(lib().swfwi_damp4t10d_set_arith(self.h, arith))
         self.arith = arith
+
+    def set_fusion(self, on: bool):
+        """Fused forward time loop (record, strips, next injection in the step)."""
+        _check(lib().swfwi_damp4t10d_set_fusion(self.h, int(bool(on))))
 
     def set_strip_format(self, fmt: int):
         """Boundary strips of the gradients: STRIP_F32 (exact), STRIP_F16 or

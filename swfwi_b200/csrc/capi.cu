@@ -183,6 +183,10 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format) {
   });
 }
 
+int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on) {
+  return guarded([&] { P(h).fuse = on != 0; });
+}
+
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest) {
   return guarded([&] {

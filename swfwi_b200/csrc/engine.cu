@@ -273,7 +273,7 @@ void Propagator::check_device_error() {
 // one velocity model): the streaming TMA kernel for float arithmetics, the
 // shared-memory tile kernel for FP64.
 void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp,
-                             int n) {
+                             int n, const Epilogue *epi) {
   double pts = (double)(nxpad - 12) * (nzpad - 12);
   if (ar == ARITH_F64) {
     cudaEvent_t done = step_timer().open(st_, pts, n, 1, 8);
@@ -299,6 +299,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.rcp = static_cast<const float *>(velrcp);
   a.damp_x = damp_x_.get();
   a.ramp = bx0;   // launch_damp_tables ramp length
+  a.epi = epi ? *epi : Epilogue{};
   a.damp_z = damp_z_.get();
   a.nx = nxpad;
   a.nz = nzpad;
@@ -309,7 +310,11 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.xchunk = stream_xchunk;
   a.shot_major = stream_shot_major;
   a.err = d_err_.get();
-  if (stream_kernel == 2) launch_wi_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  if (epi) {
+    // the fused step is the warp-specialised kernel with 376-deep bands
+    if (stream_kernel != 1) a.xchunk = 64;
+    launch_ws_step(ar, damped, 376, stream_kernel == 1 ? stream_depth : 3, a, n, st_);
+  } else if (stream_kernel == 2) launch_wi_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   else if (stream_kernel == 1) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   else launch_stream_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
@@ -444,16 +449,81 @@ void Propagator::ensure_work(Work<T> &w, int n, bool strips) {
   w.obj.resize(n);
 }
 
+bool Propagator::line_of(const int *xs, const int *zs, int n, PtLine &out) const {
+  if (n <= 0) return false;
+  out = PtLine{xs[0] + bx0, zs[0] + bz0, 0, 0, n};
+  if (n == 1) return true;
+  out.jx = xs[1] - xs[0];
+  out.jz = zs[1] - zs[0];
+  if (out.jx == 0 && out.jz == 0) return false;
+  for (int i = 2; i < n; i++)
+    if (xs[i] - xs[i - 1] != out.jx || zs[i] - zs[i - 1] != out.jz) return false;
+  return true;
+}
+
+bool Propagator::shot_lines(const int *ids, int k, bool per_shot_receivers, std::vector<PtLine> &src,
+                            std::vector<PtLine> &rec) const {
+  src.resize(k);
+  rec.resize(k);
+  for (int j = 0; j < k; j++) {
+    const int s = ids[j];
+    if (!line_of(&h_src_x[s], &h_src_z[s], 1, src[j])) return false;
+    const bool ok = per_shot_receivers
+                        ? line_of(&h_rec_x[(size_t)s * ngmax], &h_rec_z[(size_t)s * ngmax], h_rec_count[s], rec[j])
+                        : line_of(h_geo_x.data(), h_geo_z.data(), ng, rec[j]);
+    if (!ok) return false;
+  }
+  return true;
+}
+
+bool Propagator::ess_lines(int k, std::vector<PtLine> &src, std::vector<PtLine> &rec) const {
+  PtLine s, r;
+  if (!line_of(h_src_x.data(), h_src_z.data(), ns, s) || !line_of(h_geo_x.data(), h_geo_z.data(), ng, r))
+    return false;
+  src.assign(k, s);
+  rec.assign(k, r);
+  return true;
+}
+
 template <typename T>
 void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                              long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
-                             bool save_strips, const void *velrcp) {
+                             bool save_strips, const void *velrcp, const std::vector<PtLine> *src_lines,
+                             const std::vector<PtLine> *rec_lines) {
   ensure_work(w, n, save_strips);
   T *p0 = w.p0.get() + kStreamCoff, *p1 = w.p1.get() + kStreamCoff;
   w.p0.zero(st_);
   w.p1.zero(st_);
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
+  const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
+                     (int)rec_lines->size() == n && bx0 >= 12 &&
+                     (!save_strips || strip_format == SWFWI_STRIP_F32);
+  if (fused) {
+    // one launch per step: the step records its input field, saves its
+    // strips and adds the next step's source to the field it makes
+    w.src_lines.upload(*src_lines, st_);
+    w.rec_lines.upload(*rec_lines, st_);
+    if (dcal) SWFWI_CUDA(cudaMemsetAsync(dcal, 0, sizeof(T) * (size_t)n * nt * ngrec, st_));
+    launch_inject<T>(p1, fstride, n, src, vals, slot_stride, i_stride, +1, st_);
+    for (int it = 0; it < nt; it++) {
+      Epilogue e{};
+      e.src = w.src_lines.get();
+      e.rec = w.rec_lines.get();
+      e.seis = dcal ? reinterpret_cast<float *>(dcal) + (long long)it * ngrec : nullptr;
+      e.seis_slot_stride = (long long)nt * ngrec;
+      e.strips = save_strips ? reinterpret_cast<float *>(w.strips.get()) + (long long)it * bsize : nullptr;
+      e.strip_slot_stride = bstride;
+      e.inj = it + 1 < nt ? reinterpret_cast<const float *>(vals) + (long long)(it + 1) * it_stride : nullptr;
+      e.inj_slot_stride = slot_stride;
+      e.inj_stride = i_stride;
+      e.bx0 = bx0;
+      step_fields(ar, true, p0, p1, velrcp, n, &e);
+      std::swap(p0, p1);
+    }
+    if (p0 != w.p0.get() + kStreamCoff) std::swap(w.p0, w.p1);
+    return;
+  }
   for (int it = 0; it < nt; it++) {
     // addSource -> stepForward -> swap -> recordSeis / writeBndry
     // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
@@ -535,14 +605,20 @@ void Propagator::fwi_forward(const float *wlt, float *dcal, int shot_id) {
   SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
   PointSet src{d_src_pos_p_.get() + shot_id, 1, nullptr};
   PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
-  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, rcp_of(vel_));
+  std::vector<PtLine> sl, rl;
+  const bool lines = shot_lines(&shot_id, 1, false, sl, rl);
+  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, rcp_of(vel_), lines ? &sl : nullptr,
+                     lines ? &rl : nullptr);
 }
 
 void Propagator::ess_forward(const float *encsrc, float *dcal, const float *vel) {
   SWFWI_REQUIRE(encsrc && dcal, "null pointer");
   PointSet src{d_src_pos_p_.get(), ns, nullptr};
   PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
-  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false, rcp_of(vel ? vel : vel_));
+  std::vector<PtLine> sl, rl;
+  const bool lines = ess_lines(1, sl, rl);
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false, rcp_of(vel ? vel : vel_),
+                     lines ? &sl : nullptr, lines ? &rl : nullptr);
 }
 
 void Propagator::ess_forward_members(const float *encsrc, const float *vels, int n, float *hona) {
@@ -567,7 +643,10 @@ void Propagator::ess_forward_members(const float *encsrc, const float *vels, int
       ~Restore() { v = 0; }
     } restore{vel_stride_};
     vel_stride_ = per;
-    run_forward<float>(w_, k, src, encsrc, ns, 0, 1, rec, ng, w_.dcal.get(), false, rcp);
+    std::vector<PtLine> sl, rl;
+    const bool lines = ess_lines(k, sl, rl);
+    run_forward<float>(w_, k, src, encsrc, ns, 0, 1, rec, ng, w_.dcal.get(), false, rcp, lines ? &sl : nullptr,
+                       lines ? &rl : nullptr);
     vel_stride_ = 0;
     // EssForwardModeling's dcal [nt][ng] -> the matrix column order [ng][nt]
     launch_transpose_traces(hona + (long long)c0 * nt * ng, w_.dcal.get(), nt, ng, k, st_);
@@ -602,8 +681,10 @@ void Propagator::forward_batch(const float *wlt, float *dcal, const int *ids, in
     w_.slot_shot.upload(ids + c0, k, st_);
     PointSet src{d_src_pos_p_.get(), 1, w_.slot_shot.get()};
     PointSet rec{d_rec_pos_p_.get(), ngmax, w_.slot_shot.get()};
+    std::vector<PtLine> sl, rl;
+    const bool lines = shot_lines(ids + c0, k, true, sl, rl);
     run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, dcal + (long long)c0 * nt * ngmax,
-                       false, rcp);
+                       false, rcp, lines ? &sl : nullptr, lines ? &rl : nullptr);
   }
 }
 
@@ -633,7 +714,10 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
     w_.image.zero(st_);
     // FwiForwardModeling and calgradient's forward sweep model the same
     // field from the same source: one sweep records dcal and saves strips.
-    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), true, rcp);
+    std::vector<PtLine> sl, rl;
+    const bool lines = shot_lines(ids + c0, k, true, sl, rl);
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), true, rcp, lines ? &sl : nullptr,
+                       lines ? &rl : nullptr);
     launch_mute_windows(w_.win.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
                         d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
     launch_muted_residual(w_.res.get(), dobs, dn, rr, w_.dcal.get(), w_.win.get(), w_.win.get(), nt,
@@ -669,7 +753,10 @@ double Propagator::trial_objective_fwi(const float *wlt, const float *dobs, cons
     w_.res.resize((size_t)k * dn);
     w_.win.resize((size_t)k * ngmax * 2);
     w_.win2.resize((size_t)k * ngmax * 2);
-    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), false, rcp);
+    std::vector<PtLine> sl, rl;
+    const bool lines = shot_lines(ids + c0, k, true, sl, rl);
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), false, rcp, lines ? &sl : nullptr,
+                       lines ? &rl : nullptr);
     // modelled data muted with the trial velocity, observed data with the
     // current one (updatesteplenop.cpp:77 and essfwiframework.cpp:205)
     launch_mute_windows(w_.win.get(), trial_vel, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
@@ -695,7 +782,10 @@ void Propagator::calgradient_ess(const float *encsrc, const float *vsrc, float *
   w_.image.resize((size_t)fstride);
   w_.image.zero(st_);
   to_pitched(w_.image.get() + kStreamCoff, grad);
-  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp);
+  std::vector<PtLine> sl, rl;
+  const bool lines = ess_lines(1, sl, rl);
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp, lines ? &sl : nullptr,
+                     lines ? &rl : nullptr);
   run_backward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, rcp);
   from_pitched(grad, w_.image.get() + kStreamCoff);
 }
@@ -709,7 +799,10 @@ void Propagator::calgradient_fwi(const float *wlt, const float *vsrc, float *gra
   w_.image.resize((size_t)fstride);
   w_.image.zero(st_);
   to_pitched(w_.image.get() + kStreamCoff, grad);
-  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp);
+  std::vector<PtLine> sl, rl;
+  const bool lines = shot_lines(&shot_id, 1, false, sl, rl);
+  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp, lines ? &sl : nullptr,
+                     lines ? &rl : nullptr);
   run_backward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, rcp);
   from_pitched(grad, w_.image.get() + kStreamCoff);
 }

@@ -50,6 +50,7 @@ struct Work {
   DevBuf<float> qscale;       // their scales [slot][nt]
   DevBuf<float> dcal, res, vsrc;   // [slot][nt][ngmax]
   DevBuf<int> win, win2, slot_shot, slot_row;
+  DevBuf<PtLine> src_lines, rec_lines;   // fused epilogue lines [slot]
   DevBuf<double> partials, obj;
 };
 
@@ -77,6 +78,7 @@ class Propagator {
   int stream_xchunk = 64;     // rows per CTA
   int stream_depth = 3;       // rows ahead (3 or 5; warp-specialised 3 or 7)
   int stream_shot_major = 0;  // launch order: 0 = shots fastest
+  bool fuse = true;           // fused forward epilogue where it applies
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);
   void set_dims(int nxpad, int nzpad);   // padded grid; uploads geometry
@@ -156,14 +158,25 @@ class Propagator {
 
   void upload_geometry();
   const float *rcp_of(const float *vel);
-  void step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp, int n);
+  void step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp, int n,
+                   const Epilogue *epi = nullptr);
+  // Point lines (padded coordinates) for the fused forward epilogue; false
+  // when the points do not form a regular line.
+  bool line_of(const int *xs, const int *zs, int n, PtLine &out) const;
+  bool shot_lines(const int *ids, int k, bool per_shot_receivers, std::vector<PtLine> &src,
+                  std::vector<PtLine> &rec) const;
+  bool ess_lines(int k, std::vector<PtLine> &src, std::vector<PtLine> &rec) const;
 
   // Forward time loop for n slots.  Source values:
   // vals + it*it_stride + slot*slot_stride + i*i_stride.
+  // With per-slot lines (src_lines, rec_lines host vectors of n) and FP32
+  // fields, the step itself records, saves FP32 strips and injects the next
+  // source (one launch per time step).
   template <typename T>
   void run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                    long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
-                   bool save_strips, const void *velrcp);
+                   bool save_strips, const void *velrcp, const std::vector<PtLine> *src_lines = nullptr,
+                   const std::vector<PtLine> *rec_lines = nullptr);
   // Backward sweep with imaging into w.image (not cleared here).
   template <typename T>
   void run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include "common.hpp"
 #include "kernels.cuh"
 #include "swfwi_gpu.h"
 
@@ -663,20 +664,34 @@ static void stream_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStr
 }
 
 // ---------------------------------------------------------------- warp-specialised step
-template <int ARITH, bool DAMPED, int NW, int D>
-static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+template <int ARITH, bool DAMPED, int NW, int D, bool EPI>
+static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
   constexpr int BZ = 128 * NW - 8;
   constexpr size_t smem = ws_smem_bytes<NW, D>();
   static bool attr_set = false;   // raise the dynamic shared memory limit once
   if (!attr_set) {
-    cudaFuncSetAttribute(fd_step_ws<ARITH, DAMPED, NW, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(fd_step_ws<ARITH, DAMPED, NW, D, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
     attr_set = true;
   }
   int nbands = (a.nz - 10 + BZ - 1) / BZ;
   int nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
   dim3 g = a.shot_major ? dim3(nbands, nchunks, nslots) : dim3(nslots, nbands, nchunks);
-  fd_step_ws<ARITH, DAMPED, NW, D><<<g, (NW + 1) * 32, smem, st>>>(a);
+  fd_step_ws<ARITH, DAMPED, NW, D, EPI><<<g, (NW + 1) * 32, smem, st>>>(a);
+}
+
+template <int ARITH, bool DAMPED, int NW, int D>
+static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+  const bool epi = a.epi.seis || a.epi.strips || a.epi.inj;
+  if constexpr (NW == 3) {
+    if (epi) {
+      ws_launch<ARITH, DAMPED, NW, D, true>(a, nslots, st);
+      return;
+    }
+  } else {
+    if (epi) throw Error(SWFWI_ERR_BAD_ARG, "the fused step runs with 376-deep bands only");
+  }
+  ws_launch<ARITH, DAMPED, NW, D, false>(a, nslots, st);
 }
 
 template <int ARITH, bool DAMPED, int D>

@@ -30,6 +30,32 @@
 
 namespace swfwi {
 
+// A regular line of points in padded grid coordinates: point i at
+// (x0 + i*jx, z0 + i*jz), i < n (a ShotPosition, shot-position.cpp:11-41).
+struct PtLine {
+  int x0, z0, jx, jz, n;
+};
+
+// Work a streaming step does at its output points besides the update (the
+// forward time loop of FwiForwardModeling / calgradient, fused):
+//   seis:   recordSeis of this step's input field (the field after the
+//           reference's swap) at the slot's receivers, seis[slot*stride + i];
+//   strips: writeBndry of the same field (FP32, strip_index order);
+//   inj:    addSource of the next step into the new field at the slot's
+//           sources, inj[slot*inj_slot_stride + i*inj_stride] (one float add).
+// Lines are per slot; a null pointer skips that part.
+struct Epilogue {
+  const PtLine *src, *rec;            // [nslots]
+  float *seis;
+  long long seis_slot_stride;
+  float *strips;
+  long long strip_slot_stride;
+  const float *inj;
+  long long inj_slot_stride;
+  int inj_stride;
+  int bx0;                            // sponge + 6 (the strips' geometry)
+};
+
 struct StreamArgs {
   float *prev;            // field origins (see layout above)
   const float *curr;
@@ -44,6 +70,7 @@ struct StreamArgs {
   int shot_major;         // 0: blockIdx = (shot, band, chunk); 1: (band, chunk, shot)
   int *err;               // set to 1 when a bounded wait gives up
   int ramp;               // damp_x is 0 on rows [ramp, nx - ramp): those rows skip its load
+  Epilogue epi;           // used by the fused variant of the warp-specialised step
 };
 
 constexpr int kStreamCoff = 8;   // floats between a slot's start and its origin
@@ -187,6 +214,52 @@ __device__ __forceinline__ float update_pt(float c, float p, float r, float uc, 
     return base + inc;
   }
 }
+
+// Walks a line's points row by row for a CTA whose output rows increase by
+// one per step from xa: at each row, at most one point when jx != 0 (all of
+// a vertical line's points sit on row x0).
+struct LineCursor {
+  int next_x, next_i, step_i, dx, left;
+  __device__ __forceinline__ void init(const PtLine &l, int xa) {
+    next_x = -1; left = 0; step_i = 0; dx = 0; next_i = 0;
+    if (l.n <= 0 || l.jx == 0) return;
+    if (l.jx > 0) {
+      int i0 = xa <= l.x0 ? 0 : (xa - l.x0 + l.jx - 1) / l.jx;
+      if (i0 >= l.n) return;
+      next_i = i0; step_i = 1; dx = l.jx; left = l.n - i0;
+    } else {
+      const int ax = -l.jx;
+      if (l.x0 < xa) return;
+      int i0 = (l.x0 - xa) / ax;
+      if (i0 > l.n - 1) i0 = l.n - 1;
+      next_i = i0; step_i = -1; dx = ax; left = i0 + 1;
+    }
+    next_x = l.x0 + next_i * l.jx;
+  }
+  // calls f(i, d) for the point on row x at depth zg + d, d < 4
+  template <typename F>
+  __device__ __forceinline__ void visit(const PtLine &l, int x, int zg, F &&f) {
+    if (l.jx != 0) {
+      if (left > 0 && x == next_x) {
+        const int z = l.z0 + next_i * l.jz;
+        if (z >= zg && z < zg + 4) f(next_i, z - zg);
+        next_i += step_i;
+        next_x += dx;
+        left--;
+      }
+    } else if (x == l.x0 && l.n > 0) {
+      if (l.jz == 0) {
+        if (l.z0 >= zg && l.z0 < zg + 4) f(0, l.z0 - zg);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+          const int t = zg + d - l.z0;
+          if (t % l.jz == 0 && t / l.jz >= 0 && t / l.jz < l.n) f(t / l.jz, d);
+        }
+      }
+    }
+  }
+};
 
 }  // namespace stream_detail
 

@@ -59,8 +59,10 @@ constexpr size_t ws_smem_bytes() {
   return ws_detail::Smem<NW * 32, D + 1>::bytes;
 }
 
-template <int ARITH, bool DAMPED, int NW, int D>
-__global__ void __launch_bounds__((NW + 1) * 32)
+// EPI: also run a.epi (record, strip save, next injection) at the output
+// points, from the staged input row and the new values before they are stored.
+template <int ARITH, bool DAMPED, int NW, int D, bool EPI = false>
+__global__ void __launch_bounds__((NW + 1) * 32, EPI ? (ARITH == ARITH_REF ? 4 : 5) : 1)
 fd_step_ws(StreamArgs a) {
   using namespace ws_detail;
   constexpr int NT = NW * 32;      // consumer threads
@@ -157,6 +159,18 @@ fd_step_ws(StreamArgs a) {
   const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
   // steps whose output row lies between the x ramps, where damp_x is 0
   const int k_ramp_lo = a.ramp - xa + 12, k_ramp_hi = nx - a.ramp - xa + 12;
+  // fused epilogue: this slot's lines, cursors from row xa, strip geometry
+  PtLine sline{0, 0, 0, 0, 0}, rline{0, 0, 0, 0, 0};
+  LineCursor scur, rcur;
+  bool strip_bot = false;   // this lane holds depths of the bottom strip band
+  if constexpr (EPI) {
+    if (a.epi.inj) sline = a.epi.src[shot];
+    if (a.epi.seis) rline = a.epi.rec[shot];
+    scur.init(sline, xa);
+    rcur.init(rline, xa);
+    const int bz = nz - a.epi.bx0;
+    strip_bot = a.epi.strips && zg + 3 >= bz && zg < bz + 6;
+  }
 
   // One step.  PH is k & 15 when known at compile time, else -1.
   auto step = [&](auto ph, int k) -> bool {
@@ -255,6 +269,46 @@ fd_step_ws(StreamArgs a) {
           float uzp = i == 3 ? ucr : get(uc4, i + 1);
           o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
                                   get(um4, i), get(up4, i), delta);
+        }
+      }
+      if constexpr (EPI) {
+        const int x = xa - 12 + k;
+        const int b = a.epi.bx0, w = 6;
+        if (a.epi.seis) {
+          float *sd = a.epi.seis + (long long)shot * a.epi.seis_slot_stride;
+          rcur.visit(rline, x, zg, [&](int i, int d) {
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (q == d && zok[q]) sd[i] = get(c4, q);
+          });
+        }
+        if (a.epi.strips) {
+          float *sd = a.epi.strips + (long long)shot * a.epi.strip_slot_stride;
+          const int nxs = nx - 2 * (b - w), nzs = nz - 6 - b;
+          if (strip_bot && x >= b - w && x < nx - b + w) {
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+              const int z = zg + d;
+              if (zok[d] && z >= nz - b && z < nz - b + w) sd[(x - b + w) * w + (z - (nz - b))] = get(c4, d);
+            }
+          }
+          const int ixb = (x >= b - w && x < b) ? x - (b - w) : ((x >= nx - b && x < nx - b + w) ? w + x - (nx - b) : -1);
+          if (ixb >= 0) {
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+              const int z = zg + d;
+              if (zok[d] && z < nz - b) sd[w * nxs + ixb * nzs + (z - 6)] = get(c4, d);
+            }
+          }
+        }
+        if (a.epi.inj) {
+          const float *iv = a.epi.inj + (long long)shot * a.epi.inj_slot_stride;
+          scur.visit(sline, x, zg, [&](int i, int d) {
+            const float v = iv[(long long)i * a.epi.inj_stride];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (q == d && zok[q]) o[q] = __fadd_rn(o[q], v);
+          });
         }
       }
       float *dst = prevg + (long long)(k - 12) * P;
