@@ -550,7 +550,8 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
 template <typename T>
 void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                               long long slot_stride, int i_stride, PointSet rec, int ngrec,
-                              const T *vsrc, const void *velrcp) {
+                              const T *vsrc, const void *velrcp, const std::vector<PtLine> *src_lines,
+                              const std::vector<PtLine> *rec_lines) {
   size_t f = (size_t)n * fstride;
   w.g0.resize(f);
   w.g1.resize(f);
@@ -561,6 +562,58 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
   int npts = (int)fstride;
+  const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
+                     (int)rec_lines->size() == n && bx0 >= 12 && strip_format == SWFWI_STRIP_F32;
+  if (fused) {
+    w.src_lines.upload(*src_lines, st_);
+    w.rec_lines.upload(*rec_lines, st_);
+    float *strips = reinterpret_cast<float *>(w.strips.get());
+    float *image = reinterpret_cast<float *>(w.image.get()) + kStreamCoff;
+    // the first step's strip restore and receiver injection; later ones are
+    // done by the previous step's kernels
+    launch_strip_read<T>(w.strips.get() + (long long)(nt - 1) * bsize, bstride, sp0, fstride, n, nxpad, nzpad,
+                         bx0, pitch, st_);
+    launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)(nt - 1) * ngrec, (long long)nt * ngrec, 1, +1,
+                     st_);
+    for (int it = nt - 1; it >= 0; it--) {
+      std::swap(sp0, sp1);
+      float t = dt * (float)it;
+      float scale = 0.0f;
+      bool last = false;
+      if ((double)t > 0.4) scale = 1.0f;
+      else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
+      else last = true;   // the reference's loop breaks after this step, before imaging
+      const bool next = !last && it >= 1;
+      Epilogue e{};
+      e.src = w.src_lines.get();
+      e.sub = reinterpret_cast<const float *>(vals) + (long long)it * it_stride;
+      e.sub_slot_stride = slot_stride;
+      e.sub_stride = i_stride;
+      if (!last) {
+        e.image = image;
+        e.gcurr = reinterpret_cast<const float *>(gp1);
+        e.scale = scale;
+      }
+      if (next) {
+        e.restore = strips + (long long)(it - 1) * bsize;
+        e.restore_slot_stride = bstride;
+      }
+      e.bx0 = bx0;
+      step_fields(ar, false, sp0, sp1, velrcp, n, &e);
+      Epilogue r{};
+      r.src = w.rec_lines.get();
+      if (next) {
+        r.inj = reinterpret_cast<const float *>(vsrc) + (long long)(it - 1) * ngrec;
+        r.inj_slot_stride = (long long)nt * ngrec;
+        r.inj_stride = 1;
+      }
+      r.bx0 = bx0;
+      step_fields(ar, true, gp0, gp1, velrcp, n, &r);
+      std::swap(gp0, gp1);
+      if (last) break;
+    }
+    return;
+  }
   for (int it = nt - 1; it >= 0; it--) {
     // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
     // subSource; receiver addSource -> stepForward -> swap; image.
@@ -724,7 +777,8 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
                           ngmax, k, st_);
     launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);
     launch_trans_vsrc(w_.vsrc.get(), w_.res.get(), nt, ngmax, k, st_);
-    run_backward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.vsrc.get(), rcp);
+    run_backward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.vsrc.get(), rcp, lines ? &sl : nullptr,
+                        lines ? &rl : nullptr);
     launch_finalize_gradient(grad, w_.image.get() + kStreamCoff, fstride, k, nxpad, nzpad, bx0, pitch,
                              (accumulate || c0 > 0) ? 1 : 0, st_);
     if (obj) {
@@ -786,7 +840,8 @@ void Propagator::calgradient_ess(const float *encsrc, const float *vsrc, float *
   const bool lines = ess_lines(1, sl, rl);
   run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp, lines ? &sl : nullptr,
                      lines ? &rl : nullptr);
-  run_backward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, rcp);
+  run_backward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, rcp, lines ? &sl : nullptr,
+                      lines ? &rl : nullptr);
   from_pitched(grad, w_.image.get() + kStreamCoff);
 }
 
@@ -803,7 +858,8 @@ void Propagator::calgradient_fwi(const float *wlt, const float *vsrc, float *gra
   const bool lines = shot_lines(&shot_id, 1, false, sl, rl);
   run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp, lines ? &sl : nullptr,
                      lines ? &rl : nullptr);
-  run_backward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, rcp);
+  run_backward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, rcp, lines ? &sl : nullptr,
+                      lines ? &rl : nullptr);
   from_pitched(grad, w_.image.get() + kStreamCoff);
 }
 

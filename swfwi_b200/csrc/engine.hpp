@@ -179,9 +179,13 @@ class Propagator {
                    const std::vector<PtLine> *rec_lines = nullptr);
   // Backward sweep with imaging into w.image (not cleared here).
   template <typename T>
+  // With per-slot lines and FP32 fields/strips: two launches per step (the
+  // source back-step also subtracts the source, images and restores the
+  // next step's strips; the receiver step injects the next residual).
   void run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                     long long slot_stride, int i_stride, PointSet rec, int ngrec, const T *vsrc,
-                    const void *velrcp);
+                    const void *velrcp, const std::vector<PtLine> *src_lines = nullptr,
+                    const std::vector<PtLine> *rec_lines = nullptr);
   template <typename T>
   void ensure_work(Work<T> &w, int n, bool strips);
   // copies between the caller's [nxpad][nzpad] layout and pitched rows

@@ -664,7 +664,7 @@ static void stream_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStr
 }
 
 // ---------------------------------------------------------------- warp-specialised step
-template <int ARITH, bool DAMPED, int NW, int D, bool EPI>
+template <int ARITH, bool DAMPED, int NW, int D, int EPI>
 static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
   constexpr int BZ = 128 * NW - 8;
   constexpr size_t smem = ws_smem_bytes<NW, D>();
@@ -682,16 +682,17 @@ static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
 
 template <int ARITH, bool DAMPED, int NW, int D>
 static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
-  const bool epi = a.epi.seis || a.epi.strips || a.epi.inj;
+  const Epilogue &e = a.epi;
+  const int mode = (e.sub || e.image || e.restore) ? 2 : ((e.seis || e.strips) ? 1 : (e.inj ? 3 : 0));
+  if (mode == 2 && (e.inj || e.seis || e.strips)) throw Error(SWFWI_ERR_BAD_ARG, "mixed fused epilogue parts");
   if constexpr (NW == 3) {
-    if (epi) {
-      ws_launch<ARITH, DAMPED, NW, D, true>(a, nslots, st);
-      return;
-    }
+    if (mode == 1) return ws_launch<ARITH, DAMPED, NW, D, 1>(a, nslots, st);
+    if (mode == 2) return ws_launch<ARITH, DAMPED, NW, D, 2>(a, nslots, st);
+    if (mode == 3) return ws_launch<ARITH, DAMPED, NW, D, 3>(a, nslots, st);
   } else {
-    if (epi) throw Error(SWFWI_ERR_BAD_ARG, "the fused step runs with 376-deep bands only");
+    if (mode) throw Error(SWFWI_ERR_BAD_ARG, "the fused step runs with 376-deep bands only");
   }
-  ws_launch<ARITH, DAMPED, NW, D, false>(a, nslots, st);
+  ws_launch<ARITH, DAMPED, NW, D, 0>(a, nslots, st);
 }
 
 template <int ARITH, bool DAMPED, int D>

@@ -37,13 +37,18 @@ struct PtLine {
 };
 
 // Work a streaming step does at its output points besides the update (the
-// forward time loop of FwiForwardModeling / calgradient, fused):
-//   seis:   recordSeis of this step's input field (the field after the
-//           reference's swap) at the slot's receivers, seis[slot*stride + i];
-//   strips: writeBndry of the same field (FP32, strip_index order);
-//   inj:    addSource of the next step into the new field at the slot's
-//           sources, inj[slot*inj_slot_stride + i*inj_stride] (one float add).
-// Lines are per slot; a null pointer skips that part.
+// time loops of FwiForwardModeling and calgradient, fused).  In order:
+//   seis:    recordSeis of this step's input field (the field after the
+//            reference's swap) at the `rec` points, seis[slot*stride + i];
+//   strips:  writeBndry of the same field (FP32, strip_index order);
+//   inj:     addSource of the next step into the new field at the `src`
+//            points, inj[slot*inj_slot_stride + i*inj_stride] (one float add);
+//   sub:     subSource into the new field at the `src` points (float sub);
+//   image:   image -= (new * gcurr) * scale at every output point
+//            (cross_correlation; gcurr, image laid out as the fields);
+//   restore: readBndry of the next backward step into the new field.
+// Lines are per slot; a null pointer skips that part; inj and sub are never
+// both set.
 struct Epilogue {
   const PtLine *src, *rec;            // [nslots]
   float *seis;
@@ -53,6 +58,14 @@ struct Epilogue {
   const float *inj;
   long long inj_slot_stride;
   int inj_stride;
+  const float *sub;
+  long long sub_slot_stride;
+  int sub_stride;
+  float *image;
+  const float *gcurr;
+  float scale;
+  const float *restore;
+  long long restore_slot_stride;
   int bx0;                            // sponge + 6 (the strips' geometry)
 };
 
@@ -145,6 +158,7 @@ __device__ __forceinline__ void fence_mbar_init() {
 }
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ld4g(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ float get(const float4 &v, int i) {
   return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));

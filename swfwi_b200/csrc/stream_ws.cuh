@@ -59,9 +59,11 @@ constexpr size_t ws_smem_bytes() {
   return ws_detail::Smem<NW * 32, D + 1>::bytes;
 }
 
-// EPI: also run a.epi (record, strip save, next injection) at the output
-// points, from the staged input row and the new values before they are stored.
-template <int ARITH, bool DAMPED, int NW, int D, bool EPI = false>
+// EPI: also run part of a.epi at the output points, from the staged input
+// row and the new values before they are stored: 1 = record, strip save and
+// next injection (forward); 2 = source subtraction, imaging and strip
+// restore (source back-step); 3 = next injection only (receiver step).
+template <int ARITH, bool DAMPED, int NW, int D, int EPI = 0>
 __global__ void __launch_bounds__((NW + 1) * 32, EPI ? (ARITH == ARITH_REF ? 4 : 5) : 1)
 fd_step_ws(StreamArgs a) {
   using namespace ws_detail;
@@ -163,13 +165,13 @@ fd_step_ws(StreamArgs a) {
   PtLine sline{0, 0, 0, 0, 0}, rline{0, 0, 0, 0, 0};
   LineCursor scur, rcur;
   bool strip_bot = false;   // this lane holds depths of the bottom strip band
-  if constexpr (EPI) {
-    if (a.epi.inj) sline = a.epi.src[shot];
-    if (a.epi.seis) rline = a.epi.rec[shot];
+  if constexpr (EPI != 0) {
+    if ((EPI != 2 && a.epi.inj) || (EPI == 2 && a.epi.sub)) sline = a.epi.src[shot];
+    if (EPI == 1 && a.epi.seis) rline = a.epi.rec[shot];
     scur.init(sline, xa);
     rcur.init(rline, xa);
     const int bz = nz - a.epi.bx0;
-    strip_bot = a.epi.strips && zg + 3 >= bz && zg < bz + 6;
+    strip_bot = ((EPI == 1 && a.epi.strips) || (EPI == 2 && a.epi.restore)) && zg + 3 >= bz && zg < bz + 6;
   }
 
   // One step.  PH is k & 15 when known at compile time, else -1.
@@ -191,6 +193,23 @@ fd_step_ws(StreamArgs a) {
     }
     const bool has_u2 = PH >= 0 || k >= 10;
     const bool has_out = PH >= 0 || k >= 12;
+    // fused imaging: this step's receiver field and image values, loaded
+    // early so their latency overlaps the update
+    float4 gimg = make_float4(0.f, 0.f, 0.f, 0.f), vimg = gimg;
+    if constexpr (EPI != 0) {
+      if (EPI == 2 && a.epi.image && has_out && outgroup) {
+        const long long o = (long long)shot * a.shot_stride + (long long)(xa - 12 + k) * P + zg;
+        if (fullgroup) {
+          gimg = ld4g(a.epi.gcurr + o);
+          vimg = ld4g(a.epi.image + o);
+        } else {
+          if (zok[0]) { gimg.x = a.epi.gcurr[o]; vimg.x = a.epi.image[o]; }
+          if (zok[1]) { gimg.y = a.epi.gcurr[o + 1]; vimg.y = a.epi.image[o + 1]; }
+          if (zok[2]) { gimg.z = a.epi.gcurr[o + 2]; vimg.z = a.epi.image[o + 2]; }
+          if (zok[3]) { gimg.w = a.epi.gcurr[o + 3]; vimg.w = a.epi.image[o + 3]; }
+        }
+      }
+    }
     if (has_u2) {
       // u2 of row r = xa - 11 + k from stages k-10 .. k
       const float *rowc = &cring[cs(-5)][0];
@@ -271,10 +290,10 @@ fd_step_ws(StreamArgs a) {
                                   get(um4, i), get(up4, i), delta);
         }
       }
-      if constexpr (EPI) {
+      if constexpr (EPI != 0) {
         const int x = xa - 12 + k;
         const int b = a.epi.bx0, w = 6;
-        if (a.epi.seis) {
+        if (EPI == 1 && a.epi.seis) {
           float *sd = a.epi.seis + (long long)shot * a.epi.seis_slot_stride;
           rcur.visit(rline, x, zg, [&](int i, int d) {
 #pragma unroll
@@ -282,7 +301,7 @@ fd_step_ws(StreamArgs a) {
               if (q == d && zok[q]) sd[i] = get(c4, q);
           });
         }
-        if (a.epi.strips) {
+        if (EPI == 1 && a.epi.strips) {
           float *sd = a.epi.strips + (long long)shot * a.epi.strip_slot_stride;
           const int nxs = nx - 2 * (b - w), nzs = nz - 6 - b;
           if (strip_bot && x >= b - w && x < nx - b + w) {
@@ -301,7 +320,7 @@ fd_step_ws(StreamArgs a) {
             }
           }
         }
-        if (a.epi.inj) {
+        if ((EPI == 1 || EPI == 3) && a.epi.inj) {
           const float *iv = a.epi.inj + (long long)shot * a.epi.inj_slot_stride;
           scur.visit(sline, x, zg, [&](int i, int d) {
             const float v = iv[(long long)i * a.epi.inj_stride];
@@ -309,6 +328,51 @@ fd_step_ws(StreamArgs a) {
             for (int q = 0; q < 4; q++)
               if (q == d && zok[q]) o[q] = __fadd_rn(o[q], v);
           });
+        }
+        if (EPI == 2 && a.epi.sub) {
+          const float *sv = a.epi.sub + (long long)shot * a.epi.sub_slot_stride;
+          scur.visit(sline, x, zg, [&](int i, int d) {
+            const float v = sv[(long long)i * a.epi.sub_stride];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (q == d && zok[q]) o[q] = __fsub_rn(o[q], v);
+          });
+        }
+        if (EPI == 2 && a.epi.image) {
+          const float sc = a.epi.scale;
+          float4 r = vimg;
+          r.x = __fsub_rn(r.x, __fmul_rn(__fmul_rn(o[0], gimg.x), sc));
+          r.y = __fsub_rn(r.y, __fmul_rn(__fmul_rn(o[1], gimg.y), sc));
+          r.z = __fsub_rn(r.z, __fmul_rn(__fmul_rn(o[2], gimg.z), sc));
+          r.w = __fsub_rn(r.w, __fmul_rn(__fmul_rn(o[3], gimg.w), sc));
+          float *ig = a.epi.image + (long long)shot * a.shot_stride + (long long)x * P + zg;
+          if (fullgroup) {
+            st4(ig, r);
+          } else {
+            if (zok[0]) ig[0] = r.x;
+            if (zok[1]) ig[1] = r.y;
+            if (zok[2]) ig[2] = r.z;
+            if (zok[3]) ig[3] = r.w;
+          }
+        }
+        if (EPI == 2 && a.epi.restore) {
+          const float *rs = a.epi.restore + (long long)shot * a.epi.restore_slot_stride;
+          const int nxs = nx - 2 * (b - w), nzs = nz - 6 - b;
+          if (strip_bot && x >= b - w && x < nx - b + w) {
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+              const int z = zg + d;
+              if (zok[d] && z >= nz - b && z < nz - b + w) o[d] = rs[(x - b + w) * w + (z - (nz - b))];
+            }
+          }
+          const int ixb = (x >= b - w && x < b) ? x - (b - w) : ((x >= nx - b && x < nx - b + w) ? w + x - (nx - b) : -1);
+          if (ixb >= 0) {
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+              const int z = zg + d;
+              if (zok[d] && z < nz - b) o[d] = rs[w * nxs + ixb * nzs + (z - 6)];
+            }
+          }
         }
       }
       float *dst = prevg + (long long)(k - 12) * P;
