@@ -229,6 +229,40 @@ __device__ __forceinline__ float update_pt(float c, float p, float r, float uc, 
   }
 }
 
+// FAST arithmetic on a pair of depths with the packed FP32x2 instructions
+// of sm_100 (each lane rounded as the scalar instruction would be).
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 lo2(const float4 &v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4 &v) { return make_float2(v.z, v.w); }
+
+// u2 of depths 2p, 2p+1 of the group (lap_pt<ARITH_FAST>'s operations in
+// the same order per lane).
+template <int P>
+__device__ __forceinline__ float2 lap_pair_fast(const float (&zn)[20], const float4 (&xm4)[6],
+                                                const float4 (&xp4)[6]) {
+  constexpr int i = 2 * P;
+  const float a[6] = {-4.0f * SWFWI_A0, SWFWI_A1, SWFWI_A2, SWFWI_A3, SWFWI_A4, SWFWI_A5};
+  float2 acc = __fmul2_rn(f2(a[0], a[0]), f2(zn[8 + i], zn[9 + i]));
+#pragma unroll
+  for (int k = 1; k <= 5; k++) {
+    const float2 zs = __fadd2_rn(f2(zn[8 + i - k], zn[9 + i - k]), f2(zn[8 + i + k], zn[9 + i + k]));
+    const float2 xs = P == 0 ? __fadd2_rn(lo2(xm4[k]), lo2(xp4[k])) : __fadd2_rn(hi2(xm4[k]), hi2(xp4[k]));
+    acc = __ffma2_rn(f2(a[k], a[k]), __fadd2_rn(zs, xs), acc);
+  }
+  return acc;
+}
+
+// Undamped FAST time update of a depth pair: out = 2c - p + r*(uc + (r/12)*lap).
+__device__ __forceinline__ float2 update_pair_fast(float2 c, float2 p, float2 r, float2 uc, float2 uzm,
+                                                   float2 uzp, float2 uxm, float2 uxp) {
+  const float2 s = __fadd2_rn(__fadd2_rn(uzm, uzp), __fadd2_rn(uxm, uxp));
+  const float2 lap = __ffma2_rn(f2(-4.0f, -4.0f), uc, s);
+  const float2 q = __fmul2_rn(r, f2(1.0f / 12.0f, 1.0f / 12.0f));
+  const float2 inc = __fmul2_rn(r, __ffma2_rn(q, lap, uc));
+  const float2 base = __ffma2_rn(f2(2.0f, 2.0f), c, __fmul2_rn(p, f2(-1.0f, -1.0f)));
+  return __fadd2_rn(base, inc);
+}
+
 // Walks a line's points row by row for a CTA whose output rows increase by
 // one per step from xa: at each row, at most one point when jx != 0 (all of
 // a vertical line's points sit on row x0).

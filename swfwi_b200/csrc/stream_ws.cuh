@@ -229,19 +229,24 @@ fd_step_ws(StreamArgs a) {
         xm4[d] = ld4(&cring[cs(-5 - d)][8 + 4 * t]);
         xp4[d] = ld4(&cring[cs(-5 + d)][8 + 4 * t]);
       }
-      float u[4];
+      if constexpr (ARITH == ARITH_FAST) {
+        const float2 u01 = lap_pair_fast<0>(zn, xm4, xp4), u23 = lap_pair_fast<1>(zn, xm4, xp4);
+        st4(&u2r[us(0)][4 * t], make_float4(u01.x, u01.y, u23.x, u23.y));
+      } else {
+        float u[4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        float xm[6], xp[6];
+        for (int i = 0; i < 4; i++) {
+          float xm[6], xp[6];
 #pragma unroll
-        for (int d = 1; d <= 5; d++) {
-          xm[d] = get(xm4[d], i);
-          xp[d] = get(xp4[d], i);
+          for (int d = 1; d <= 5; d++) {
+            xm[d] = get(xm4[d], i);
+            xp[d] = get(xp4[d], i);
+          }
+          xm[0] = xp[0] = 0.f;
+          u[i] = lap_pt<ARITH>(zn, i, xm, xp);
         }
-        xm[0] = xp[0] = 0.f;
-        u[i] = lap_pt<ARITH>(zn, i, xm, xp);
+        st4(&u2r[us(0)][4 * t], make_float4(u[0], u[1], u[2], u[3]));
       }
-      st4(&u2r[us(0)][4 * t], make_float4(u[0], u[1], u[2], u[3]));
     }
     consumer_sync<NT>();
     if (*(volatile int *)s_fail) return false;
@@ -272,12 +277,20 @@ fd_step_ws(StreamArgs a) {
         damp = coldamp || dxr != 0.f;
       }
       if (!damp) {
+        if constexpr (ARITH == ARITH_FAST) {
+          const float2 a = update_pair_fast(lo2(c4), lo2(p4), lo2(r4), lo2(uc4), f2(ucl, uc4.x), f2(uc4.y, uc4.z),
+                                            lo2(um4), lo2(up4));
+          const float2 b = update_pair_fast(hi2(c4), hi2(p4), hi2(r4), hi2(uc4), f2(uc4.y, uc4.z),
+                                            f2(uc4.w, ucr), hi2(um4), hi2(up4));
+          o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+        } else {
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          float uzm = i == 0 ? ucl : get(uc4, i - 1);
-          float uzp = i == 3 ? ucr : get(uc4, i + 1);
-          o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
-                                  get(um4, i), get(up4, i), 0.0f);
+          for (int i = 0; i < 4; i++) {
+            float uzm = i == 0 ? ucl : get(uc4, i - 1);
+            float uzp = i == 3 ? ucr : get(uc4, i + 1);
+            o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
+                                    get(um4, i), get(up4, i), 0.0f);
+          }
         }
       } else {
 #pragma unroll
