@@ -12,9 +12,9 @@ shots, 0.6 GB).
 
 Arithmetic: FP32 with FMA by default (seismograms within 1e-5, gradients
 within 1e-4 relative L2 of the reference, the tests' bounds); --arith ref
-reproduces the reference's float/double rounding bit for bit.  The forward
-and backward time loops run fused (record, strip save/restore, injections
-and imaging inside the step kernels).
+reproduces the reference's float/double rounding bit for bit.  --fuse on
+runs the time loops fused (record, strip save/restore, injections and
+imaging inside the step kernels).
 
 value: stencil point-updates executed per second over the timed steps
 (Gpts/s), device-timed with CUDA events, max over ranks.  e2e: the same
@@ -247,6 +247,7 @@ def run_kernel_mode(args):
     ss = s.scaled(nt=args.nt)
     m = S.Damp4t10d.from_survey(ss, arith=arith)
     m.set_tuning(**(json.loads(args.tuning) if args.tuning else autotune.DEFAULT))
+    m.set_fusion(args.fuse == "on")
     vel = torch.from_numpy(ex).cuda()
     m.bindVelocity(vel)
     wlt = torch.from_numpy(S.ricker_wavelet(ss.nt, ss.fm, ss.dt)).cuda()
@@ -276,6 +277,8 @@ def main():
                          "tune: print the autotuner's table")
     ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")
     ap.add_argument("--tuning", default="", help="stencil launch shape as JSON (skips the autotuner)")
+    ap.add_argument("--fuse", default="off", choices=["on", "off"],
+                    help="fused time loops (record, strips, injections, imaging inside the step kernels)")
     ap.add_argument("--strips", default="f32", choices=["f32", "f16", "bf16"],
                     help="storage of the boundary strips the gradient saves")
     ap.add_argument("--workload-nt", type=int, default=0,
@@ -307,6 +310,7 @@ def main():
     elif not args.no_tune:
         tuning, _ = autotune.tune(s, exi_h, arith)
     m.set_tuning(**tuning)
+    m.set_fusion(args.fuse == "on")
     m.set_strip_format({"f32": S.STRIP_F32, "f16": S.STRIP_F16, "bf16": S.STRIP_BF16}[args.strips])
     grad = torch.zeros((nxpad, nzpad), dtype=torch.float32, device="cuda")
 
@@ -411,7 +415,7 @@ def main():
                                        f"nt={nt}, uneven spreads 200-921"
                                        + (" (REDUCED time axis: not the benchmark)" if args.workload_nt else ""),
                            "shots": int(ns), "nt": int(nt), "grid": [int(nxpad), int(nzpad)],
-                           "arith": args.arith, "strips": args.strips, "tuning": tuning,
+                           "arith": args.arith, "strips": args.strips, "fused": args.fuse == "on", "tuning": tuning,
                            "point_updates_per_step": updates_rank / args.steps,
                            "l2": "inputs larger than L2 (strips 14 GB, fields 0.5 GB): no flush",
                            "parallelism": f"replicas{world}",

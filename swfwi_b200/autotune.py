@@ -34,6 +34,7 @@ def candidates(nz: int):
 def time_config(method, wlt, dcal, ids, cfg, repeats=2) -> float:
     """Mean stencil launch time (microseconds) of a short batched forward."""
     import swfwi_b200 as S
+    method.set_fusion(False)          # time the launch shape itself
     method.set_tuning(**cfg)
     method.forward_batch(wlt, dcal, ids)      # warm-up
     S.stats_reset()

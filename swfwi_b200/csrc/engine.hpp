@@ -78,7 +78,7 @@ class Propagator {
   int stream_xchunk = 64;     // rows per CTA
   int stream_depth = 3;       // rows ahead (3 or 5; warp-specialised 3 or 7)
   int stream_shot_major = 0;  // launch order: 0 = shots fastest
-  bool fuse = true;           // fused forward epilogue where it applies
+  bool fuse = false;          // fused time loops where they apply
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);
   void set_dims(int nxpad, int nzpad);   // padded grid; uploads geometry

@@ -48,6 +48,7 @@ def test_fused_geometries_match_reference(cuda, ref, geom):
     ex = M.expand_domain(v)
     wlt = ref.ricker(s.nt, s.fm, s.dt)
     m = S.Damp4t10d.from_survey(s)
+    m.set_fusion(True)
     vel = t(torch, ex)
     m.bindVelocity(vel)
     d = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
@@ -63,10 +64,21 @@ def test_fused_geometries_match_reference(cuda, ref, geom):
     np.testing.assert_array_equal(de.cpu().numpy(), M.ess_forward(enc))
 
 
+def test_fused_ess_gradient_bit_exact(cuda):
+    torch = cuda
+    s, m, g, _ = small_method(torch)
+    m.set_fusion(True)
+    enc = (g["wlt"][:, None] * g["ess_codes"][None, :].astype(np.float32)).astype(np.float32)
+    gr = torch.zeros(g["grad_ess"].shape, device="cuda")
+    m.calgradient_ess(t(torch, enc), t(torch, g["vsrc"]), gr)
+    np.testing.assert_array_equal(gr.cpu().numpy(), g["grad_ess"])
+
+
 def test_fused_strips_gradient_bit_exact(cuda):
     # the gradient's forward sweep saves FP32 strips in the fused step
     torch = cuda
     s, m, g, _ = small_method(torch)
+    m.set_fusion(True)
     gr = torch.zeros(g["grad_shot1"].shape, device="cuda")
     m.calgradient_fwi(t(torch, g["wlt"]), t(torch, g["vsrc"]), gr, 1)
     np.testing.assert_array_equal(gr.cpu().numpy(), g["grad_shot1"])
