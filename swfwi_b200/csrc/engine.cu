@@ -461,6 +461,13 @@ bool Propagator::line_of(const int *xs, const int *zs, int n, PtLine &out) const
   return true;
 }
 
+// The fused steps inject at a line's single depth: horizontal lines or points.
+static bool injectable(const std::vector<PtLine> &ls) {
+  for (const PtLine &l : ls)
+    if (!(l.n == 1 || l.jz == 0)) return false;
+  return true;
+}
+
 bool Propagator::shot_lines(const int *ids, int k, bool per_shot_receivers, std::vector<PtLine> &src,
                             std::vector<PtLine> &rec) const {
   src.resize(k);
@@ -497,7 +504,7 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
   const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
-                     (int)rec_lines->size() == n && bx0 >= 12 &&
+                     (int)rec_lines->size() == n && bx0 >= 12 && injectable(*src_lines) &&
                      (!save_strips || strip_format == SWFWI_STRIP_F32);
   if (fused) {
     // one launch per step: the step records its input field, saves its
@@ -563,7 +570,8 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   long long bstride = (long long)nt * bsize;
   int npts = (int)fstride;
   const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
-                     (int)rec_lines->size() == n && bx0 >= 12 && strip_format == SWFWI_STRIP_F32;
+                     (int)rec_lines->size() == n && bx0 >= 12 && strip_format == SWFWI_STRIP_F32 &&
+                     injectable(*src_lines) && injectable(*rec_lines);
   if (fused) {
     w.src_lines.upload(*src_lines, st_);
     w.rec_lines.upload(*rec_lines, st_);

@@ -270,7 +270,14 @@ struct LineCursor {
   int next_x, next_i, step_i, dx, left;
   __device__ __forceinline__ void init(const PtLine &l, int xa) {
     next_x = -1; left = 0; step_i = 0; dx = 0; next_i = 0;
-    if (l.n <= 0 || l.jx == 0) return;
+    if (l.n <= 0) return;
+    if (l.jx == 0) {   // a single point (vertical lines are visited row-wise below)
+      if (l.n == 1 && l.x0 >= xa) {
+        next_x = l.x0;
+        left = 1;
+      }
+      return;
+    }
     if (l.jx > 0) {
       int i0 = xa <= l.x0 ? 0 : (xa - l.x0 + l.jx - 1) / l.jx;
       if (i0 >= l.n) return;
