@@ -276,6 +276,10 @@ int swfwi_fwi_get_update_obj(const swfwi_fwi *h, float *obj);
 int swfwi_fwi_get_init_obj(const swfwi_fwi *h, float *obj);
 /* current padded transformed velocity, host [nxpad][nzpad] */
 int swfwi_fwi_get_velocity(swfwi_fwi *h, float *exvel);
+/* Replace the framework's velocity (host [nxpad][nzpad], transformed): an
+ * EnKF analysis moving the member, as the reference's analysis writes the
+ * members' Velocity objects in place (enkfanalyze.cpp:72-108). */
+int swfwi_fwi_set_velocity(swfwi_fwi *h, const float *exvel);
 /* sfWriteVel (damp4t10d.cpp:254-265) without the file: interior velocity in
  * m/s, host [nx][nz]. */
 int swfwi_fwi_write_vel(swfwi_fwi *h, float *vel);

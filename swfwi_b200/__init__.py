@@ -95,6 +95,7 @@ _SIGS = {
     "swfwi_cal_objective": [_vp, C.c_longlong, _dp, _vp],
     "swfwi_cal_objective_static": [_vp, C.c_longlong, C.c_int, _vp, _vp],
     "swfwi_encode_source": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
+    "swfwi_fwi_set_velocity": [_vp, _fp],
     "swfwi_damp4t10d_set_fusion": [_vp, C.c_int],
     "swfwi_rsf_get": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int],
     "swfwi_rsf_dims": [C.c_char_p, _ip, _ip, _fp, _fp],
@@ -622,6 +623,10 @@ class _Framework:
         out = np.zeros(self.shape, np.float32)
         _check(lib().swfwi_fwi_get_velocity(self.h, out.ctypes.data_as(_fp)))
         return out
+
+    def setVelocity(self, exvel: np.ndarray):
+        v, vp = _host_f32(exvel)
+        _check(lib().swfwi_fwi_set_velocity(self.h, vp))
 
     def writeVel(self) -> np.ndarray:
         nxpad, nzpad = self.shape

@@ -602,6 +602,10 @@ int swfwi_fwi_get_velocity(swfwi_fwi *h, float *exvel) {
   return guarded([&] { SWFWI_REQUIRE(exvel, "null output"); R(h).get_velocity(exvel); });
 }
 
+int swfwi_fwi_set_velocity(swfwi_fwi *h, const float *exvel) {
+  return guarded([&] { SWFWI_REQUIRE(exvel, "null input"); R(h).set_velocity(exvel); });
+}
+
 int swfwi_fwi_write_vel(swfwi_fwi *h, float *vel) {
   return guarded([&] { SWFWI_REQUIRE(vel, "null output"); R(h).write_vel(vel); });
 }

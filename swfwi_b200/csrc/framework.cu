@@ -293,6 +293,12 @@ void FwiRunner::get_velocity(float *host) {
   SWFWI_CUDA(cudaStreamSynchronize(p_.stream()));
 }
 
+void FwiRunner::set_velocity(const float *host) {
+  SWFWI_CUDA(cudaMemcpyAsync(vel_.get(), host, sizeof(float) * n_, cudaMemcpyHostToDevice, p_.stream()));
+  SWFWI_CUDA(cudaStreamSynchronize(p_.stream()));
+  p_.bind_velocity(vel_.get());   // contents changed: recompute 1/vt
+}
+
 // sfWriteVel (damp4t10d.cpp:254-265): recoverVel v = sqrt(dx^2/(dt^2 vt))
 // then the interior columns from depth 6.
 void FwiRunner::write_vel(float *host) {

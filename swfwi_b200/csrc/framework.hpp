@@ -50,6 +50,7 @@ class FwiRunner {
   void epoch(int iter);
   float update_obj = 0, init_obj = 0;
   void get_velocity(float *host);
+  void set_velocity(const float *host);   // the member moved by an EnKF analysis
   void write_vel(float *host);   // sfWriteVel without the file
   StepSearch search;
 

@@ -165,3 +165,13 @@ def small(nz=40, nx=50, nt=200, ns=3, nb=10, dx=25.0, dt=0.002, fm=10.0) -> Surv
     jsx = max(1, (nx - 2) // ns)
     return Survey(name="small", nz=nz, nx=nx, dx=dx, dt=dt, nt=nt, fm=fm, nb=nb, ns=ns,
                   sxbeg=1 + jsx // 2, jsx=jsx, ng=nx, szbeg=2, gzbeg=2)
+
+
+def gaussian_random_field(nx: int, nz: int, dx: float, corr_len: float, std: float, seed: int) -> np.ndarray:
+    """Seeded Gaussian random field [nx][nz] (float32): white noise smoothed
+    with a Gaussian of the correlation length, rescaled to `std` (the
+    ensemble members' perturbations of the EnKF workload: 200 m, 100 m/s)."""
+    rng = np.random.default_rng(seed)
+    f = smooth(rng.standard_normal((nx, nz)), corr_len / dx)
+    f = f - f.mean()
+    return (f * (std / max(f.std(), 1e-30))).astype(np.float32)
