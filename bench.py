@@ -13,8 +13,8 @@ shots, 0.6 GB).
 Arithmetic: FP32 with FMA by default (seismograms within 1e-5, gradients
 within 1e-4 relative L2 of the reference, the tests' bounds); --arith ref
 reproduces the reference's float/double rounding bit for bit.  --fuse on
-runs the time loops fused (record, strip save/restore, injections and
-imaging inside the step kernels).
+runs the backward time loop fused (source subtraction and imaging in the
+source back-step, residual injection in the receiver step).
 
 value: stencil point-updates executed per second over the timed steps
 (Gpts/s), device-timed with CUDA events, max over ranks.  e2e: the same
@@ -278,7 +278,8 @@ def main():
     ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")
     ap.add_argument("--tuning", default="", help="stencil launch shape as JSON (skips the autotuner)")
     ap.add_argument("--fuse", default="off", choices=["on", "off"],
-                    help="fused time loops (record, strips, injections, imaging inside the step kernels)")
+                    help="fused backward time loop (source subtraction, imaging and residual injection "
+                         "inside the step kernels)")
     ap.add_argument("--strips", default="f32", choices=["f32", "f16", "bf16"],
                     help="storage of the boundary strips the gradient saves")
     ap.add_argument("--workload-nt", type=int, default=0,

@@ -113,13 +113,12 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
  * depth 240, 360 or 480 = 2-4 consumer warps plus a copy warp, rows ahead 3
  * or 7); rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot
  * together. */
-/* Fused time loops (default off): where sources and receivers form regular
- * lines, the fields are FP32 and strips (if any) FP32, the forward step also
- * records the seismogram, saves the strips and injects the next source, and
- * the backward steps also subtract the source, image, restore the strips and
- * inject the next residual (warp-specialised kernel, 376-deep bands): one
- * launch per forward step, two per backward step.  Off: separate launches.
- * Results are bit-identical either way. */
+/* Fused backward time loop (default off): where sources and receivers form
+ * horizontal lines (or single points) and the fields are FP32, the source
+ * back-step also subtracts the source and images, and the receiver step
+ * also injects the next residual (warp-specialised kernel, 376-deep bands),
+ * in place of the separate source, residual and image launches.  Results
+ * are bit-identical either way. */
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on);
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest);

@@ -495,42 +495,13 @@ bool Propagator::ess_lines(int k, std::vector<PtLine> &src, std::vector<PtLine> 
 template <typename T>
 void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                              long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
-                             bool save_strips, const void *velrcp, const std::vector<PtLine> *src_lines,
-                             const std::vector<PtLine> *rec_lines) {
+                             bool save_strips, const void *velrcp) {
   ensure_work(w, n, save_strips);
   T *p0 = w.p0.get() + kStreamCoff, *p1 = w.p1.get() + kStreamCoff;
   w.p0.zero(st_);
   w.p1.zero(st_);
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
-  const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
-                     (int)rec_lines->size() == n && bx0 >= 12 && injectable(*src_lines) &&
-                     (!save_strips || strip_format == SWFWI_STRIP_F32);
-  if (fused) {
-    // one launch per step: the step records its input field, saves its
-    // strips and adds the next step's source to the field it makes
-    w.src_lines.upload(*src_lines, st_);
-    w.rec_lines.upload(*rec_lines, st_);
-    if (dcal) SWFWI_CUDA(cudaMemsetAsync(dcal, 0, sizeof(T) * (size_t)n * nt * ngrec, st_));
-    launch_inject<T>(p1, fstride, n, src, vals, slot_stride, i_stride, +1, st_);
-    for (int it = 0; it < nt; it++) {
-      Epilogue e{};
-      e.src = w.src_lines.get();
-      e.rec = w.rec_lines.get();
-      e.seis = dcal ? reinterpret_cast<float *>(dcal) + (long long)it * ngrec : nullptr;
-      e.seis_slot_stride = (long long)nt * ngrec;
-      e.strips = save_strips ? reinterpret_cast<float *>(w.strips.get()) + (long long)it * bsize : nullptr;
-      e.strip_slot_stride = bstride;
-      e.inj = it + 1 < nt ? reinterpret_cast<const float *>(vals) + (long long)(it + 1) * it_stride : nullptr;
-      e.inj_slot_stride = slot_stride;
-      e.inj_stride = i_stride;
-      e.bx0 = bx0;
-      step_fields(ar, true, p0, p1, velrcp, n, &e);
-      std::swap(p0, p1);
-    }
-    if (p0 != w.p0.get() + kStreamCoff) std::swap(w.p0, w.p1);
-    return;
-  }
   for (int it = 0; it < nt; it++) {
     // addSource -> stepForward -> swap -> recordSeis / writeBndry
     // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
@@ -570,20 +541,19 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   long long bstride = (long long)nt * bsize;
   int npts = (int)fstride;
   const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
-                     (int)rec_lines->size() == n && bx0 >= 12 && strip_format == SWFWI_STRIP_F32 &&
-                     injectable(*src_lines) && injectable(*rec_lines);
+                     (int)rec_lines->size() == n && injectable(*src_lines) && injectable(*rec_lines);
   if (fused) {
+    // two launches and the strip restore per step: the source back-step
+    // also subtracts the source and images, the receiver step also injects
+    // the next residual
     w.src_lines.upload(*src_lines, st_);
     w.rec_lines.upload(*rec_lines, st_);
-    float *strips = reinterpret_cast<float *>(w.strips.get());
     float *image = reinterpret_cast<float *>(w.image.get()) + kStreamCoff;
-    // the first step's strip restore and receiver injection; later ones are
-    // done by the previous step's kernels
-    launch_strip_read<T>(w.strips.get() + (long long)(nt - 1) * bsize, bstride, sp0, fstride, n, nxpad, nzpad,
-                         bx0, pitch, st_);
     launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)(nt - 1) * ngrec, (long long)nt * ngrec, 1, +1,
                      st_);
     for (int it = nt - 1; it >= 0; it--) {
+      launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad, nzpad, bx0,
+                           pitch, st_);
       std::swap(sp0, sp1);
       float t = dt * (float)it;
       float scale = 0.0f;
@@ -591,7 +561,6 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
       if ((double)t > 0.4) scale = 1.0f;
       else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
       else last = true;   // the reference's loop breaks after this step, before imaging
-      const bool next = !last && it >= 1;
       Epilogue e{};
       e.src = w.src_lines.get();
       e.sub = reinterpret_cast<const float *>(vals) + (long long)it * it_stride;
@@ -602,21 +571,15 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
         e.gcurr = reinterpret_cast<const float *>(gp1);
         e.scale = scale;
       }
-      if (next) {
-        e.restore = strips + (long long)(it - 1) * bsize;
-        e.restore_slot_stride = bstride;
-      }
-      e.bx0 = bx0;
       step_fields(ar, false, sp0, sp1, velrcp, n, &e);
       Epilogue r{};
       r.src = w.rec_lines.get();
-      if (next) {
+      if (!last && it >= 1) {
         r.inj = reinterpret_cast<const float *>(vsrc) + (long long)(it - 1) * ngrec;
         r.inj_slot_stride = (long long)nt * ngrec;
         r.inj_stride = 1;
       }
-      r.bx0 = bx0;
-      step_fields(ar, true, gp0, gp1, velrcp, n, &r);
+      step_fields(ar, true, gp0, gp1, velrcp, n, r.inj ? &r : nullptr);
       std::swap(gp0, gp1);
       if (last) break;
     }
@@ -666,20 +629,14 @@ void Propagator::fwi_forward(const float *wlt, float *dcal, int shot_id) {
   SWFWI_REQUIRE(shot_id >= 0 && shot_id < ns, "shot id out of range");
   PointSet src{d_src_pos_p_.get() + shot_id, 1, nullptr};
   PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
-  std::vector<PtLine> sl, rl;
-  const bool lines = shot_lines(&shot_id, 1, false, sl, rl);
-  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, rcp_of(vel_), lines ? &sl : nullptr,
-                     lines ? &rl : nullptr);
+  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, dcal, false, rcp_of(vel_));
 }
 
 void Propagator::ess_forward(const float *encsrc, float *dcal, const float *vel) {
   SWFWI_REQUIRE(encsrc && dcal, "null pointer");
   PointSet src{d_src_pos_p_.get(), ns, nullptr};
   PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
-  std::vector<PtLine> sl, rl;
-  const bool lines = ess_lines(1, sl, rl);
-  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false, rcp_of(vel ? vel : vel_),
-                     lines ? &sl : nullptr, lines ? &rl : nullptr);
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, dcal, false, rcp_of(vel ? vel : vel_));
 }
 
 void Propagator::ess_forward_members(const float *encsrc, const float *vels, int n, float *hona) {
@@ -704,10 +661,7 @@ void Propagator::ess_forward_members(const float *encsrc, const float *vels, int
       ~Restore() { v = 0; }
     } restore{vel_stride_};
     vel_stride_ = per;
-    std::vector<PtLine> sl, rl;
-    const bool lines = ess_lines(k, sl, rl);
-    run_forward<float>(w_, k, src, encsrc, ns, 0, 1, rec, ng, w_.dcal.get(), false, rcp, lines ? &sl : nullptr,
-                       lines ? &rl : nullptr);
+    run_forward<float>(w_, k, src, encsrc, ns, 0, 1, rec, ng, w_.dcal.get(), false, rcp);
     vel_stride_ = 0;
     // EssForwardModeling's dcal [nt][ng] -> the matrix column order [ng][nt]
     launch_transpose_traces(hona + (long long)c0 * nt * ng, w_.dcal.get(), nt, ng, k, st_);
@@ -742,10 +696,8 @@ void Propagator::forward_batch(const float *wlt, float *dcal, const int *ids, in
     w_.slot_shot.upload(ids + c0, k, st_);
     PointSet src{d_src_pos_p_.get(), 1, w_.slot_shot.get()};
     PointSet rec{d_rec_pos_p_.get(), ngmax, w_.slot_shot.get()};
-    std::vector<PtLine> sl, rl;
-    const bool lines = shot_lines(ids + c0, k, true, sl, rl);
     run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, dcal + (long long)c0 * nt * ngmax,
-                       false, rcp, lines ? &sl : nullptr, lines ? &rl : nullptr);
+                       false, rcp);
   }
 }
 
@@ -777,8 +729,7 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
     // field from the same source: one sweep records dcal and saves strips.
     std::vector<PtLine> sl, rl;
     const bool lines = shot_lines(ids + c0, k, true, sl, rl);
-    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), true, rcp, lines ? &sl : nullptr,
-                       lines ? &rl : nullptr);
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), true, rcp);
     launch_mute_windows(w_.win.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
                         d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
     launch_muted_residual(w_.res.get(), dobs, dn, rr, w_.dcal.get(), w_.win.get(), w_.win.get(), nt,
@@ -815,10 +766,7 @@ double Propagator::trial_objective_fwi(const float *wlt, const float *dobs, cons
     w_.res.resize((size_t)k * dn);
     w_.win.resize((size_t)k * ngmax * 2);
     w_.win2.resize((size_t)k * ngmax * 2);
-    std::vector<PtLine> sl, rl;
-    const bool lines = shot_lines(ids + c0, k, true, sl, rl);
-    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), false, rcp, lines ? &sl : nullptr,
-                       lines ? &rl : nullptr);
+    run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), false, rcp);
     // modelled data muted with the trial velocity, observed data with the
     // current one (updatesteplenop.cpp:77 and essfwiframework.cpp:205)
     launch_mute_windows(w_.win.get(), trial_vel, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
@@ -846,8 +794,7 @@ void Propagator::calgradient_ess(const float *encsrc, const float *vsrc, float *
   to_pitched(w_.image.get() + kStreamCoff, grad);
   std::vector<PtLine> sl, rl;
   const bool lines = ess_lines(1, sl, rl);
-  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp, lines ? &sl : nullptr,
-                     lines ? &rl : nullptr);
+  run_forward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, rcp);
   run_backward<float>(w_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, rcp, lines ? &sl : nullptr,
                       lines ? &rl : nullptr);
   from_pitched(grad, w_.image.get() + kStreamCoff);
@@ -864,8 +811,7 @@ void Propagator::calgradient_fwi(const float *wlt, const float *vsrc, float *gra
   to_pitched(w_.image.get() + kStreamCoff, grad);
   std::vector<PtLine> sl, rl;
   const bool lines = shot_lines(&shot_id, 1, false, sl, rl);
-  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp, lines ? &sl : nullptr,
-                     lines ? &rl : nullptr);
+  run_forward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, rcp);
   run_backward<float>(w_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, rcp, lines ? &sl : nullptr,
                       lines ? &rl : nullptr);
   from_pitched(grad, w_.image.get() + kStreamCoff);

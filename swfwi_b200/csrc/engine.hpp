@@ -169,19 +169,15 @@ class Propagator {
 
   // Forward time loop for n slots.  Source values:
   // vals + it*it_stride + slot*slot_stride + i*i_stride.
-  // With per-slot lines (src_lines, rec_lines host vectors of n) and FP32
-  // fields, the step itself records, saves FP32 strips and injects the next
-  // source (one launch per time step).
   template <typename T>
   void run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                    long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
-                   bool save_strips, const void *velrcp, const std::vector<PtLine> *src_lines = nullptr,
-                   const std::vector<PtLine> *rec_lines = nullptr);
+                   bool save_strips, const void *velrcp);
   // Backward sweep with imaging into w.image (not cleared here).
   template <typename T>
-  // With per-slot lines and FP32 fields/strips: two launches per step (the
-  // source back-step also subtracts the source, images and restores the
-  // next step's strips; the receiver step injects the next residual).
+  // With per-slot horizontal lines, FP32 fields and fusion on: the source
+  // back-step also subtracts the source and images, the receiver step also
+  // injects the next residual.
   void run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                     long long slot_stride, int i_stride, PointSet rec, int ngrec, const T *vsrc,
                     const void *velrcp, const std::vector<PtLine> *src_lines = nullptr,

@@ -683,10 +683,9 @@ static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
 template <int ARITH, bool DAMPED, int NW, int D>
 static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
   const Epilogue &e = a.epi;
-  const int mode = (e.sub || e.image || e.restore) ? 2 : ((e.seis || e.strips) ? 1 : (e.inj ? 3 : 0));
-  if (mode == 2 && (e.inj || e.seis || e.strips)) throw Error(SWFWI_ERR_BAD_ARG, "mixed fused epilogue parts");
+  const int mode = (e.sub || e.image) ? 2 : (e.inj ? 3 : 0);
+  if (mode == 2 && e.inj) throw Error(SWFWI_ERR_BAD_ARG, "mixed fused epilogue parts");
   if constexpr (NW == 3) {
-    if (mode == 1) return ws_launch<ARITH, DAMPED, NW, D, 1>(a, nslots, st);
     if (mode == 2) return ws_launch<ARITH, DAMPED, NW, D, 2>(a, nslots, st);
     if (mode == 3) return ws_launch<ARITH, DAMPED, NW, D, 3>(a, nslots, st);
   } else {

@@ -36,25 +36,18 @@ struct PtLine {
   int x0, z0, jx, jz, n;
 };
 
-// Work a streaming step does at its output points besides the update (the
-// time loops of FwiForwardModeling and calgradient, fused).  In order:
-//   seis:    recordSeis of this step's input field (the field after the
-//            reference's swap) at the `rec` points, seis[slot*stride + i];
-//   strips:  writeBndry of the same field (FP32, strip_index order);
-//   inj:     addSource of the next step into the new field at the `src`
-//            points, inj[slot*inj_slot_stride + i*inj_stride] (one float add);
-//   sub:     subSource into the new field at the `src` points (float sub);
-//   image:   image -= (new * gcurr) * scale at every output point
-//            (cross_correlation; gcurr, image laid out as the fields);
-//   restore: readBndry of the next backward step into the new field.
-// Lines are per slot; a null pointer skips that part; inj and sub are never
-// both set.
+// Work a streaming step of the backward time loop does at its output points
+// besides the update (calgradient, fused):
+//   sub:   subSource into the new field at the `src` points,
+//          sub[slot*sub_slot_stride + i*sub_stride] (one float subtraction);
+//   image: image -= (new * gcurr) * scale at every output point
+//          (cross_correlation; gcurr and image laid out as the fields);
+//   inj:   addSource of the next step into the new field at the `src`
+//          points (one float addition) -- the receiver step's residual.
+// `src` lines are per slot and horizontal (or single points); a null
+// pointer skips that part; inj is never set with sub or image.
 struct Epilogue {
-  const PtLine *src, *rec;            // [nslots]
-  float *seis;
-  long long seis_slot_stride;
-  float *strips;
-  long long strip_slot_stride;
+  const PtLine *src;                  // [nslots]
   const float *inj;
   long long inj_slot_stride;
   int inj_stride;
@@ -64,9 +57,6 @@ struct Epilogue {
   float *image;
   const float *gcurr;
   float scale;
-  const float *restore;
-  long long restore_slot_stride;
-  int bx0;                            // sponge + 6 (the strips' geometry)
 };
 
 struct StreamArgs {

@@ -17,13 +17,11 @@
 // depths outside the sponge take an undamped fast path.  Every wait is
 // bounded; on timeout the CTA raises the error flag and the producer stops.
 //
-// Fused variants (EPI != 0) add the time loop's point work without putting
-// it in the consumers' unrolled loop (whose code must stay in the
-// instruction cache): the whole producer warp records the seismogram and
-// saves the strips from the staged input rows (EPI 1) or restores the next
-// step's strips into finished output rows (EPI 2); the consumers only add or
-// subtract the source at a horizontal line's single depth (EPI 1, 2, 3) and
-// image (EPI 2).
+// Fused variants for the backward time loop keep the added work small,
+// because the unrolled loop's code must stay in the instruction cache: the
+// source back-step also subtracts the source and images (EPI 2), the
+// receiver step also injects the next residual (EPI 3); a source or
+// receiver line must be horizontal (or one point), so one lane per row adds.
 #pragma once
 #include <utility>
 #include "stream.cuh"
@@ -67,10 +65,9 @@ constexpr size_t ws_smem_bytes() {
   return ws_detail::Smem<NW * 32, D + 1>::bytes;
 }
 
-// EPI: also run part of a.epi at the output points, from the staged input
-// row and the new values before they are stored: 1 = record, strip save and
-// next injection (forward); 2 = source subtraction, imaging and strip
-// restore (source back-step); 3 = next injection only (receiver step).
+// EPI: also run part of a.epi at the output points with the new values
+// before they are stored: 2 = source subtraction and imaging (source
+// back-step); 3 = next injection (receiver step).
 template <int ARITH, bool DAMPED, int NW, int D, int EPI = 0>
 __global__ void __launch_bounds__((NW + 1) * 32, EPI ? (ARITH == ARITH_REF ? 4 : 5) : 1)
 fd_step_ws(StreamArgs a) {
@@ -114,126 +111,36 @@ fd_step_ws(StreamArgs a) {
 
   // ---------------------------------------------------------------- producer
   if (tid >= NT) {
-    const int lane = tid - NT;
-    if constexpr (EPI != 1 && EPI != 2) {
-      if (lane != 0) return;
-    }
+    if (tid != NT) return;
     const int cz = z0 - 12, pz = z0 - 4;
     const int clen = min(WC, P - kStreamCoff - cz), plen = min(WP, P - kStreamCoff - pz);
     const uint32_t cbytes = (uint32_t)clen * 4u, pbytes = (uint32_t)plen * 4u;
     const float *curr = a.curr + (long long)shot * a.shot_stride + cz;
     const float *prevw = a.prev + (long long)shot * a.shot_stride + pz;
     const float *rcpw = a.rcp + (long long)(shot / a.shots_per_vel) * a.vel_stride + pz;
-    // fused point work: this CTA's output depths, the strips' geometry
-    const int zlo = max(z0, 6), zhi = min(z0 + BZ, nz - 6);
-    const int b = a.epi.bx0, nxs = nx - 2 * (b - 6), nzs = nz - 6 - b;
-    auto strip_col = [&](int x) -> int {   // side-band column of row x, or -1
-      return (x >= b - 6 && x < b) ? x - (b - 6) : ((x >= nx - b && x < nx - b + 6) ? 6 + x - (nx - b) : -1);
-    };
-    PtLine rl{0, 0, 0, 0, 0};
-    if constexpr (EPI == 1) {
-      if (a.epi.seis) rl = a.epi.rec[shot];
-    }
-    // EPI 1: recordSeis / writeBndry of staged row s (the step's input row xa-6+s)
-    auto record_stage = [&](int s) -> bool {
-      if (!mbar_wait(&full[s & (NC - 1)], (uint32_t)((s >> 4) & 1))) return false;
-      const float *row = &cring[s & (NC - 1)][0] - cz;   // row[z] = field at depth z
-      const int x = xa - 6 + s;
-      if (a.epi.seis) {
-        float *sd = a.epi.seis + (long long)shot * a.epi.seis_slot_stride;
-        if (rl.jx != 0) {
-          const int t = x - rl.x0;
-          if (lane == 0 && t % rl.jx == 0 && t / rl.jx >= 0 && t / rl.jx < rl.n) {
-            const int i = t / rl.jx, z = rl.z0 + i * rl.jz;
-            if (z >= zlo && z < zhi) sd[i] = row[z];
-          }
-        } else if (x == rl.x0) {
-          for (int i = lane; i < rl.n; i += 32) {
-            const int z = rl.z0 + i * rl.jz;
-            if (z >= zlo && z < zhi) sd[i] = row[z];
-          }
-        }
-      }
-      if (a.epi.strips) {
-        float *sd = a.epi.strips + (long long)shot * a.epi.strip_slot_stride;
-        if (x >= b - 6 && x < nx - b + 6 && lane < 6) {
-          const int z = nz - b + lane;
-          if (z >= zlo && z < zhi) sd[(x - b + 6) * 6 + lane] = row[z];
-        }
-        const int ixb = strip_col(x);
-        if (ixb >= 0)
-          for (int z = max(6, zlo) + lane; z < min(nz - b, zhi); z += 32) sd[6 * nxs + ixb * nzs + (z - 6)] = row[z];
-      }
-      return true;
-    };
-    // EPI 2: readBndry of the next backward step into finished output row x
-    auto restore_row = [&](int x) {
-      const float *rs = a.epi.restore + (long long)shot * a.epi.restore_slot_stride;
-      float *out = a.prev + (long long)shot * a.shot_stride + (long long)x * P;
-      if (x >= b - 6 && x < nx - b + 6 && lane < 6) {
-        const int z = nz - b + lane;
-        if (z >= zlo && z < zhi) out[z] = rs[(x - b + 6) * 6 + lane];
-      }
-      const int ixb = strip_col(x);
-      if (ixb >= 0)
-        for (int z = max(6, zlo) + lane; z < min(nz - b, zhi); z += 32) out[z] = rs[6 * nxs + ixb * nzs + (z - 6)];
-    };
-    constexpr int kLag = 8;   // stages between a copy and its recording (< 16)
-    bool ok = true;
     for (int k = 0; k < K; k++) {
-      int released = -1;   // prev/vel stage whose release lane 0 waited for
-      if (lane == 0) {
-        if (*(volatile int *)s_fail) ok = false;
-        if (ok && k >= NC && !mbar_wait(&emptyc[k & (NC - 1)], (uint32_t)(((k >> 4) + 1) & 1))) ok = false;
-        const bool pv = k >= 12;
-        const int ps = (k - 12) & (NP - 1);
-        if (ok && pv && k - 12 >= NP) {
-          if (mbar_wait(&emptyp[ps], (uint32_t)((((k - 12) / NP) + 1) & 1))) released = k - NP;
-          else ok = false;
-        }
-        if (ok) {
-          uint64_t *fb = &full[k & (NC - 1)];
-          mbar_expect_tx(fb, cbytes + (pv ? 2u * pbytes : 0u));
-          bulk_g2s(&cring[k & (NC - 1)][0], curr + (long long)(xa - 6 + k) * P, cbytes, fb);
-          if (pv) {
-            long long off = (long long)(xa - 12 + k) * P;
-            bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
-            bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
-          }
-        }
+      if (*(volatile int *)s_fail) break;
+      if (k >= NC && !mbar_wait(&emptyc[k & (NC - 1)], (uint32_t)(((k >> 4) + 1) & 1))) {
+        atomicExch(a.err, 1);
+        *(volatile int *)s_fail = 1;
+        break;
       }
-      if constexpr (EPI == 1 || EPI == 2) {
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        released = __shfl_sync(0xffffffffu, released, 0);
-        if (ok && EPI == 1 && k - kLag >= 6 && k - kLag < K - 6) ok = __all_sync(0xffffffffu, record_stage(k - kLag));
-        if (ok && EPI == 2 && released >= 12 && a.epi.restore) restore_row(xa - 12 + released);
+      const bool pv = k >= 12;
+      const int ps = (k - 12) & (NP - 1);
+      if (pv && k - 12 >= NP &&
+          !mbar_wait(&emptyp[ps], (uint32_t)((((k - 12) / NP) + 1) & 1))) {
+        atomicExch(a.err, 1);
+        *(volatile int *)s_fail = 1;
+        break;
       }
-      if (!ok) {
-        if (lane == 0) {
-          atomicExch(a.err, 1);
-          *(volatile int *)s_fail = 1;
-        }
-        return;
+      uint64_t *fb = &full[k & (NC - 1)];
+      mbar_expect_tx(fb, cbytes + (pv ? 2u * pbytes : 0u));
+      bulk_g2s(&cring[k & (NC - 1)][0], curr + (long long)(xa - 6 + k) * P, cbytes, fb);
+      if (pv) {
+        long long off = (long long)(xa - 12 + k) * P;
+        bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
+        bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
       }
-    }
-    if constexpr (EPI == 1) {
-      for (int s = max(6, K - kLag); s < K - 6; s++)
-        if (!__all_sync(0xffffffffu, record_stage(s))) {
-          if (lane == 0) atomicExch(a.err, 1);
-          return;
-        }
-    }
-    if constexpr (EPI == 2) {
-      // the last prev/vel stages: wait for the consumers' release, then restore
-      if (a.epi.restore)
-        for (int q = max(12, K - NP); q < K; q++) {
-          if (!__all_sync(0xffffffffu,
-                          mbar_wait(&emptyp[(q - 12) & (NP - 1)], (uint32_t)(((q - 12) / NP) & 1)))) {
-            if (lane == 0) atomicExch(a.err, 1);
-            return;
-          }
-          restore_row(xa - 12 + q);
-        }
     }
     return;
   }
@@ -259,11 +166,10 @@ fd_step_ws(StreamArgs a) {
   const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
   // steps whose output row lies between the x ramps, where damp_x is 0
   const int k_ramp_lo = a.ramp - xa + 12, k_ramp_hi = nx - a.ramp - xa + 12;
-  // fused source work (EPI 1, 3: add; EPI 2: subtract) on a horizontal line
-  // or a single point: the lane holding the line's depth, its depth index
-  // and a cursor along the rows
-  int hit_d = -1;
-  LineCursor cur;
+  // fused source work (EPI 3: add; EPI 2: subtract) on a horizontal line or
+  // a single point: the lane holding the line's depth, its depth index and
+  // the next point's row and index (rows increase by one per step)
+  int hit_d = -1, hit_x = -1, hit_i = 0, hit_di = 0, hit_dx = 0, hit_left = 0;
   const float *hit_vals = nullptr;
   int hit_stride = 0;
   if constexpr (EPI != 0) {
@@ -272,8 +178,14 @@ fd_step_ws(StreamArgs a) {
       const PtLine l = a.epi.src[shot];
       const int d = l.z0 - zg;
       if (l.n > 0 && (l.jz == 0 || l.n == 1) && d >= 0 && d < 4 && zok[d]) {
+        LineCursor c;
+        c.init(l, xa);
         hit_d = d;
-        cur.init(l, xa);
+        hit_x = c.next_x;
+        hit_i = c.next_i;
+        hit_di = c.step_i;
+        hit_dx = c.dx;
+        hit_left = c.left;
         hit_vals = vals + (long long)shot * (EPI == 2 ? a.epi.sub_slot_stride : a.epi.inj_slot_stride);
         hit_stride = EPI == 2 ? a.epi.sub_stride : a.epi.inj_stride;
       }
@@ -410,14 +322,14 @@ fd_step_ws(StreamArgs a) {
         }
       }
       if constexpr (EPI != 0) {
-        if (hit_d >= 0 && cur.left > 0 && xa - 12 + k == cur.next_x) {
-          const float v = hit_vals[(long long)cur.next_i * hit_stride];
+        if (hit_left > 0 && xa - 12 + k == hit_x) {
+          const float v = hit_vals[(long long)hit_i * hit_stride];
 #pragma unroll
           for (int q = 0; q < 4; q++)
             if (q == hit_d) o[q] = EPI == 2 ? __fsub_rn(o[q], v) : __fadd_rn(o[q], v);
-          cur.next_i += cur.step_i;
-          cur.next_x += cur.dx;
-          cur.left--;
+          hit_i += hit_di;
+          hit_x += hit_dx;
+          hit_left--;
         }
         if (EPI == 2 && a.epi.image) {
           const float sc = a.epi.scale;
@@ -464,14 +376,6 @@ fd_step_ws(StreamArgs a) {
   }
   for (; ok && k < K; k++) ok = step(std::integral_constant<int, -1>{}, k);
 
-  if constexpr (EPI == 2) {
-    // release the last prev/vel stage too: the producer restores that row
-    // once every consumer has stored it
-    if (ok) {
-      consumer_sync<NT>();
-      if (t == 0) mbar_arrive(&emptyp[(K - 1 - 12) & (NP - 1)]);
-    }
-  }
   if (!ok && t == 0) {
     // wait (bounded) for copies the producer already issued
     for (int i = k; i < K && i < k + NC; i++) mbar_wait(&full[i & (NC - 1)], (uint32_t)((i >> 4) & 1));
