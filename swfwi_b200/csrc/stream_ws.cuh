@@ -192,6 +192,7 @@ fd_step_ws(StreamArgs a) {
     }
   }
 
+  bool next_ready = false;   // stage k+1 seen complete during step k
   // One step.  PH is k & 15 when known at compile time, else -1.
   auto step = [&](auto ph, int k) -> bool {
     constexpr int PH = decltype(ph)::value;
@@ -204,7 +205,8 @@ fd_step_ws(StreamArgs a) {
       else return (k + off) & 3;
     };
     const int fs = cs(0);
-    if (!mbar_wait(&full[fs], (uint32_t)((k >> 4) & 1))) {
+    // the previous step tested this stage already; wait only if it was not in
+    if (!next_ready && !mbar_wait(&full[fs], (uint32_t)((k >> 4) & 1))) {
       atomicExch(a.err, 1);
       *(volatile int *)s_fail = 1;
       return false;
@@ -266,6 +268,8 @@ fd_step_ws(StreamArgs a) {
         st4(&u2r[us(0)][4 * t], make_float4(u[0], u[1], u[2], u[3]));
       }
     }
+    // test the next stage now, so the answer is in by the next step
+    next_ready = k + 1 < K && mbar_test(&full[cs(1)], (uint32_t)(((k + 1) >> 4) & 1));
     consumer_sync<NT>();
     if (*(volatile int *)s_fail) return false;
     // release stage k-10's current row and stage k-1's prev/vel rows
