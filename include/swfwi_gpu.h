@@ -111,8 +111,11 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
  * depth 120, 248 or 376 = 1-3 consumer warps plus a copy warp, rows ahead 3
  * or 7), kernel 2 = streaming step with independent consumer warps (band
  * depth 240, 360 or 480 = 2-4 consumer warps plus a copy warp, rows ahead 3
- * or 7); rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot
- * together. */
+ * or 7), kernel 3 = kernel 1 with two output rows per consumer step (band
+ * depth 120, 248 or 376, rows ahead 3 or 7); rows per CTA >= 1;
+ * shots_slowest = 1 runs the CTAs of one shot together. */
+int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
+                               int rows_in_flight, int shots_slowest);
 /* Fused backward time loop (default off): where sources and receivers form
  * horizontal lines (or single points) and the fields are FP32, the source
  * back-step also subtracts the source and images, and the receiver step
@@ -120,8 +123,6 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
  * in place of the separate source, residual and image launches.  Results
  * are bit-identical either way. */
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on);
-int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
-                               int rows_in_flight, int shots_slowest);
 /* Per-shot receiver lists (uneven spreads; not in the reference, whose
  * ShotPosition is one common line): shot s has receivers
  * [offsets[s], offsets[s+1]) of gx/gz (unpadded, host arrays).  The

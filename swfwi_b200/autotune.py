@@ -23,6 +23,9 @@ def candidates(nz: int):
     for bz, rows, depth, order in itertools.product((120, 248, 376), (48, 64, 128), (3, 7), (False, True)):
         yield {"kernel": 1, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": order}
+    for bz, rows, depth in itertools.product((248, 376), (48, 64, 128), (3, 7)):
+        yield {"kernel": 3, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
+               "shots_slowest": False}
     for bz, rows, depth in itertools.product((240, 360, 480), (48, 64, 128), (3, 7)):
         yield {"kernel": 2, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": False}

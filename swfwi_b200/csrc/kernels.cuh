@@ -78,6 +78,10 @@ void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs 
 // or 7 rows ahead.
 void launch_wi_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
                     cudaStream_t st);
+// Warp-specialised step with two output rows per consumer step
+// (stream_ws2.cuh): bz = 120, 248 or 376, depth = 3 or 7 rows ahead.
+void launch_ws2_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
+                     cudaStream_t st);
 // out[s][ig*nt + it] = in[s][it*ng + ig] for nslots seismograms
 // (matrix_transpose of common.cpp:14-24 with n1 = ng, n2 = nt).
 void launch_transpose_traces(float *out, const float *in, int nt, int ng, int nslots, cudaStream_t st);
