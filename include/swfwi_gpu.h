@@ -270,6 +270,7 @@ typedef struct swfwi_fwi swfwi_fwi;
 int swfwi_fwi_create(swfwi_fwi **out, swfwi_damp4t10d *method, const float *exvel, float vmin,
                      float vmax, int nita, float maxdv, const float *wlt, const float *dobs,
                      int encoded);
+/* Destroy a framework before the propagator it was created on. */
 int swfwi_fwi_destroy(swfwi_fwi *h);
 int swfwi_fwi_epoch(swfwi_fwi *h, int iter);
 int swfwi_fwi_get_update_obj(const swfwi_fwi *h, float *obj);
@@ -374,6 +375,69 @@ int swfwi_rsf_read_shots(const char *path, float *dobs, int ns, int nt, int ng);
  * acquisition keys (fm, szbeg, ...) as header lines, or NULL. */
 int swfwi_rsf_write_shots(const char *path, const char *data_path, const float *dobs, int ns, int nt, int ng,
                           float dt, float dgx, const char *extra);
+
+/* ------------------------------------------------------------------------
+ * Learned preconditioner (no counterpart in the reference; it sits beside
+ * the plain epoch of src/fwi/fwiframework.cpp:269-356, whose line search
+ * accepts or rejects every step it proposes).  A 4-level convolutional
+ * encoder-decoder, widths w[4] (multiples of 16, at most 64; default
+ * 16/32/64/64), BF16 weights and activations, FP32 accumulation on the
+ * tensor cores, FP32 master weights, Adam.  Images are [n][H][W] with H, W
+ * multiples of 8; all tensors below are DEVICE pointers.
+ * ---------------------------------------------------------------------- */
+typedef struct swfwi_precond swfwi_precond;
+/* widths NULL: 16/32/64/64.  Weights start from a fixed seeded He-uniform
+ * draw. */
+int swfwi_precond_create(swfwi_precond **out, const int *widths);
+int swfwi_precond_destroy(swfwi_precond *h);
+int swfwi_precond_num_params(const swfwi_precond *h, long long *n);
+/* Layer l in 0..13 (3x3 convs, weights [cout][3][3][cin] then bias[cout]),
+ * 14 = the 1x1 output layer (weights [cin], bias [1]): offsets in floats
+ * into the flat parameter vector. */
+int swfwi_precond_layer(const swfwi_precond *h, int l, int *cin, int *cout, long long *w_off,
+                        long long *b_off);
+/* Flat FP32 parameters / last gradient, host.  set resets Adam. */
+int swfwi_precond_set_params(swfwi_precond *h, const float *params);
+int swfwi_precond_get_params(swfwi_precond *h, float *params);
+int swfwi_precond_get_grads(swfwi_precond *h, float *grads);
+/* x [n][H][W][3] -> y [n][H][W] (y may be NULL to keep it internal). */
+int swfwi_precond_forward(swfwi_precond *h, const float *x, float *y, int n, int H, int W,
+                          void *stream);
+/* Mean-square loss of the last forward against t [n][H][W] and the
+ * parameter gradient; loss (host) may be NULL. */
+int swfwi_precond_backward(swfwi_precond *h, const float *t, double *loss, void *stream);
+int swfwi_precond_adam_step(swfwi_precond *h, float lr, void *stream);
+/* forward + backward + Adam; loss before the step (host, may be NULL). */
+int swfwi_precond_train_step(swfwi_precond *h, const float *x, const float *t, int n, int H, int W,
+                             float lr, double *loss, void *stream);
+/* Network input of one model: the propagator's interior as an image with
+ * H = roundup8(nx) rows (x) and W = roundup8(nz) columns (depth), x3
+ * [H][W][3]: gradient / RMS, standardised transformed velocity,
+ * (log10(illum / max + 1e-6) + 3) / 3 (illum may be NULL: 0).  grad, vel,
+ * illum: [nxpad][nzpad]. */
+int swfwi_precond_features(swfwi_precond *h, const swfwi_damp4t10d *method, const float *grad,
+                           const float *vel, const float *illum, float *x3, void *stream);
+/* Training target: the interior of dv [nxpad][nzpad] at unit RMS, t [H][W]. */
+int swfwi_precond_target(swfwi_precond *h, const swfwi_damp4t10d *method, const float *dv, float *t,
+                         void *stream);
+/* features -> forward -> direction dir [nxpad][nzpad] (zero outside the
+ * interior). */
+int swfwi_precond_propose(swfwi_precond *h, const swfwi_damp4t10d *method, const float *grad,
+                          const float *vel, const float *illum, float *dir, void *stream);
+
+/* Attach a network to a plain (encoded = 0) framework (NULL detaches; the
+ * network must outlive its use).  Each epoch then tries the network's
+ * direction under its own step-length search first and keeps the step only
+ * when the search confirms an objective decrease; otherwise the plain CG
+ * step is taken.  Source illumination is accumulated every 4 steps of the
+ * gradient's forward sweep while a network is attached or collect is on. */
+int swfwi_fwi_set_preconditioner(swfwi_fwi *h, swfwi_precond *net);
+int swfwi_fwi_collect_illumination(swfwi_fwi *h, int on);
+/* The last epoch's gradient / illumination, host [nxpad][nzpad]. */
+int swfwi_fwi_get_gradient(swfwi_fwi *h, float *grad);
+int swfwi_fwi_get_illumination(swfwi_fwi *h, float *illum);
+/* last = 1 if the last epoch took the network's step; counts since create. */
+int swfwi_fwi_learned_stats(const swfwi_fwi *h, int *last, int *tried, int *accepted);
 
 #ifdef __cplusplus
 }

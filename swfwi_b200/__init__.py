@@ -122,6 +122,25 @@ _SIGS = {
     "swfwi_fwi_get_velocity": [_vp, _fp],
     "swfwi_fwi_write_vel": [_vp, _fp],
     "swfwi_fwi_last_line_search": [_vp, _fp, _fp],
+    "swfwi_precond_create": [C.POINTER(_vp), _ip],
+    "swfwi_precond_destroy": [_vp],
+    "swfwi_precond_num_params": [_vp, C.POINTER(C.c_longlong)],
+    "swfwi_precond_layer": [_vp, C.c_int, _ip, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "swfwi_precond_set_params": [_vp, _fp],
+    "swfwi_precond_get_params": [_vp, _fp],
+    "swfwi_precond_get_grads": [_vp, _fp],
+    "swfwi_precond_forward": [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, _vp],
+    "swfwi_precond_backward": [_vp, _vp, _dp, _vp],
+    "swfwi_precond_adam_step": [_vp, C.c_float, _vp],
+    "swfwi_precond_train_step": [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_float, _dp, _vp],
+    "swfwi_precond_features": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "swfwi_precond_target": [_vp, _vp, _vp, _vp, _vp],
+    "swfwi_precond_propose": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "swfwi_fwi_set_preconditioner": [_vp, _vp],
+    "swfwi_fwi_collect_illumination": [_vp, C.c_int],
+    "swfwi_fwi_get_gradient": [_vp, _fp],
+    "swfwi_fwi_get_illumination": [_vp, _fp],
+    "swfwi_fwi_learned_stats": [_vp, _ip, _ip, _ip],
     "swfwi_stats_reset": [],
     "swfwi_stats_enable_step_timing": [C.c_int],
     "swfwi_stats_read": [C.POINTER(Stats)],
@@ -634,6 +653,31 @@ class _Framework:
         out = np.zeros((nxpad - 2 * nb - 12, nzpad - nb - 12), np.float32)
         _check(lib().swfwi_fwi_write_vel(self.h, out.ctypes.data_as(_fp)))
         return out
+
+    # ---- learned preconditioner (plain FWI only) ----
+    def setPreconditioner(self, net):
+        """Attach a swfwi_b200.precond.Preconditioner (None detaches)."""
+        _check(lib().swfwi_fwi_set_preconditioner(self.h, net.h if net is not None else None))
+        self._net = net     # keep it alive while attached
+
+    def collectIllumination(self, on: bool = True):
+        _check(lib().swfwi_fwi_collect_illumination(self.h, int(on)))
+
+    def gradient(self) -> np.ndarray:
+        out = np.zeros(self.shape, np.float32)
+        _check(lib().swfwi_fwi_get_gradient(self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def illumination(self) -> np.ndarray:
+        out = np.zeros(self.shape, np.float32)
+        _check(lib().swfwi_fwi_get_illumination(self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def learnedStats(self):
+        """(last epoch took the network's step, tried, accepted)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().swfwi_fwi_learned_stats(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return bool(a.value), b.value, c.value
 
     def lastLineSearch(self):
         a = np.zeros(4, np.float32)

@@ -4,6 +4,7 @@
 #include <memory>
 #include <string>
 #include "framework.hpp"
+#include "precond.hpp"
 
 namespace swfwi {
 thread_local std::string g_last_error;
@@ -19,6 +20,10 @@ struct swfwi_damp4t10d {
 
 struct swfwi_fwi {
   std::unique_ptr<FwiRunner> r;
+};
+
+struct swfwi_precond {
+  std::unique_ptr<Preconditioner> n;
 };
 
 namespace {
@@ -45,6 +50,12 @@ FwiRunner &R(swfwi_fwi *h) {
 const FwiRunner &R(const swfwi_fwi *h) {
   if (!h || !h->r) throw Error(SWFWI_ERR_BAD_ARG, "null framework handle");
   return *h->r;
+}
+
+Preconditioner &NET(swfwi_precond *h, void *stream) {
+  if (!h || !h->n) throw Error(SWFWI_ERR_BAD_ARG, "null preconditioner handle");
+  h->n->set_stream(as_stream(stream));
+  return *h->n;
 }
 
 StepArgs drop_in_args(float *prev, const float *curr, const float *vel, int nx, int nz, int nb,
@@ -643,6 +654,143 @@ int swfwi_fwi_last_line_search(const swfwi_fwi *h, float *alpha, float *obj) {
       alpha[i] = R(h).search.alpha[i];
       obj[i] = R(h).search.obj[i];
     }
+  });
+}
+
+// ------------------------------------------------------- learned preconditioner
+int swfwi_precond_create(swfwi_precond **out, const int *widths) {
+  return guarded([&] {
+    SWFWI_REQUIRE(out, "null output");
+    *out = nullptr;
+    const int def[4] = {16, 32, 64, 64};
+    std::unique_ptr<swfwi_precond> h(new swfwi_precond);
+    h->n.reset(new Preconditioner(widths ? widths : def));
+    *out = h.release();
+  });
+}
+
+int swfwi_precond_destroy(swfwi_precond *h) {
+  return guarded([&] { delete h; });
+}
+
+int swfwi_precond_num_params(const swfwi_precond *h, long long *n) {
+  return guarded([&] {
+    SWFWI_REQUIRE(h && h->n && n, "null argument");
+    *n = h->n->num_params();
+  });
+}
+
+int swfwi_precond_layer(const swfwi_precond *h, int l, int *cin, int *cout, long long *w_off,
+                        long long *b_off) {
+  return guarded([&] {
+    SWFWI_REQUIRE(h && h->n && cin && cout && w_off && b_off, "null argument");
+    SWFWI_REQUIRE(l >= 0 && l <= Preconditioner::kConvs, "layer out of range");
+    if (l < Preconditioner::kConvs) {
+      const ConvSpec &c = h->n->convs()[l];
+      *cin = c.cin; *cout = c.cout; *w_off = c.w_off; *b_off = c.b_off;
+    } else {
+      *cin = h->n->convs()[Preconditioner::kConvs - 1].cout; *cout = 1;
+      *w_off = h->n->out_w_off(); *b_off = h->n->out_b_off();
+    }
+  });
+}
+
+int swfwi_precond_set_params(swfwi_precond *h, const float *params) {
+  return guarded([&] { NET(h, nullptr).set_params(params); });
+}
+
+int swfwi_precond_get_params(swfwi_precond *h, float *params) {
+  return guarded([&] { SWFWI_REQUIRE(params, "null output"); NET(h, nullptr).get_params(params); });
+}
+
+int swfwi_precond_get_grads(swfwi_precond *h, float *grads) {
+  return guarded([&] { SWFWI_REQUIRE(grads, "null output"); NET(h, nullptr).get_grads(grads); });
+}
+
+int swfwi_precond_forward(swfwi_precond *h, const float *x, float *y, int n, int H, int W,
+                          void *stream) {
+  return guarded([&] {
+    NET(h, stream).forward(x, y, n, H, W);
+    check_launch();
+  });
+}
+
+int swfwi_precond_backward(swfwi_precond *h, const float *t, double *loss, void *stream) {
+  return guarded([&] {
+    const double l = NET(h, stream).backward(t);
+    if (loss) *loss = l;
+  });
+}
+
+int swfwi_precond_adam_step(swfwi_precond *h, float lr, void *stream) {
+  return guarded([&] {
+    SWFWI_REQUIRE(lr > 0 && std::isfinite(lr), "bad learning rate");
+    NET(h, stream).adam_step(lr);
+    check_launch();
+  });
+}
+
+int swfwi_precond_train_step(swfwi_precond *h, const float *x, const float *t, int n, int H, int W,
+                             float lr, double *loss, void *stream) {
+  return guarded([&] {
+    SWFWI_REQUIRE(lr > 0 && std::isfinite(lr), "bad learning rate");
+    const double l = NET(h, stream).train_step(x, t, n, H, W, lr);
+    if (loss) *loss = l;
+  });
+}
+
+int swfwi_precond_features(swfwi_precond *h, const swfwi_damp4t10d *method, const float *grad,
+                           const float *vel, const float *illum, float *x3, void *stream) {
+  return guarded([&] {
+    const Propagator &p = P(method);
+    NET(h, stream).features(grad, vel, illum, p.nxpad, p.nzpad, p.bx0, p.bxn, p.bz0, p.bzn, x3);
+    check_launch();
+  });
+}
+
+int swfwi_precond_target(swfwi_precond *h, const swfwi_damp4t10d *method, const float *dv, float *t,
+                         void *stream) {
+  return guarded([&] {
+    const Propagator &p = P(method);
+    NET(h, stream).target(dv, p.nxpad, p.nzpad, p.bx0, p.bxn, p.bz0, p.bzn, t);
+    check_launch();
+  });
+}
+
+int swfwi_precond_propose(swfwi_precond *h, const swfwi_damp4t10d *method, const float *grad,
+                          const float *vel, const float *illum, float *dir, void *stream) {
+  return guarded([&] {
+    const Propagator &p = P(method);
+    NET(h, stream).propose(grad, vel, illum, p.nxpad, p.nzpad, p.bx0, p.bxn, p.bz0, p.bzn, dir);
+    check_launch();
+  });
+}
+
+int swfwi_fwi_set_preconditioner(swfwi_fwi *h, swfwi_precond *net) {
+  return guarded([&] {
+    FwiRunner &r = R(h);
+    SWFWI_REQUIRE(!net || net->n, "null preconditioner handle");
+    r.set_preconditioner(net ? net->n.get() : nullptr);
+  });
+}
+
+int swfwi_fwi_collect_illumination(swfwi_fwi *h, int on) {
+  return guarded([&] { R(h).set_collect_illumination(on != 0); });
+}
+
+int swfwi_fwi_get_gradient(swfwi_fwi *h, float *grad) {
+  return guarded([&] { SWFWI_REQUIRE(grad, "null output"); R(h).get_gradient(grad); });
+}
+
+int swfwi_fwi_get_illumination(swfwi_fwi *h, float *illum) {
+  return guarded([&] { SWFWI_REQUIRE(illum, "null output"); R(h).get_illumination(illum); });
+}
+
+int swfwi_fwi_learned_stats(const swfwi_fwi *h, int *last, int *tried, int *accepted) {
+  return guarded([&] {
+    SWFWI_REQUIRE(last && tried && accepted, "null output");
+    const FwiRunner &r = R(h);
+    *last = r.last_step_learned; *tried = r.learned_tried; *accepted = r.learned_accepted;
   });
 }
 

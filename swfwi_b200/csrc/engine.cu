@@ -5,6 +5,7 @@
 #include <cstring>
 #include <utility>
 #include "engine.hpp"
+#include "precond.hpp"
 
 namespace swfwi {
 
@@ -520,6 +521,9 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
       else
         launch_strip_write<T>(w.strips.get() + (long long)it * bsize, bstride, p0, fstride, n, nxpad,
                               nzpad, bx0, pitch, st_);
+      if (sizeof(T) == 4 && illum && it % std::max(illum_every, 1) == 0)
+        launch_illum_accum(illum, reinterpret_cast<const float *>(p0), fstride, n, nxpad, nzpad, pitch,
+                           st_);
     }
   }
   // leave the final (current, next) pair for a backward sweep
@@ -540,7 +544,10 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   T *gp0 = w.g0.get() + kStreamCoff, *gp1 = w.g1.get() + kStreamCoff;
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
-  int npts = (int)fstride;
+  // image every point of the pitched field, nxpad rows of pitch floats from
+  // kStreamCoff on: (slot j) j*fstride + kStreamCoff + [0, nxpad*pitch)
+  // stays inside the slot's fstride floats
+  const int npts = nxpad * pitch;
   const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
                      (int)rec_lines->size() == n && injectable(*src_lines) && injectable(*rec_lines);
   if (fused) {

@@ -79,11 +79,23 @@ class Propagator {
   int stream_depth = 3;       // rows ahead (3 or 5; warp-specialised 3 or 7)
   int stream_shot_major = 0;  // launch order: 0 = shots fastest
   bool fuse = false;          // fused time loops where they apply
+  // Source illumination: while set, the forward sweeps that save strips
+  // add sum over slots of p^2 into illum [nxpad][nzpad] every illum_every
+  // steps (the caller zeroes it).
+  float *illum = nullptr;
+  int illum_every = 4;
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);
   void set_dims(int nxpad, int nzpad);   // padded grid; uploads geometry
   void expand_domain(const float *vel, float *exvel) const;   // host
   void bind_velocity(const float *exvel_dev);
+  // Forget the bound velocity if it is v (its owner is going away).
+  void unbind_velocity(const float *v) {
+    if (vel_ == v) {
+      vel_ = nullptr;
+      rcp_for_ = nullptr;
+    }
+  }
   const float *velocity() const { return vel_; }
 
   // ---- reference-compatible single-field operations (device pointers,

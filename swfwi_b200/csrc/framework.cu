@@ -3,6 +3,7 @@
 #include <cmath>
 #include <numeric>
 #include "framework.hpp"
+#include "precond.hpp"
 
 namespace swfwi {
 
@@ -158,6 +159,8 @@ FwiRunner::FwiRunner(Propagator &p, const float *exvel_host, float vmin, float v
   SWFWI_REQUIRE(vmax_t_ > vmin_t_, "vmax must exceed vmin");
   search.nita = nita;
   search.maxdv = maxdv;
+  learned_search.nita = nita;
+  learned_search.maxdv = maxdv;
   n_ = p.nxpad * p.nzpad;
   cudaStream_t st = p.stream();
   vel_.upload(exvel_host, n_, st);
@@ -212,11 +215,26 @@ void FwiRunner::plain_epoch(int iter) {
   cudaStream_t st = p_.stream();
   p_.bind_velocity(vel_.get());
   std::vector<double> obj(p_.ns);
-  p_.gradient_batch(wlt_.get(), dobs_.get(), ids_.data(), p_.ns, g_.get(), obj.data());
+  const bool want_illum = collect_illum_ || net_;
+  if (want_illum) {
+    illum_.resize(n_);
+    illum_.zero(st);
+    p_.illum = illum_.get();
+  }
+  try {
+    p_.gradient_batch(wlt_.get(), dobs_.get(), ids_.data(), p_.ns, g_.get(), obj.data());
+  } catch (...) {
+    p_.illum = nullptr;
+    throw;
+  }
+  p_.illum = nullptr;
   float obj1 = 0.0f;
   for (double o : obj) obj1 += (float)o;
   if (iter == 0) init_obj = obj1;
-  update_grad(iter);
+  update_grad(restart_cg_ ? 0 : iter);
+  restart_cg_ = false;
+  last_step_learned = 0;
+  if (net_ && try_learned_step(obj1)) return;
 
   launch_max_alpha(reinterpret_cast<float *>(scratch_.get()), vel_.get(), dir_.get(), n_, p_.dt,
                    p_.dx, search.maxdv, st);
@@ -235,6 +253,53 @@ void FwiRunner::plain_epoch(int iter) {
   launch_refill_boundary(vel_.get(), p_.nxpad, p_.nzpad, p_.bz0, p_.bzn, p_.bx0, p_.bxn, st);
   p_.bind_velocity(vel_.get());
   SWFWI_CUDA(cudaStreamSynchronize(st));
+}
+
+bool FwiRunner::try_learned_step(float obj1) {
+  cudaStream_t st = p_.stream();
+  learned_tried++;
+  ldir_.resize(n_);
+  net_->set_stream(st);
+  net_->propose(g_.get(), vel_.get(), illum_.get(), p_.nxpad, p_.nzpad, p_.bx0, p_.bxn, p_.bz0, p_.bzn,
+                ldir_.get());
+  launch_max_alpha(reinterpret_cast<float *>(scratch_.get()), vel_.get(), ldir_.get(), n_, p_.dt, p_.dx,
+                   learned_search.maxdv, st);
+  float a2max = 0;
+  SWFWI_CUDA(cudaMemcpyAsync(&a2max, scratch_.get(), sizeof(float), cudaMemcpyDeviceToHost, st));
+  SWFWI_CUDA(cudaStreamSynchronize(st));
+  if (!(a2max > 0.0f) || !std::isfinite(a2max)) return false;
+  auto f = [&](float alpha) -> float {
+    launch_update_vel(trial_.get(), vel_.get(), ldir_.get(), n_, alpha, vmin_t_, vmax_t_, st);
+    return (float)p_.trial_objective_fwi(wlt_.get(), dobs_.get(), ids_.data(), p_.ns, trial_.get());
+  };
+  float objv = 0;
+  const float step = learned_search.calsteplen(f, obj1, 2 * a2max, objv);
+  const float tried_best = std::min(learned_search.obj[1], learned_search.obj[2]);
+  if (!(std::isfinite(objv) && objv < obj1 && tried_best < obj1 && step > 0.0f)) {
+    // rejected: the next search along the network starts from scratch
+    learned_search.preserved_init = false;
+    return false;
+  }
+  update_obj = objv;
+  launch_update_vel(vel_.get(), vel_.get(), ldir_.get(), n_, step, vmin_t_, vmax_t_, st);
+  launch_refill_boundary(vel_.get(), p_.nxpad, p_.nzpad, p_.bz0, p_.bzn, p_.bx0, p_.bxn, st);
+  p_.bind_velocity(vel_.get());
+  SWFWI_CUDA(cudaStreamSynchronize(st));
+  restart_cg_ = true;
+  last_step_learned = 1;
+  learned_accepted++;
+  return true;
+}
+
+void FwiRunner::get_gradient(float *host) {
+  SWFWI_CUDA(cudaMemcpyAsync(host, g_.get(), sizeof(float) * n_, cudaMemcpyDeviceToHost, p_.stream()));
+  SWFWI_CUDA(cudaStreamSynchronize(p_.stream()));
+}
+
+void FwiRunner::get_illumination(float *host) {
+  SWFWI_REQUIRE(illum_.size() == (size_t)n_, "no illumination recorded: enable collection first");
+  SWFWI_CUDA(cudaMemcpyAsync(host, illum_.get(), sizeof(float) * n_, cudaMemcpyDeviceToHost, p_.stream()));
+  SWFWI_CUDA(cudaStreamSynchronize(p_.stream()));
 }
 
 // EssFwiFramework::epoch (essfwiframework.cpp:191-239).

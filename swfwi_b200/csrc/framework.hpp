@@ -43,16 +43,37 @@ struct StepSearch {
                    float &objval);
 };
 
+class Preconditioner;
+
 class FwiRunner {
  public:
   FwiRunner(Propagator &p, const float *exvel_host, float vmin, float vmax, int nita, float maxdv,
             const float *wlt_host, const float *dobs_host, bool encoded);
+  ~FwiRunner() { p_.unbind_velocity(vel_.get()); }
   void epoch(int iter);
   float update_obj = 0, init_obj = 0;
   void get_velocity(float *host);
   void set_velocity(const float *host);   // the member moved by an EnKF analysis
   void write_vel(float *host);   // sfWriteVel without the file
   StepSearch search;
+
+  // Learned preconditioner (not owned; null = plain FWI).  With a network
+  // set, each plain epoch first searches along the network's direction with
+  // its own copy of the step-length search and takes that step only when
+  // the search confirms an objective decrease (its vertex objective and an
+  // evaluated trial both below the current objective); otherwise it takes
+  // the plain step.  After a learned step the next CG direction restarts.
+  void set_preconditioner(Preconditioner *net) {
+    SWFWI_REQUIRE(!net || !encoded_, "the learned step applies to plain FWI");
+    net_ = net;
+  }
+  // Accumulate the source illumination during the gradient's forward sweep
+  // (always on while a network is set).
+  void set_collect_illumination(bool on) { collect_illum_ = on; }
+  void get_gradient(float *host);       // the last epoch's gradient
+  void get_illumination(float *host);   // the last epoch's illumination
+  int last_step_learned = 0, learned_tried = 0, learned_accepted = 0;
+  StepSearch learned_search;
 
  private:
   Propagator &p_;
@@ -61,6 +82,11 @@ class FwiRunner {
   int n_;                   // nxpad*nzpad
   DevBuf<float> vel_, trial_, g_, g0_, dir_, wlt_, dobs_, encsrc_, encobs_, dcal_, vsrc_, res_;
   DevBuf<int> codes_;
+  DevBuf<float> illum_, ldir_;
+  Preconditioner *net_ = nullptr;
+  bool collect_illum_ = false;
+  bool restart_cg_ = false;
+  bool try_learned_step(float obj1);
   DevBuf<double> scratch_;
   RandomCodes codes_gen_;
   std::vector<int> ids_;

@@ -223,6 +223,7 @@ __global__ void k_mute_windows(int *win, const float *vel, int nxpad, int nzpad,
   int gz0 = rz[0];
   int gmin = sz < gz0 ? sz : gz0, gmax = sz > gz0 ? sz : gz0;
   int rows = gmax - gmin + 1;
+  if (gmin < 0 || gmax >= nzpad) rows = 0;   // positions off the grid: mute nothing
   long long total = (long long)nxpad * rows;
   float acc = 0.0f;
   for (long long base = 0; base < total; base += CH) {
@@ -237,13 +238,13 @@ __global__ void k_mute_windows(int *win, const float *vel, int nxpad, int nzpad,
       for (int j = 0; j < cnt; j++) acc = __fadd_rn(acc, buf[j]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) s_avg = __fdiv_rn(acc, (float)(nxpad * rows));
+  if (threadIdx.x == 0) s_avg = rows > 0 ? __fdiv_rn(acc, (float)(nxpad * rows)) : -1.0f;
   __syncthreads();
   float avg = s_avg;
   for (int ig = threadIdx.x; ig < ng; ig += blockDim.x) {
     int gx = rx[ig], gz = rz[ig];
     int start = nt, end = nt;   // an unused receiver entry mutes nothing
-    if (gx >= 0) {
+    if (gx >= 0 && avg >= 0.0f) {
       float dist = (float)((gx - sx) * (gx - sx) + (gz - sz) * (gz - sz));
       int t = (int)__fsqrt_rn(__fmul_rn(dist, avg));
       start = t;

@@ -1,0 +1,863 @@
+// Learned preconditioner: BF16 tensor-core convolutions (forward, data
+// gradient, weight gradient), the encoder-decoder around them, its training
+// step and the features/scatter between the padded model grid and the
+// network's image.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include "kernels.cuh"
+#include "precond.hpp"
+
+namespace swfwi {
+namespace {
+
+using bf16 = __nv_bfloat16;
+constexpr int kEw = 256;   // threads of the elementwise kernels
+
+inline void noted() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+inline unsigned blocks_for(long long n, int threads = kEw) {
+  long long b = (n + threads - 1) / threads;
+  return (unsigned)std::max(1LL, std::min(b, 148LL * 64));
+}
+
+__device__ __forceinline__ uint32_t ldu32(const bf16 *p) {
+  return __ldg(reinterpret_cast<const unsigned int *>(p));
+}
+
+// D = A(16x16, row) * B(16x8, col) + D, bf16 operands, f32 accumulate.
+// Fragment layout (PTX ISA, mma.m16n8k16 .bf16): with g = lane/4, t = lane%4,
+// a0 = A[g][2t..2t+1], a1 = A[g+8][2t..], a2 = A[g][2t+8..], a3 = A[g+8][2t+8..],
+// b0 = B[2t..2t+1][g], b1 = B[2t+8..2t+9][g],
+// c0,c1 = D[g][2t..2t+1], c2,c3 = D[g+8][2t..2t+1]; lower k in the low half.
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// ---------------------------------------------------------------- 3x3 conv
+// Implicit GEMM: M = pixels (16 consecutive columns of one image row per
+// warp), N = output channels (8*NJ per CTA), K = 9 taps x cin (16 channels
+// of one tap per mma).  Zero padding at the image edges.  F32: FP32 output
+// without bias (the data gradient), else BF16 output with bias and ReLU.
+template <int NJ, bool F32>
+__global__ void __launch_bounds__(128) k_conv3x3(const bf16 *__restrict__ in, int cin,
+                                                 const bf16 *__restrict__ w,
+                                                 const float *__restrict__ bias, void *out, int accum,
+                                                 int cout, int H, int W) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int nh = blockIdx.y;
+  const int n = nh / H, h = nh - n * H;
+  const int w0 = blockIdx.x * 64 + warp * 16;
+  if (w0 >= W) return;   // whole warp
+  const int co0 = blockIdx.z * (8 * NJ);
+  const int wa = w0 + g, wb = w0 + g + 8;
+  float acc[NJ][4];
+#pragma unroll
+  for (int j = 0; j < NJ; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+  for (int ky = 0; ky < 3; ky++) {
+    const int hh = h + ky - 1;
+    const bool hok = hh >= 0 && hh < H;
+    const bf16 *row = in + (long long)(n * H + (hok ? hh : 0)) * W * cin;
+    for (int kx = 0; kx < 3; kx++) {
+      const int xa = wa + kx - 1, xb = wb + kx - 1;
+      const bool oka = hok && wa < W && xa >= 0 && xa < W;
+      const bool okb = hok && wb < W && xb >= 0 && xb < W;
+      const bf16 *pa = row + (long long)(oka ? xa : 0) * cin + 2 * t;
+      const bf16 *pb = row + (long long)(okb ? xb : 0) * cin + 2 * t;
+      const bf16 *wt = w + ((long long)(co0 + g) * 9 + ky * 3 + kx) * cin + 2 * t;
+      for (int c0 = 0; c0 < cin; c0 += 16) {
+        const uint32_t a0 = oka ? ldu32(pa + c0) : 0u, a2 = oka ? ldu32(pa + c0 + 8) : 0u;
+        const uint32_t a1 = okb ? ldu32(pb + c0) : 0u, a3 = okb ? ldu32(pb + c0 + 8) : 0u;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+          const bf16 *wj = wt + (long long)j * 8 * 9 * cin + c0;
+          mma_bf16(acc[j], a0, a1, a2, a3, ldu32(wj), ldu32(wj + 8));
+        }
+      }
+    }
+  }
+  const long long pixa = (long long)nh * W + wa, pixb = (long long)nh * W + wb;
+#pragma unroll
+  for (int j = 0; j < NJ; j++) {
+    const int co = co0 + j * 8 + 2 * t;
+    if constexpr (F32) {
+      float2 *o = reinterpret_cast<float2 *>(out);
+      if (wa < W) {
+        float2 v = make_float2(acc[j][0], acc[j][1]);
+        if (accum) { float2 q = o[(pixa * cout + co) / 2]; v.x += q.x; v.y += q.y; }
+        o[(pixa * cout + co) / 2] = v;
+      }
+      if (wb < W) {
+        float2 v = make_float2(acc[j][2], acc[j][3]);
+        if (accum) { float2 q = o[(pixb * cout + co) / 2]; v.x += q.x; v.y += q.y; }
+        o[(pixb * cout + co) / 2] = v;
+      }
+    } else {
+      uint32_t *o = reinterpret_cast<uint32_t *>(out);
+      const float b0 = bias[co], b1 = bias[co + 1];
+      if (wa < W)
+        o[(pixa * cout + co) / 2] = pack_bf16(fmaxf(acc[j][0] + b0, 0.0f), fmaxf(acc[j][1] + b1, 0.0f));
+      if (wb < W)
+        o[(pixb * cout + co) / 2] = pack_bf16(fmaxf(acc[j][2] + b0, 0.0f), fmaxf(acc[j][3] + b1, 0.0f));
+    }
+  }
+}
+
+// Weight gradient of one tap: dw[co][tap][ci] += sum_p dz[p][co] x[p + tap][ci].
+// GEMM M = output channels (16 per warp, 64 per CTA), N = input channels
+// (8*NJ), K = pixels (32 per stage, staged transposed in shared memory so
+// that fragment pairs run along pixels).  FP32 atomics into dw at the end.
+template <int NJ>
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad(const bf16 *__restrict__ dz, int cout,
+                                                       const bf16 *__restrict__ x,
+                                                       float *__restrict__ dw, int N, int H, int W,
+                                                       int pix_per_cta) {
+  constexpr int CIN = 8 * NJ, KS = 32, LD = 40;
+  __shared__ __align__(16) uint16_t zt[64][LD];
+  __shared__ __align__(16) uint16_t xt[CIN][LD];
+  const int tap = blockIdx.y, ky = tap / 3, kx = tap - 3 * (tap / 3);
+  const int co0 = blockIdx.z * 64;
+  const int ncol = min(64, cout - co0);
+  const long long P = (long long)N * H * W;
+  const long long p_begin = (long long)blockIdx.x * pix_per_cta;
+  const long long p_end = min(P, p_begin + pix_per_cta);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const bool mw = warp * 16 < ncol;
+  const int HW = H * W;
+  float acc[NJ][4];
+#pragma unroll
+  for (int j = 0; j < NJ; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+  for (long long pb = p_begin; pb < p_end; pb += KS) {
+    const int zpairs = ncol / 2;
+    for (int e = threadIdx.x; e < KS * zpairs; e += 128) {
+      const int i = e / zpairs, cp = e - i * zpairs;
+      const long long p = pb + i;
+      uint32_t v = 0;
+      if (p < p_end) v = ldu32(dz + p * cout + co0 + 2 * cp);
+      zt[2 * cp][i] = (uint16_t)(v & 0xffffu);
+      zt[2 * cp + 1][i] = (uint16_t)(v >> 16);
+    }
+    constexpr int xpairs = CIN / 2;
+    for (int e = threadIdx.x; e < KS * xpairs; e += 128) {
+      const int i = e / xpairs, cp = e - i * xpairs;
+      const long long p = pb + i;
+      uint32_t v = 0;
+      if (p < p_end) {
+        const int n = (int)(p / HW);
+        const int r = (int)(p - (long long)n * HW);
+        const int h = r / W, w = r - h * W;
+        const int hh = h + ky - 1, ww = w + kx - 1;
+        if (hh >= 0 && hh < H && ww >= 0 && ww < W)
+          v = ldu32(x + ((long long)(n * H + hh) * W + ww) * CIN + 2 * cp);
+      }
+      xt[2 * cp][i] = (uint16_t)(v & 0xffffu);
+      xt[2 * cp + 1][i] = (uint16_t)(v >> 16);
+    }
+    __syncthreads();
+    if (mw) {
+      const int r0 = warp * 16 + g;
+#pragma unroll
+      for (int ks = 0; ks < KS; ks += 16) {
+        const uint32_t a0 = *reinterpret_cast<const uint32_t *>(&zt[r0][ks + 2 * t]);
+        const uint32_t a1 = *reinterpret_cast<const uint32_t *>(&zt[r0 + 8][ks + 2 * t]);
+        const uint32_t a2 = *reinterpret_cast<const uint32_t *>(&zt[r0][ks + 2 * t + 8]);
+        const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&zt[r0 + 8][ks + 2 * t + 8]);
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+          const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&xt[j * 8 + g][ks + 2 * t]);
+          const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&xt[j * 8 + g][ks + 2 * t + 8]);
+          mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!mw) return;
+  const int coa = co0 + warp * 16 + g, cob = coa + 8;
+#pragma unroll
+  for (int j = 0; j < NJ; j++) {
+    const int ci = j * 8 + 2 * t;
+    atomicAdd(dw + ((long long)coa * 9 + tap) * CIN + ci, acc[j][0]);
+    atomicAdd(dw + ((long long)coa * 9 + tap) * CIN + ci + 1, acc[j][1]);
+    atomicAdd(dw + ((long long)cob * 9 + tap) * CIN + ci, acc[j][2]);
+    atomicAdd(dw + ((long long)cob * 9 + tap) * CIN + ci + 1, acc[j][3]);
+  }
+}
+
+// --------------------------------------------------------- elementwise parts
+__global__ void k_pack3(const float *__restrict__ x3, bf16 *__restrict__ x16, long long P) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
+       p += (long long)gridDim.x * blockDim.x) {
+    uint4 lo, hi;
+    lo.x = pack_bf16(x3[3 * p], x3[3 * p + 1]);
+    lo.y = pack_bf16(x3[3 * p + 2], 0.0f);
+    lo.z = lo.w = 0u;
+    hi.x = hi.y = hi.z = hi.w = 0u;
+    uint4 *o = reinterpret_cast<uint4 *>(x16 + p * 16);
+    o[0] = lo;
+    o[1] = hi;
+  }
+}
+
+__global__ void k_pool(const bf16 *__restrict__ in, bf16 *__restrict__ out, int N, int H, int W,
+                       int C) {
+  const int Ho = H / 2, Wo = W / 2, cp = C / 2;
+  const long long total = (long long)N * Ho * Wo * cp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = 2 * (int)(e % cp);
+    long long q = e / cp;
+    const int wo = (int)(q % Wo);
+    q /= Wo;
+    const int ho = (int)(q % Ho);
+    const int n = (int)(q / Ho);
+    const long long r0 = ((long long)(n * H + 2 * ho) * W + 2 * wo) * C + c;
+    const long long r1 = r0 + (long long)W * C;
+    const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162 *>(in + r0);
+    const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162 *>(in + r0 + C);
+    const __nv_bfloat162 d = *reinterpret_cast<const __nv_bfloat162 *>(in + r1);
+    const __nv_bfloat162 f = *reinterpret_cast<const __nv_bfloat162 *>(in + r1 + C);
+    const float lo = (((__low2float(a) + __low2float(b)) + __low2float(d)) + __low2float(f)) * 0.25f;
+    const float hi = (((__high2float(a) + __high2float(b)) + __high2float(d)) + __high2float(f)) * 0.25f;
+    reinterpret_cast<uint32_t *>(out)[(((long long)(n * Ho + ho) * Wo + wo) * C + c) / 2] = pack_bf16(lo, hi);
+  }
+}
+
+// din (fine grid) += 0.25 dout (coarse grid)
+__global__ void k_pool_bwd(const float *__restrict__ dout, float *__restrict__ din, int N, int H,
+                           int W, int C) {
+  const long long total = (long long)N * H * W * C;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e % C);
+    long long q = e / C;
+    const int w = (int)(q % W);
+    q /= W;
+    const int h = (int)(q % H);
+    const int n = (int)(q / H);
+    din[e] += 0.25f * dout[((long long)(n * (H / 2) + h / 2) * (W / 2) + w / 2) * C + c];
+  }
+}
+
+// cat[n][h][w] = (low[n][h/2][w/2][0..C1), skip[n][h][w][0..C2))
+__global__ void k_upcat(const bf16 *__restrict__ low, int C1, const bf16 *__restrict__ skip, int C2,
+                        bf16 *__restrict__ cat, int N, int H, int W) {
+  const int Ct = C1 + C2, cp = Ct / 2;
+  const long long total = (long long)N * H * W * cp;
+  const uint32_t *lo = reinterpret_cast<const uint32_t *>(low);
+  const uint32_t *sk = reinterpret_cast<const uint32_t *>(skip);
+  uint32_t *o = reinterpret_cast<uint32_t *>(cat);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = 2 * (int)(e % cp);
+    const long long pix = e / cp;
+    const int w = (int)(pix % W);
+    const long long nh = pix / W;
+    const int h = (int)(nh % H);
+    const int n = (int)(nh / H);
+    uint32_t v;
+    if (c < C1) v = lo[(((long long)(n * (H / 2) + h / 2) * (W / 2) + w / 2) * C1 + c) / 2];
+    else v = sk[(pix * C2 + (c - C1)) / 2];
+    o[e] = v;
+  }
+}
+
+// dlow[n][h][w][c] = sum of the four fine gradients of its copies
+__global__ void k_upcat_bwd_low(const float *__restrict__ dcat, int Ct, int C1, float *__restrict__ dlow,
+                                int N, int Hl, int Wl) {
+  const long long total = (long long)N * Hl * Wl * C1;
+  const int H = 2 * Hl, W = 2 * Wl;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e % C1);
+    long long q = e / C1;
+    const int w = (int)(q % Wl);
+    q /= Wl;
+    const int h = (int)(q % Hl);
+    const int n = (int)(q / Hl);
+    const long long r0 = ((long long)(n * H + 2 * h) * W + 2 * w) * Ct + c;
+    const long long r1 = r0 + (long long)W * Ct;
+    dlow[e] = ((dcat[r0] + dcat[r0 + Ct]) + dcat[r1]) + dcat[r1 + Ct];
+  }
+}
+
+__global__ void k_upcat_bwd_skip(const float *__restrict__ dcat, int Ct, int C1, float *__restrict__ dskip,
+                                 long long P, int C2) {
+  const long long total = P * C2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / C2;
+    const int c = (int)(e - p * C2);
+    dskip[e] = dcat[p * Ct + C1 + c];
+  }
+}
+
+// y[p] = b + sum_c w[c] u[p][c]   (FP32)
+__global__ void k_out_fwd(const bf16 *__restrict__ u, const float *__restrict__ w,
+                          const float *__restrict__ b, float *__restrict__ y, long long P, int C) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
+       p += (long long)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int c = 0; c < C; c++) s = fmaf(w[c], __bfloat162float(u[p * C + c]), s);
+    y[p] = s + b[0];
+  }
+}
+
+__global__ void k_out_bwd_dx(const float *__restrict__ dy, const float *__restrict__ w,
+                             float *__restrict__ du, long long P, int C) {
+  const long long total = P * C;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / C;
+    du[e] = dy[p] * w[e - p * C];
+  }
+}
+
+// out[c] += sum_p a[p][c] * (wgt ? wgt[p] : 1); C divides the block size.
+__global__ void k_chan_dot(const bf16 *__restrict__ a, const float *__restrict__ wgt, long long P,
+                           int C, float *__restrict__ out) {
+  __shared__ float red[kEw];
+  const int c = threadIdx.x % C, lp = threadIdx.x / C, ps = kEw / C;
+  float s = 0.0f;
+  for (long long p = (long long)blockIdx.x * ps + lp; p < P; p += (long long)gridDim.x * ps) {
+    const float v = __bfloat162float(a[p * C + c]);
+    s += wgt ? v * wgt[p] : v;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x < C) {
+    float tsum = 0.0f;
+    for (int k = 0; k < ps; k++) tsum += red[k * C + threadIdx.x];
+    atomicAdd(out + threadIdx.x, tsum);
+  }
+}
+
+__global__ void k_sum(const float *__restrict__ a, long long n, float *__restrict__ out) {
+  float s = 0.0f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    s += a[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+// dy = scale (y - t); loss += (y - t)^2 (FP64)
+__global__ void k_mse(const float *__restrict__ y, const float *__restrict__ t, float *__restrict__ dy,
+                      long long P, float scale, double *__restrict__ loss) {
+  double s = 0.0;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P;
+       p += (long long)gridDim.x * blockDim.x) {
+    const float r = y[p] - t[p];
+    dy[p] = scale * r;
+    s += (double)r * r;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, s);
+}
+
+// ReLU gradient, rounded to BF16 for the tensor-core products
+__global__ void k_relu_mask(const float *__restrict__ dy, const bf16 *__restrict__ y, bf16 *__restrict__ dz,
+                            long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dz[i] = __float2bfloat16_rn(__bfloat162float(y[i]) > 0.0f ? dy[i] : 0.0f);
+}
+
+// wt[ci][tap][co] = w[co][8 - tap][ci]: the data gradient as a forward conv
+__global__ void k_flip(const bf16 *__restrict__ w, bf16 *__restrict__ wt, int cout, int cin) {
+  const long long total = (long long)cout * 9 * cin;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int co = (int)(e % cout);
+    const long long q = e / cout;
+    const int tap = (int)(q % 9);
+    const int ci = (int)(q / 9);
+    wt[e] = w[((long long)co * 9 + (8 - tap)) * cin + ci];
+  }
+}
+
+__global__ void k_adam(float *__restrict__ p, float *__restrict__ m, float *__restrict__ v,
+                       const float *__restrict__ g, long long n, float lr_t, float b1, float b2,
+                       float eps) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr_t * mi / (sqrtf(vi) + eps);
+  }
+}
+
+__global__ void k_to_bf16(const float *__restrict__ a, bf16 *__restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16_rn(a[i]);
+}
+
+// Interior statistics: s[0] += sum a^2, s[1] += sum b, s[2] += sum b^2,
+// s[3] = max c (c >= 0; its FP64 bits order as integers).
+__global__ void k_stats(const float *__restrict__ a, const float *__restrict__ b,
+                        const float *__restrict__ c, int nzpad, int x0, int z0, int nx, int nz,
+                        double *__restrict__ s) {
+  double sa = 0, sb = 0, sb2 = 0, mc = 0;
+  const long long total = (long long)nx * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(e / nz), iz = (int)(e - (long long)ix * nz);
+    const long long q = (long long)(x0 + ix) * nzpad + z0 + iz;
+    if (a) sa += (double)a[q] * a[q];
+    if (b) { sb += b[q]; sb2 += (double)b[q] * b[q]; }
+    if (c) mc = fmax(mc, (double)fmaxf(c[q], 0.0f));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sa += __shfl_down_sync(0xffffffffu, sa, o);
+    sb += __shfl_down_sync(0xffffffffu, sb, o);
+    sb2 += __shfl_down_sync(0xffffffffu, sb2, o);
+    mc = fmax(mc, __shfl_down_sync(0xffffffffu, mc, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(s, sa);
+    atomicAdd(s + 1, sb);
+    atomicAdd(s + 2, sb2);
+    atomicMax(reinterpret_cast<unsigned long long *>(s + 3), (unsigned long long)__double_as_longlong(mc));
+  }
+}
+
+__global__ void k_features(const float *__restrict__ gr, const float *__restrict__ vel,
+                           const float *__restrict__ il, int nzpad, int x0, int z0, int nx, int nz,
+                           int Hp, int Wp, const double *__restrict__ s, float *__restrict__ x3) {
+  const double cnt = (double)nx * nz;
+  const double rms = sqrt(s[0] / cnt);
+  const double mean = s[1] / cnt;
+  const double var = fmax(s[2] / cnt - mean * mean, 0.0);
+  const double sd = sqrt(var);
+  const double imax = s[3];
+  const long long total = (long long)Hp * Wp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int h = (int)(e / Wp), w = (int)(e - (long long)h * Wp);
+    float f0 = 0, f1 = 0, f2 = 0;
+    if (h < nx && w < nz) {
+      const long long q = (long long)(x0 + h) * nzpad + z0 + w;
+      if (rms > 0) f0 = (float)(gr[q] / rms);
+      if (sd > 0) f1 = (float)((vel[q] - mean) / sd);
+      if (il && imax > 0) f2 = (log10f((float)(fmaxf(il[q], 0.0f) / imax) + 1e-6f) + 3.0f) / 3.0f;
+    }
+    x3[3 * e] = f0;
+    x3[3 * e + 1] = f1;
+    x3[3 * e + 2] = f2;
+  }
+}
+
+__global__ void k_target(const float *__restrict__ dv, int nzpad, int x0, int z0, int nx, int nz,
+                         int Hp, int Wp, const double *__restrict__ s, float *__restrict__ t) {
+  const double rms = sqrt(s[0] / ((double)nx * nz));
+  const long long total = (long long)Hp * Wp;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int h = (int)(e / Wp), w = (int)(e - (long long)h * Wp);
+    float v = 0;
+    if (h < nx && w < nz && rms > 0) v = (float)(dv[(long long)(x0 + h) * nzpad + z0 + w] / rms);
+    t[e] = v;
+  }
+}
+
+__global__ void k_scatter(const float *__restrict__ y, int nzpad, int x0, int z0, int nx, int nz,
+                          int Wp, float *__restrict__ dir) {
+  const long long total = (long long)nx * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(e / nz), iz = (int)(e - (long long)ix * nz);
+    dir[(long long)(x0 + ix) * nzpad + z0 + iz] = y[(long long)ix * Wp + iz];
+  }
+}
+
+__global__ void k_illum(float *__restrict__ illum, const float *__restrict__ p, long long fstride,
+                        int n, int nxpad, int nzpad, int pitch) {
+  const long long total = (long long)nxpad * nzpad;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(e / nzpad), z = (int)(e - (long long)x * nzpad);
+    float s = 0.0f;
+    for (int j = 0; j < n; j++) {
+      const float v = p[j * fstride + (long long)x * pitch + z];
+      s = fmaf(v, v, s);
+    }
+    illum[e] += s;
+  }
+}
+
+template <int NJ, bool F32>
+void conv_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out, bool accum,
+             int cout, int N, int H, int W, cudaStream_t st) {
+  dim3 grid((W + 63) / 64, N * H, cout / (8 * NJ));
+  k_conv3x3<NJ, F32><<<grid, 128, 0, st>>>(in, cin, w, bias, out, accum ? 1 : 0, cout, H, W);
+  noted();
+}
+
+template <int NJ>
+void wgrad_go(const bf16 *dz, int cout, const bf16 *x, float *dw, int N, int H, int W,
+              cudaStream_t st) {
+  const long long P = (long long)N * H * W;
+  const long long chunks_wanted = 128;
+  long long ppc = 32 * std::max(1LL, (P + 32 * chunks_wanted - 1) / (32 * chunks_wanted));
+  dim3 grid((unsigned)((P + ppc - 1) / ppc), 9, (cout + 63) / 64);
+  k_conv3x3_wgrad<NJ><<<grid, 128, 0, st>>>(dz, cout, x, dw, N, H, W, (int)ppc);
+  noted();
+}
+
+int roundup8(int v) { return (v + 7) / 8 * 8; }
+
+}  // namespace
+
+void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out,
+                    bool out_f32, bool accum, int cout, int N, int H, int W, cudaStream_t st) {
+  SWFWI_REQUIRE(cin > 0 && cin % 16 == 0 && cout > 0 && cout % 16 == 0, "conv widths must be multiples of 16");
+  SWFWI_REQUIRE(N > 0 && H > 0 && W > 0 && (long long)N * H <= 65535, "conv image size out of range");
+  SWFWI_REQUIRE(out_f32 || bias, "BF16 conv output needs a bias");
+  const int nj = cout % 64 == 0 ? 8 : (cout % 32 == 0 ? 4 : 2);
+  if (out_f32) {
+    if (nj == 8) conv_go<8, true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+    else if (nj == 4) conv_go<4, true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+    else conv_go<2, true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+  } else {
+    if (nj == 8) conv_go<8, false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+    else if (nj == 4) conv_go<4, false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+    else conv_go<2, false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+  }
+}
+
+void launch_conv3x3_wgrad(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, int N, int H,
+                          int W, cudaStream_t st) {
+  SWFWI_REQUIRE(cout > 0 && cout % 16 == 0, "conv widths must be multiples of 16");
+  switch (cin) {
+    case 16: wgrad_go<2>(dz, cout, x, dw, N, H, W, st); break;
+    case 32: wgrad_go<4>(dz, cout, x, dw, N, H, W, st); break;
+    case 48: wgrad_go<6>(dz, cout, x, dw, N, H, W, st); break;
+    case 64: wgrad_go<8>(dz, cout, x, dw, N, H, W, st); break;
+    case 96: wgrad_go<12>(dz, cout, x, dw, N, H, W, st); break;
+    case 128: wgrad_go<16>(dz, cout, x, dw, N, H, W, st); break;
+    default: throw Error(SWFWI_ERR_BAD_ARG, "weight gradient: input width must be 16/32/48/64/96/128");
+  }
+}
+
+void launch_illum_accum(float *illum, const float *p, long long fstride, int n, int nxpad, int nzpad,
+                        int pitch, cudaStream_t st) {
+  const long long total = (long long)nxpad * nzpad;
+  k_illum<<<blocks_for(total), kEw, 0, st>>>(illum, p, fstride, n, nxpad, nzpad, pitch);
+  noted();
+}
+
+// ------------------------------------------------------------------ network
+Preconditioner::Preconditioner(const int widths[4]) {
+  for (int i = 0; i < 4; i++) {
+    SWFWI_REQUIRE(widths[i] > 0 && widths[i] % 16 == 0 && widths[i] <= 64,
+                  "preconditioner widths must be multiples of 16 up to 64");
+    w_[i] = widths[i];
+  }
+  const int c0 = w_[0], c1 = w_[1], c2 = w_[2], c3 = w_[3];
+  const int io[kConvs][2] = {{kInCh, c0}, {c0, c0}, {c0, c1}, {c1, c1}, {c1, c2},
+                             {c2, c2},    {c2, c3}, {c3, c3}, {c3 + c2, c2}, {c2, c2},
+                             {c2 + c1, c1}, {c1, c1}, {c1 + c0, c0}, {c0, c0}};
+  long long off = 0;
+  size_t maxw = 0;
+  for (int l = 0; l < kConvs; l++) {
+    ConvSpec s{io[l][0], io[l][1], 0, 0};
+    s.w_off = off;
+    off += (long long)s.cout * 9 * s.cin;
+    s.b_off = off;
+    off += s.cout;
+    maxw = std::max(maxw, (size_t)s.cout * 9 * s.cin);
+    conv_.push_back(s);
+  }
+  out_w_ = off;
+  off += c0;
+  out_b_ = off;
+  off += 1;
+  nparam_ = off;
+  params_.resize(nparam_);
+  grads_.resize(nparam_);
+  m_.resize(nparam_);
+  v_.resize(nparam_);
+  wbf_.resize(nparam_);
+  wflip_.resize(maxw);
+  red_.resize(8);
+  // He-uniform conv weights, zero biases, small output layer (seeded)
+  std::vector<float> h(nparam_, 0.0f);
+  std::mt19937 gen(12345u);
+  for (const ConvSpec &s : conv_) {
+    const float lim = std::sqrt(6.0f / (9.0f * s.cin));
+    std::uniform_real_distribution<float> U(-lim, lim);
+    for (long long i = 0; i < (long long)s.cout * 9 * s.cin; i++) h[s.w_off + i] = U(gen);
+  }
+  {
+    const float lim = 1.0f / std::sqrt((float)c0);
+    std::uniform_real_distribution<float> U(-lim, lim);
+    for (int i = 0; i < c0; i++) h[out_w_ + i] = U(gen);
+  }
+  set_params(h.data());
+}
+
+void Preconditioner::refresh_bf16() {
+  k_to_bf16<<<blocks_for(nparam_), kEw, 0, st_>>>(params_.get(), wbf_.get(), nparam_);
+  noted();
+}
+
+void Preconditioner::set_params(const float *host) {
+  SWFWI_REQUIRE(host, "null parameters");
+  params_.upload(host, nparam_, st_);
+  refresh_bf16();
+  reset_optimizer();
+}
+
+void Preconditioner::reset_optimizer() {
+  m_.zero(st_);
+  v_.zero(st_);
+  grads_.zero(st_);
+  step_ = 0;
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Preconditioner::get_params(float *host) {
+  SWFWI_CUDA(cudaMemcpyAsync(host, params_.get(), sizeof(float) * nparam_, cudaMemcpyDeviceToHost, st_));
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Preconditioner::get_grads(float *host) {
+  SWFWI_CUDA(cudaMemcpyAsync(host, grads_.get(), sizeof(float) * nparam_, cudaMemcpyDeviceToHost, st_));
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Preconditioner::conv_fwd(int l, const bf16 *in, bf16 *out, long long, int H, int W) {
+  const ConvSpec &s = conv_[l];
+  launch_conv3x3(in, s.cin, wbf_.get() + s.w_off, params_.get() + s.b_off, out, false, false, s.cout,
+                 N_, H, W, st_);
+}
+
+void Preconditioner::forward(const float *x, float *y, int N, int H, int W) {
+  SWFWI_REQUIRE(x && N > 0 && H > 0 && W > 0 && H % 8 == 0 && W % 8 == 0,
+                "network input must be N x H x W with H and W multiples of 8");
+  SWFWI_REQUIRE((long long)N * H <= 65535, "network batch too large");
+  N_ = N;
+  H_ = H;
+  W_ = W;
+  const int c0 = w_[0], c1 = w_[1], c2 = w_[2], c3 = w_[3];
+  const long long P0 = (long long)N * H * W, P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64;
+  x16_.resize(P0 * kInCh);
+  a0_.resize(P0 * c0); s0_.resize(P0 * c0); p0_.resize(P1 * c0);
+  a1_.resize(P1 * c1); s1_.resize(P1 * c1); p1_.resize(P2 * c1);
+  a2_.resize(P2 * c2); s2_.resize(P2 * c2); p2_.resize(P3 * c2);
+  a3_.resize(P3 * c3); b3_.resize(P3 * c3);
+  cat2_.resize(P2 * (c3 + c2)); a4_.resize(P2 * c2); u2_.resize(P2 * c2);
+  cat1_.resize(P1 * (c2 + c1)); a5_.resize(P1 * c1); u1_.resize(P1 * c1);
+  cat0_.resize(P0 * (c1 + c0)); a6_.resize(P0 * c0); u0_.resize(P0 * c0);
+  y_.resize(P0);
+  k_pack3<<<blocks_for(P0), kEw, 0, st_>>>(x, x16_.get(), P0);
+  noted();
+  const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+  conv_fwd(0, x16_.get(), a0_.get(), P0, H, W);
+  conv_fwd(1, a0_.get(), s0_.get(), P0, H, W);
+  k_pool<<<blocks_for(P1 * c0 / 2), kEw, 0, st_>>>(s0_.get(), p0_.get(), N, H, W, c0);
+  noted();
+  conv_fwd(2, p0_.get(), a1_.get(), P1, H1, W1);
+  conv_fwd(3, a1_.get(), s1_.get(), P1, H1, W1);
+  k_pool<<<blocks_for(P2 * c1 / 2), kEw, 0, st_>>>(s1_.get(), p1_.get(), N, H1, W1, c1);
+  noted();
+  conv_fwd(4, p1_.get(), a2_.get(), P2, H2, W2);
+  conv_fwd(5, a2_.get(), s2_.get(), P2, H2, W2);
+  k_pool<<<blocks_for(P3 * c2 / 2), kEw, 0, st_>>>(s2_.get(), p2_.get(), N, H2, W2, c2);
+  noted();
+  conv_fwd(6, p2_.get(), a3_.get(), P3, H3, W3);
+  conv_fwd(7, a3_.get(), b3_.get(), P3, H3, W3);
+  k_upcat<<<blocks_for(P2 * (c3 + c2) / 2), kEw, 0, st_>>>(b3_.get(), c3, s2_.get(), c2, cat2_.get(), N, H2, W2);
+  noted();
+  conv_fwd(8, cat2_.get(), a4_.get(), P2, H2, W2);
+  conv_fwd(9, a4_.get(), u2_.get(), P2, H2, W2);
+  k_upcat<<<blocks_for(P1 * (c2 + c1) / 2), kEw, 0, st_>>>(u2_.get(), c2, s1_.get(), c1, cat1_.get(), N, H1, W1);
+  noted();
+  conv_fwd(10, cat1_.get(), a5_.get(), P1, H1, W1);
+  conv_fwd(11, a5_.get(), u1_.get(), P1, H1, W1);
+  k_upcat<<<blocks_for(P0 * (c1 + c0) / 2), kEw, 0, st_>>>(u1_.get(), c1, s0_.get(), c0, cat0_.get(), N, H, W);
+  noted();
+  conv_fwd(12, cat0_.get(), a6_.get(), P0, H, W);
+  conv_fwd(13, a6_.get(), u0_.get(), P0, H, W);
+  k_out_fwd<<<blocks_for(P0), kEw, 0, st_>>>(u0_.get(), params_.get() + out_w_, params_.get() + out_b_,
+                                              y_.get(), P0, c0);
+  noted();
+  if (y) SWFWI_CUDA(cudaMemcpyAsync(y, y_.get(), sizeof(float) * P0, cudaMemcpyDeviceToDevice, st_));
+}
+
+void Preconditioner::conv_bwd(int l, const bf16 *in, const bf16 *out, const float *dY, float *dX,
+                              int H, int W) {
+  const ConvSpec &s = conv_[l];
+  const long long P = (long long)N_ * H * W;
+  k_relu_mask<<<blocks_for(P * s.cout), kEw, 0, st_>>>(dY, out, dz_.get(), P * s.cout);
+  noted();
+  k_chan_dot<<<blocks_for(P * s.cout), kEw, 0, st_>>>(dz_.get(), nullptr, P, s.cout, grads_.get() + s.b_off);
+  noted();
+  launch_conv3x3_wgrad(dz_.get(), s.cout, in, s.cin, grads_.get() + s.w_off, N_, H, W, st_);
+  if (dX) {
+    k_flip<<<blocks_for((long long)s.cout * 9 * s.cin), kEw, 0, st_>>>(wbf_.get() + s.w_off, wflip_.get(),
+                                                                        s.cout, s.cin);
+    noted();
+    launch_conv3x3(dz_.get(), s.cout, wflip_.get(), nullptr, dX, true, false, s.cin, N_, H, W, st_);
+  }
+}
+
+double Preconditioner::backward(const float *t) {
+  SWFWI_REQUIRE(t && N_ > 0, "backward needs a forward and a target");
+  const int N = N_, H = H_, W = W_;
+  const int c0 = w_[0], c1 = w_[1], c2 = w_[2], c3 = w_[3];
+  const long long P0 = (long long)N * H * W, P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64;
+  const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
+  const long long big = std::max({P0 * (c1 + c0), P1 * (c2 + c1), P2 * (c3 + c2), P0 * c0});
+  dy_.resize(P0);
+  dA_.resize(big);
+  dB_.resize(big);
+  dCat_.resize(big);
+  dLow_.resize(big);
+  dS0_.resize(P0 * c0);
+  dS1_.resize(P1 * c1);
+  dS2_.resize(P2 * c2);
+  dz_.resize(big);
+  grads_.zero(st_);
+  red_.zero(st_);
+  k_mse<<<blocks_for(P0), kEw, 0, st_>>>(y_.get(), t, dy_.get(), P0, 2.0f / (float)P0, red_.get());
+  noted();
+  // output layer
+  k_chan_dot<<<blocks_for(P0 * c0), kEw, 0, st_>>>(u0_.get(), dy_.get(), P0, c0, grads_.get() + out_w_);
+  noted();
+  k_sum<<<blocks_for(P0), kEw, 0, st_>>>(dy_.get(), P0, grads_.get() + out_b_);
+  noted();
+  k_out_bwd_dx<<<blocks_for(P0 * c0), kEw, 0, st_>>>(dy_.get(), params_.get() + out_w_, dA_.get(), P0, c0);
+  noted();
+  // decoder level 0
+  conv_bwd(13, a6_.get(), u0_.get(), dA_.get(), dB_.get(), H, W);
+  conv_bwd(12, cat0_.get(), a6_.get(), dB_.get(), dCat_.get(), H, W);
+  k_upcat_bwd_low<<<blocks_for(P1 * c1), kEw, 0, st_>>>(dCat_.get(), c1 + c0, c1, dLow_.get(), N, H1, W1);
+  noted();
+  k_upcat_bwd_skip<<<blocks_for(P0 * c0), kEw, 0, st_>>>(dCat_.get(), c1 + c0, c1, dS0_.get(), P0, c0);
+  noted();
+  // decoder level 1
+  conv_bwd(11, a5_.get(), u1_.get(), dLow_.get(), dA_.get(), H1, W1);
+  conv_bwd(10, cat1_.get(), a5_.get(), dA_.get(), dCat_.get(), H1, W1);
+  k_upcat_bwd_low<<<blocks_for(P2 * c2), kEw, 0, st_>>>(dCat_.get(), c2 + c1, c2, dLow_.get(), N, H2, W2);
+  noted();
+  k_upcat_bwd_skip<<<blocks_for(P1 * c1), kEw, 0, st_>>>(dCat_.get(), c2 + c1, c2, dS1_.get(), P1, c1);
+  noted();
+  // decoder level 2
+  conv_bwd(9, a4_.get(), u2_.get(), dLow_.get(), dA_.get(), H2, W2);
+  conv_bwd(8, cat2_.get(), a4_.get(), dA_.get(), dCat_.get(), H2, W2);
+  k_upcat_bwd_low<<<blocks_for(P3 * c3), kEw, 0, st_>>>(dCat_.get(), c3 + c2, c3, dLow_.get(), N, H3, W3);
+  noted();
+  k_upcat_bwd_skip<<<blocks_for(P2 * c2), kEw, 0, st_>>>(dCat_.get(), c3 + c2, c3, dS2_.get(), P2, c2);
+  noted();
+  // bottleneck
+  conv_bwd(7, a3_.get(), b3_.get(), dLow_.get(), dA_.get(), H3, W3);
+  conv_bwd(6, p2_.get(), a3_.get(), dA_.get(), dB_.get(), H3, W3);
+  k_pool_bwd<<<blocks_for(P2 * c2), kEw, 0, st_>>>(dB_.get(), dS2_.get(), N, H2, W2, c2);
+  noted();
+  // encoder level 2
+  conv_bwd(5, a2_.get(), s2_.get(), dS2_.get(), dA_.get(), H2, W2);
+  conv_bwd(4, p1_.get(), a2_.get(), dA_.get(), dB_.get(), H2, W2);
+  k_pool_bwd<<<blocks_for(P1 * c1), kEw, 0, st_>>>(dB_.get(), dS1_.get(), N, H1, W1, c1);
+  noted();
+  // encoder level 1
+  conv_bwd(3, a1_.get(), s1_.get(), dS1_.get(), dA_.get(), H1, W1);
+  conv_bwd(2, p0_.get(), a1_.get(), dA_.get(), dB_.get(), H1, W1);
+  k_pool_bwd<<<blocks_for(P0 * c0), kEw, 0, st_>>>(dB_.get(), dS0_.get(), N, H, W, c0);
+  noted();
+  // encoder level 0
+  conv_bwd(1, a0_.get(), s0_.get(), dS0_.get(), dA_.get(), H, W);
+  conv_bwd(0, x16_.get(), a0_.get(), dA_.get(), nullptr, H, W);
+  double loss = 0;
+  SWFWI_CUDA(cudaMemcpyAsync(&loss, red_.get(), sizeof(double), cudaMemcpyDeviceToHost, st_));
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+  if (!std::isfinite(loss)) throw Error(SWFWI_ERR_NONFINITE, "preconditioner loss is not finite");
+  return loss / (double)P0;
+}
+
+void Preconditioner::adam_step(float lr, float beta1, float beta2, float eps) {
+  step_++;
+  const double bc1 = 1.0 - std::pow((double)beta1, (double)step_);
+  const double bc2 = 1.0 - std::pow((double)beta2, (double)step_);
+  const float lr_t = (float)(lr * std::sqrt(bc2) / bc1);
+  k_adam<<<blocks_for(nparam_), kEw, 0, st_>>>(params_.get(), m_.get(), v_.get(), grads_.get(), nparam_,
+                                               lr_t, beta1, beta2, eps);
+  noted();
+  refresh_bf16();
+}
+
+double Preconditioner::train_step(const float *x, const float *t, int N, int H, int W, float lr) {
+  forward(x, nullptr, N, H, W);
+  const double loss = backward(t);
+  adam_step(lr);
+  return loss;
+}
+
+void Preconditioner::features(const float *grad, const float *vel, const float *illum, int nxpad,
+                              int nzpad, int bx0, int bxn, int bz0, int bzn, float *x3) {
+  SWFWI_REQUIRE(grad && vel && x3, "null field");
+  const int nx = nxpad - bx0 - bxn, nz = nzpad - bz0 - bzn;
+  SWFWI_REQUIRE(nx > 0 && nz > 0, "empty interior");
+  const int Hp = roundup8(nx), Wp = roundup8(nz);
+  red_.zero(st_);
+  k_stats<<<blocks_for((long long)nx * nz), kEw, 0, st_>>>(grad, vel, illum, nzpad, bx0, bz0, nx, nz,
+                                                             red_.get());
+  noted();
+  k_features<<<blocks_for((long long)Hp * Wp), kEw, 0, st_>>>(grad, vel, illum, nzpad, bx0, bz0, nx, nz, Hp,
+                                                                Wp, red_.get(), x3);
+  noted();
+}
+
+void Preconditioner::target(const float *dv, int nxpad, int nzpad, int bx0, int bxn, int bz0, int bzn,
+                            float *t) {
+  SWFWI_REQUIRE(dv && t, "null field");
+  const int nx = nxpad - bx0 - bxn, nz = nzpad - bz0 - bzn;
+  SWFWI_REQUIRE(nx > 0 && nz > 0, "empty interior");
+  const int Hp = roundup8(nx), Wp = roundup8(nz);
+  red_.zero(st_);
+  k_stats<<<blocks_for((long long)nx * nz), kEw, 0, st_>>>(dv, nullptr, nullptr, nzpad, bx0, bz0, nx, nz,
+                                                             red_.get());
+  noted();
+  k_target<<<blocks_for((long long)Hp * Wp), kEw, 0, st_>>>(dv, nzpad, bx0, bz0, nx, nz, Hp, Wp, red_.get(), t);
+  noted();
+}
+
+void Preconditioner::scatter(const float *y, int nxpad, int nzpad, int bx0, int bxn, int bz0, int bzn,
+                             float *dir) {
+  SWFWI_REQUIRE(y && dir, "null field");
+  const int nx = nxpad - bx0 - bxn, nz = nzpad - bz0 - bzn;
+  SWFWI_REQUIRE(nx > 0 && nz > 0, "empty interior");
+  SWFWI_CUDA(cudaMemsetAsync(dir, 0, sizeof(float) * (size_t)nxpad * nzpad, st_));
+  k_scatter<<<blocks_for((long long)nx * nz), kEw, 0, st_>>>(y, nzpad, bx0, bz0, nx, nz, roundup8(nz), dir);
+  noted();
+}
+
+void Preconditioner::propose(const float *grad, const float *vel, const float *illum, int nxpad,
+                             int nzpad, int bx0, int bxn, int bz0, int bzn, float *dir) {
+  const int nx = nxpad - bx0 - bxn, nz = nzpad - bz0 - bzn;
+  const int Hp = roundup8(nx), Wp = roundup8(nz);
+  feat_.resize((size_t)Hp * Wp * 3);
+  outimg_.resize((size_t)Hp * Wp);
+  features(grad, vel, illum, nxpad, nzpad, bx0, bxn, bz0, bzn, feat_.get());
+  forward(feat_.get(), outimg_.get(), 1, Hp, Wp);
+  scatter(outimg_.get(), nxpad, nzpad, bx0, bxn, bz0, bzn, dir);
+}
+
+}  // namespace swfwi
