@@ -260,6 +260,118 @@ def run_kernel_mode(args):
     return 0
 
 
+def network_flops(layers, N, H, W):
+    """Multiply-add FLOPs of one forward of the preconditioner network and of
+    one training step (forward, weight gradient, data gradient of every conv
+    but the first) on N images of H x W; layers: the library's layer table
+    [(cin, cout, w_off, b_off)] (14 convs, then the 1x1 output)."""
+    P0 = N * H * W
+    level = [0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0]
+    fwd = sum(2.0 * (P0 // 4 ** level[l]) * 9 * ci * co for l, (ci, co, _, _) in enumerate(layers[:-1]))
+    fwd += 2.0 * P0 * layers[-1][0]
+    first = 2.0 * P0 * 9 * layers[0][0] * layers[0][1]
+    return fwd, 3 * fwd - first
+
+
+def run_learned_mode(args):
+    """FWI wall-clock to equal model error, learned vs plain: train the
+    preconditioner on plain FWI runs over seeded models, then on each
+    held-out model run plain FWI for its epoch budget and learned FWI until
+    it reaches the lowest model error plain reached.  value: the geometric
+    mean over the held-out models of plain seconds / learned seconds.  Also
+    times the network's kernels."""
+    import math
+    import torch
+    from swfwi_b200 import precond as P
+    s = P.demo_survey(nz=args.learned_nz, nx=args.learned_nx, nt=args.learned_nt,
+                      ns=args.learned_shots).scaled(maxdv=100.0)
+    net, st = P.train_from_plain(s, range(100, 100 + args.learned_models), args.learned_iters,
+                                 args.learned_epochs, batch=16)
+    print(json.dumps({"training": st}), file=sys.stderr, flush=True)
+    tests = []
+    for seed in args.learned_test_seeds:
+        r = P.compare(s, net, seed, args.learned_iters, min_decrease=args.learned_min_decrease)
+        sp = (r["plain_s"] / r["learned_s"]) if (r["plain_s"] and r["learned_s"]) else None
+        tests.append({"seed": seed, "speedup": sp, "plain_s": r["plain_s"], "learned_s": r["learned_s"],
+                      "target_model_error": r["target_error"], "initial_model_error": r["initial_error"],
+                      "learned_steps": {"tried": r["learned_stats"][1], "accepted": r["learned_stats"][2]},
+                      "plain_history": [[round(a, 3), b] for a, b, _, _ in r["plain_history"]],
+                      "learned_history": [[round(a, 3), b, bool(d)] for a, b, _, d in r["learned_history"]]})
+        print(json.dumps({k: v for k, v in tests[-1].items() if "history" not in k}), file=sys.stderr, flush=True)
+    sps = [t["speedup"] for t in tests]
+    value = math.exp(sum(math.log(x) for x in sps) / len(sps)) if all(sps) else None
+    H, W = P.image_shape(P.Damp4t10d.from_survey(s))
+    network = time_network(net, 16, H, W)
+    line = {
+        "metric": "FWI wall-clock to equal model L2, learned vs plain",
+        "value": value, "unit": "x (plain seconds / learned seconds, geometric mean over held-out models)",
+        "higher_is_better": True, "n_gpus": 1, "dtype": "f32 wavefields, bf16 network (f32 accumulate)",
+        "data": "synthetic",
+        "model_error": "relative L2 of the interior velocity (m/s) against the true model; target: the "
+                       "lowest error the plain run reaches in its epoch budget",
+        "config": {"workload": f"learned-preconditioned FWI, {s.nx}x{s.nz} grid (dx {s.dx} m), nt={s.nt}, "
+                               f"{s.ns} shots, {s.fm} Hz Ricker; seeded gradient+anomaly models",
+                   "train_models": args.learned_models, "plain_iters": args.learned_iters,
+                   "train_epochs": args.learned_epochs, "maxdv": s.maxdv,
+                   "learned_min_decrease": args.learned_min_decrease,
+                   "test_seeds": list(args.learned_test_seeds)},
+        "training": st, "tests": tests, "network": network,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def time_network(net, N, H, W, reps=10):
+    """The preconditioner's kernels on a batch of N images of H x W: forward
+    and training step (forward, backward, Adam) timed with CUDA events on the
+    launching stream, with the tensor-core throughput of the training step."""
+    import torch
+    x = torch.randn((N, H, W, 3), device="cuda")
+    t = torch.randn((N, H, W), device="cuda")
+    for _ in range(3):
+        net.forward(x)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        net.forward(x)
+    e1.record(st)
+    e1.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / reps
+    saved = net.params()
+    e0.record(st)
+    for _ in range(reps):
+        net.train_step(x, t, 1e-9)
+    e1.record(st)
+    e1.synchronize()
+    train_ms = e0.elapsed_time(e1) / reps
+    net.set_params(saved)
+    fwd_flop, train_flop = network_flops(net.layers(), N, H, W)
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, peak_basis = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, peak_basis = 1590.0, "fallback"
+    return {"image": [H, W], "batch": N, "forward_ms": fwd_ms, "train_step_ms": train_ms,
+            "forward_gflop": fwd_flop / 1e9, "train_gflop": train_flop / 1e9,
+            "forward_tflops": fwd_flop / fwd_ms / 1e9, "train_tflops": train_flop / train_ms / 1e9,
+            "bf16_peak_tflops": peak, "peak_basis": peak_basis,
+            "train_frac": train_flop / train_ms / 1e9 / peak}
+
+
+def run_network_mode(args):
+    """The preconditioner's kernels alone (a seeded network, random images of
+    the learned workload's interior): the small case for ncu."""
+    import torch
+    from swfwi_b200 import precond as P
+    s = P.demo_survey(nz=args.learned_nz, nx=args.learned_nx, nt=args.learned_nt, ns=args.learned_shots)
+    H, W = P.image_shape(P.Damp4t10d.from_survey(s))
+    torch.manual_seed(0)
+    net = P.Preconditioner()
+    print(json.dumps({"mode": "network", **time_network(net, 16, H, W)}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -272,9 +384,20 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "kernel", "tune"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "kernel", "tune", "learned", "network"],
                     help="kernel: short 96-shot batched forward (the small case for ncu); "
-                         "tune: print the autotuner's table")
+                         "tune: print the autotuner's table; learned: FWI wall-clock to equal model "
+                         "error, learned preconditioner vs plain")
+    ap.add_argument("--learned-models", type=int, default=16, help="training models of --mode learned")
+    ap.add_argument("--learned-iters", type=int, default=30, help="plain epochs per training/test run")
+    ap.add_argument("--learned-epochs", type=int, default=100, help="training epochs of the network")
+    ap.add_argument("--learned-nx", type=int, default=240)
+    ap.add_argument("--learned-nz", type=int, default=80)
+    ap.add_argument("--learned-nt", type=int, default=1000)
+    ap.add_argument("--learned-shots", type=int, default=12)
+    ap.add_argument("--learned-test-seeds", type=int, nargs="+", default=[200, 201, 202])
+    ap.add_argument("--learned-min-decrease", type=float, default=0.02,
+                    help="a learned step is kept only if it lowers the objective by this fraction")
     ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")
     ap.add_argument("--tuning", default="", help="stencil launch shape as JSON (skips the autotuner)")
     ap.add_argument("--fuse", default="off", choices=["on", "off"],
@@ -288,6 +411,10 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "learned":
+        return run_learned_mode(args)
+    if args.mode == "network":
+        return run_network_mode(args)
     if args.mode != "bench":
         return run_kernel_mode(args)
 

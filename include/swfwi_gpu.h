@@ -432,6 +432,9 @@ int swfwi_precond_propose(swfwi_precond *h, const swfwi_damp4t10d *method, const
  * step is taken.  Source illumination is accumulated every 4 steps of the
  * gradient's forward sweep while a network is attached or collect is on. */
 int swfwi_fwi_set_preconditioner(swfwi_fwi *h, swfwi_precond *net);
+/* Keep a learned step only if it lowers the objective by at least this
+ * fraction (default 0: any decrease the search confirms); in [0, 1). */
+int swfwi_fwi_set_learned_min_decrease(swfwi_fwi *h, float frac);
 int swfwi_fwi_collect_illumination(swfwi_fwi *h, int on);
 /* The last epoch's gradient / illumination, host [nxpad][nzpad]. */
 int swfwi_fwi_get_gradient(swfwi_fwi *h, float *grad);

@@ -138,6 +138,7 @@ _SIGS = {
     "swfwi_precond_propose": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "swfwi_fwi_set_preconditioner": [_vp, _vp],
     "swfwi_fwi_collect_illumination": [_vp, C.c_int],
+    "swfwi_fwi_set_learned_min_decrease": [_vp, C.c_float],
     "swfwi_fwi_get_gradient": [_vp, _fp],
     "swfwi_fwi_get_illumination": [_vp, _fp],
     "swfwi_fwi_learned_stats": [_vp, _ip, _ip, _ip],
@@ -659,6 +660,11 @@ class _Framework:
         """Attach a swfwi_b200.precond.Preconditioner (None detaches)."""
         _check(lib().swfwi_fwi_set_preconditioner(self.h, net.h if net is not None else None))
         self._net = net     # keep it alive while attached
+
+    def setLearnedMinDecrease(self, frac: float):
+        """Keep a learned step only if it lowers the objective by at least
+        this fraction (default 0)."""
+        _check(lib().swfwi_fwi_set_learned_min_decrease(self.h, frac))
 
     def collectIllumination(self, on: bool = True):
         _check(lib().swfwi_fwi_collect_illumination(self.h, int(on)))

@@ -774,6 +774,13 @@ int swfwi_fwi_set_preconditioner(swfwi_fwi *h, swfwi_precond *net) {
   });
 }
 
+int swfwi_fwi_set_learned_min_decrease(swfwi_fwi *h, float frac) {
+  return guarded([&] {
+    SWFWI_REQUIRE(frac >= 0.0f && frac < 1.0f, "fraction must be in [0, 1)");
+    R(h).learned_min_decrease = frac;
+  });
+}
+
 int swfwi_fwi_collect_illumination(swfwi_fwi *h, int on) {
   return guarded([&] { R(h).set_collect_illumination(on != 0); });
 }

@@ -275,7 +275,8 @@ bool FwiRunner::try_learned_step(float obj1) {
   float objv = 0;
   const float step = learned_search.calsteplen(f, obj1, 2 * a2max, objv);
   const float tried_best = std::min(learned_search.obj[1], learned_search.obj[2]);
-  if (!(std::isfinite(objv) && objv < obj1 && tried_best < obj1 && step > 0.0f)) {
+  const float bar = obj1 * (1.0f - learned_min_decrease);
+  if (!(std::isfinite(objv) && objv < bar && tried_best < obj1 && step > 0.0f)) {
     // rejected: the next search along the network starts from scratch
     learned_search.preserved_init = false;
     return false;

@@ -73,6 +73,9 @@ class FwiRunner {
   void get_gradient(float *host);       // the last epoch's gradient
   void get_illumination(float *host);   // the last epoch's illumination
   int last_step_learned = 0, learned_tried = 0, learned_accepted = 0;
+  // A learned step must lower the objective by at least this fraction
+  // (0: any confirmed decrease).
+  float learned_min_decrease = 0.0f;
   StepSearch learned_search;
 
  private:

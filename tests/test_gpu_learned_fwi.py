@@ -1,0 +1,29 @@
+"""What the trained preconditioner gains over plain FWI, on a held-out
+seeded model (the measurement itself, at full size and over several
+models, is `bench.py --mode learned`)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_learned_fwi_against_plain(cuda):
+    from swfwi_b200 import precond as P
+    s = P.demo_survey(nt=1000).scaled(maxdv=100.0)
+    iters = 15
+    net, st = P.train_from_plain(s, range(100, 106), iters, epochs=40, batch=16)
+    assert np.isfinite(st["loss_last"]) and st["loss_last"] < 0.5 * st["loss_first"], st
+    r = P.compare(s, net, 200, iters, min_decrease=0.02)
+    plain_best = r["target_error"]
+    learned_errs = [h[1] for h in r["learned_history"]]
+    _, tried, accepted = r["learned_stats"]
+    ratio = (r["plain_s"] / r["learned_s"]) if r["learned_s"] else None
+    print(f"\nplain: {r['initial_error']:.5f} -> best {plain_best:.5f} in {r['plain_s']:.2f} s; "
+          f"learned: best {min(learned_errs):.5f}, reached plain's best in "
+          f"{'%.2f s' % r['learned_s'] if r['learned_s'] else 'not reached'}; "
+          f"learned steps {accepted}/{tried}; wall-clock ratio {ratio}")
+    assert accepted >= 1
+    # every epoch keeps the objective falling, so the learned run reaches
+    # the plain run's error level within the same epoch budget
+    assert min(learned_errs) <= 1.10 * plain_best
+    assert learned_errs[-1] < r["initial_error"]
