@@ -291,20 +291,26 @@ def run_learned_mode(args):
     tests = []
     for seed in args.learned_test_seeds:
         r = P.compare(s, net, seed, args.learned_iters, min_decrease=args.learned_min_decrease)
-        sp = (r["plain_s"] / r["learned_s"]) if (r["plain_s"] and r["learned_s"]) else None
-        tests.append({"seed": seed, "speedup": sp, "plain_s": r["plain_s"], "learned_s": r["learned_s"],
+        reached = r["learned_s"] is not None
+        # a learned run that never reaches the target counts with its whole
+        # run time: an upper bound on its speed-up
+        learned_s = r["learned_s"] if reached else r["learned_history"][-1][0]
+        sp = r["plain_s"] / learned_s
+        tests.append({"seed": seed, "speedup": sp, "reached": reached, "plain_s": r["plain_s"],
+                      "learned_s": learned_s,
                       "target_model_error": r["target_error"], "initial_model_error": r["initial_error"],
                       "learned_steps": {"tried": r["learned_stats"][1], "accepted": r["learned_stats"][2]},
                       "plain_history": [[round(a, 3), b] for a, b, _, _ in r["plain_history"]],
                       "learned_history": [[round(a, 3), b, bool(d)] for a, b, _, d in r["learned_history"]]})
         print(json.dumps({k: v for k, v in tests[-1].items() if "history" not in k}), file=sys.stderr, flush=True)
     sps = [t["speedup"] for t in tests]
-    value = math.exp(sum(math.log(x) for x in sps) / len(sps)) if all(sps) else None
+    value = math.exp(sum(math.log(x) for x in sps) / len(sps))
     H, W = P.image_shape(P.Damp4t10d.from_survey(s))
     network = time_network(net, 16, H, W)
     line = {
         "metric": "FWI wall-clock to equal model L2, learned vs plain",
-        "value": value, "unit": "x (plain seconds / learned seconds, geometric mean over held-out models)",
+        "value": value, "unit": "x (plain seconds / learned seconds, geometric mean over held-out models; "
+                                "a learned run that never reaches the target counts with its whole time)",
         "higher_is_better": True, "n_gpus": 1, "dtype": "f32 wavefields, bf16 network (f32 accumulate)",
         "data": "synthetic",
         "model_error": "relative L2 of the interior velocity (m/s) against the true model; target: the "

@@ -123,6 +123,12 @@ int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, i
  * in place of the separate source, residual and image launches.  Results
  * are bit-identical either way. */
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on);
+/* CUDA graphs for the forward and backward time loops (default on): from a
+ * loop's second use, while a step covers at most 8e6 points (fields x
+ * nxpad x nzpad) and stencil timing is off, the loop is captured on a
+ * private stream and replayed on the propagator's stream.  Same kernels,
+ * same results. */
+int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on);
 /* Per-shot receiver lists (uneven spreads; not in the reference, whose
  * ShotPosition is one common line): shot s has receivers
  * [offsets[s], offsets[s+1]) of gx/gz (unpadded, host arrays).  The
@@ -435,6 +441,9 @@ int swfwi_fwi_set_preconditioner(swfwi_fwi *h, swfwi_precond *net);
 /* Keep a learned step only if it lowers the objective by at least this
  * fraction (default 0: any decrease the search confirms); in [0, 1). */
 int swfwi_fwi_set_learned_min_decrease(swfwi_fwi *h, float frac);
+/* Stop proposing learned steps after this many rejected ones (default 0:
+ * never stop). */
+int swfwi_fwi_set_learned_patience(swfwi_fwi *h, int rejections);
 int swfwi_fwi_collect_illumination(swfwi_fwi *h, int on);
 /* The last epoch's gradient / illumination, host [nxpad][nzpad]. */
 int swfwi_fwi_get_gradient(swfwi_fwi *h, float *grad);

@@ -97,6 +97,7 @@ _SIGS = {
     "swfwi_encode_source": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
     "swfwi_fwi_set_velocity": [_vp, _fp],
     "swfwi_damp4t10d_set_fusion": [_vp, C.c_int],
+    "swfwi_damp4t10d_set_graphs": [_vp, C.c_int],
     "swfwi_rsf_get": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int],
     "swfwi_rsf_dims": [C.c_char_p, _ip, _ip, _fp, _fp],
     "swfwi_rsf_read": [C.c_char_p, _fp, C.c_longlong, C.c_longlong],
@@ -139,6 +140,7 @@ _SIGS = {
     "swfwi_fwi_set_preconditioner": [_vp, _vp],
     "swfwi_fwi_collect_illumination": [_vp, C.c_int],
     "swfwi_fwi_set_learned_min_decrease": [_vp, C.c_float],
+    "swfwi_fwi_set_learned_patience": [_vp, C.c_int],
     "swfwi_fwi_get_gradient": [_vp, _fp],
     "swfwi_fwi_get_illumination": [_vp, _fp],
     "swfwi_fwi_learned_stats": [_vp, _ip, _ip, _ip],
@@ -446,8 +448,13 @@ class Damp4t10d:
         self.arith = arith
 
     def set_fusion(self, on: bool):
-        """Fused forward time loop (record, strips, next injection in the step)."""
+        """Fused backward time loop (source subtraction and imaging in the
+        source back-step, residual injection in the receiver step)."""
         _check(lib().swfwi_damp4t10d_set_fusion(self.h, int(bool(on))))
+
+    def set_graphs(self, on: bool):
+        """CUDA graphs for the forward/backward time loops of small steps."""
+        _check(lib().swfwi_damp4t10d_set_graphs(self.h, int(bool(on))))
 
     def set_strip_format(self, fmt: int):
         """Boundary strips of the gradients: STRIP_F32 (exact), STRIP_F16 or
@@ -665,6 +672,10 @@ class _Framework:
         """Keep a learned step only if it lowers the objective by at least
         this fraction (default 0)."""
         _check(lib().swfwi_fwi_set_learned_min_decrease(self.h, frac))
+
+    def setLearnedPatience(self, rejections: int):
+        """Stop proposing learned steps after this many rejections (0: never)."""
+        _check(lib().swfwi_fwi_set_learned_patience(self.h, rejections))
 
     def collectIllumination(self, on: bool = True):
         _check(lib().swfwi_fwi_collect_illumination(self.h, int(on)))

@@ -198,6 +198,10 @@ int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on) {
   return guarded([&] { P(h).fuse = on != 0; });
 }
 
+int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on) {
+  return guarded([&] { P(h).graphs = on != 0; });
+}
+
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest) {
   return guarded([&] {
@@ -778,6 +782,13 @@ int swfwi_fwi_set_learned_min_decrease(swfwi_fwi *h, float frac) {
   return guarded([&] {
     SWFWI_REQUIRE(frac >= 0.0f && frac < 1.0f, "fraction must be in [0, 1)");
     R(h).learned_min_decrease = frac;
+  });
+}
+
+int swfwi_fwi_set_learned_patience(swfwi_fwi *h, int rejections) {
+  return guarded([&] {
+    SWFWI_REQUIRE(rejections >= 0, "negative patience");
+    R(h).learned_patience = rejections;
   });
 }
 

@@ -100,7 +100,49 @@ Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, f
 }
 
 // the handle owns no stream: work goes to the caller's (default: legacy stream 0)
-Propagator::~Propagator() {}
+Propagator::~Propagator() {
+  for (cudaGraphExec_t &g : gexec_)
+    if (g) cudaGraphExecDestroy(g);
+  if (cap_) cudaStreamDestroy(cap_);
+}
+
+template <typename F>
+void Propagator::run_loop(int which, double points_per_step, F &&body) {
+  const bool use = graphs && loop_warm_[which] && points_per_step <= kGraphMaxPoints &&
+                   !step_timer().enabled.load(std::memory_order_relaxed);
+  loop_warm_[which] = true;
+  if (!use) {
+    body();
+    return;
+  }
+  if (!cap_) SWFWI_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
+  cudaStream_t user = st_;
+  cudaGraph_t g = nullptr;
+  SWFWI_CUDA(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal));
+  st_ = cap_;
+  try {
+    body();
+  } catch (...) {
+    st_ = user;
+    cudaStreamEndCapture(cap_, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  st_ = user;
+  SWFWI_CUDA(cudaStreamEndCapture(cap_, &g));
+  if (gexec_[which]) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(gexec_[which], g, &info) != cudaSuccess) {
+      (void)cudaGetLastError();   // a different topology: instantiate anew
+      cudaGraphExecDestroy(gexec_[which]);
+      gexec_[which] = nullptr;
+    }
+  }
+  cudaError_t e = gexec_[which] ? cudaSuccess : cudaGraphInstantiate(&gexec_[which], g, 0);
+  cudaGraphDestroy(g);
+  SWFWI_CUDA(e);
+  SWFWI_CUDA(cudaGraphLaunch(gexec_[which], st_));
+}
 
 void Propagator::set_stream(cudaStream_t s) { st_ = s; }
 
@@ -504,6 +546,7 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
   w.p1.zero(st_);
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
+  run_loop(0, (double)n * nxpad * nzpad, [&] {
   for (int it = 0; it < nt; it++) {
     // addSource -> stepForward -> swap -> recordSeis / writeBndry
     // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
@@ -526,6 +569,7 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
                            st_);
     }
   }
+  });
   // leave the final (current, next) pair for a backward sweep
   if (p0 != w.p0.get() + kStreamCoff) std::swap(w.p0, w.p1);
 }
@@ -559,6 +603,7 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
     float *image = reinterpret_cast<float *>(w.image.get()) + kStreamCoff;
     launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)(nt - 1) * ngrec, (long long)nt * ngrec, 1, +1,
                      st_);
+    run_loop(1, (double)n * nxpad * nzpad, [&] {
     for (int it = nt - 1; it >= 0; it--) {
       launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad, nzpad, bx0,
                            pitch, st_);
@@ -591,8 +636,10 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
       std::swap(gp0, gp1);
       if (last) break;
     }
+    });
     return;
   }
+  run_loop(1, (double)n * nxpad * nzpad, [&] {
   for (int it = nt - 1; it >= 0; it--) {
     // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
     // subSource; receiver addSource -> stepForward -> swap; image.
@@ -618,6 +665,7 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
     else break;
     launch_image<T>(w.image.get() + kStreamCoff, fstride, sp0, gp0, fstride, n, npts, scale, st_);
   }
+  });
 }
 
 template <typename T>

@@ -84,6 +84,11 @@ class Propagator {
   // steps (the caller zeroes it).
   float *illum = nullptr;
   int illum_every = 4;
+  // CUDA graphs for the time loops of the forward and backward sweeps when
+  // a step is small enough to be launch-bound (n fields x nxpad x nzpad at
+  // most kGraphMaxPoints); never while stencil launches are being timed.
+  bool graphs = true;
+  static constexpr double kGraphMaxPoints = 8e6;
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);
   void set_dims(int nxpad, int nzpad);   // padded grid; uploads geometry
@@ -196,6 +201,14 @@ class Propagator {
                     const std::vector<PtLine> *rec_lines = nullptr);
   template <typename T>
   void ensure_work(Work<T> &w, int n, bool strips);
+  // Runs body (launches on st_ only, no allocation or synchronisation):
+  // directly, or captured into a graph on a private stream and launched on
+  // st_.  which: 0 forward loop, 1 backward loop (cached executable each).
+  template <typename F>
+  void run_loop(int which, double points_per_step, F &&body);
+  cudaStream_t cap_ = nullptr;
+  cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
+  bool loop_warm_[2] = {false, false};
   // copies between the caller's [nxpad][nzpad] layout and pitched rows
   template <typename T>
   void to_pitched(T *dst, const T *src);

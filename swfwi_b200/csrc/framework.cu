@@ -234,7 +234,8 @@ void FwiRunner::plain_epoch(int iter) {
   update_grad(restart_cg_ ? 0 : iter);
   restart_cg_ = false;
   last_step_learned = 0;
-  if (net_ && try_learned_step(obj1)) return;
+  if (net_ && (learned_patience == 0 || learned_rejected < learned_patience) && try_learned_step(obj1))
+    return;
 
   launch_max_alpha(reinterpret_cast<float *>(scratch_.get()), vel_.get(), dir_.get(), n_, p_.dt,
                    p_.dx, search.maxdv, st);
@@ -279,6 +280,7 @@ bool FwiRunner::try_learned_step(float obj1) {
   if (!(std::isfinite(objv) && objv < bar && tried_best < obj1 && step > 0.0f)) {
     // rejected: the next search along the network starts from scratch
     learned_search.preserved_init = false;
+    learned_rejected++;
     return false;
   }
   update_obj = objv;

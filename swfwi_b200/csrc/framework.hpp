@@ -76,6 +76,11 @@ class FwiRunner {
   // A learned step must lower the objective by at least this fraction
   // (0: any confirmed decrease).
   float learned_min_decrease = 0.0f;
+  // Stop proposing learned steps after this many rejections (0: never):
+  // the network helps most early in a run, and a rejected proposal costs
+  // its trial forwards.
+  int learned_patience = 0;
+  int learned_rejected = 0;
   StepSearch learned_search;
 
  private:

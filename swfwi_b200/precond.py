@@ -163,7 +163,8 @@ def model_error(fw: FwiFramework, v_true_interior: np.ndarray) -> float:
 
 def run_fwi(method: Damp4t10d, exvel0: np.ndarray, wlt: np.ndarray, dobs: np.ndarray, survey, iters: int,
             v_true_interior: np.ndarray | None = None, net: Preconditioner | None = None,
-            collect: bool = False, target_error: float | None = None, min_decrease: float = 0.0):
+            collect: bool = False, target_error: float | None = None, min_decrease: float = 0.0,
+            patience: int = 0):
     """Plain FWI (net None) or learned-preconditioned FWI for `iters` epochs.
 
     Returns a dict: history [(seconds since start, model error, objective,
@@ -175,6 +176,7 @@ def run_fwi(method: Damp4t10d, exvel0: np.ndarray, wlt: np.ndarray, dobs: np.nda
     if net is not None:
         fw.setPreconditioner(net)
         fw.setLearnedMinDecrease(min_decrease)
+        fw.setLearnedPatience(patience)
     if collect:
         fw.collectIllumination(True)
     hist, samples = [], []
@@ -347,7 +349,7 @@ def train_from_plain(survey, train_seeds, iters: int, epochs: int, lr: float = 1
 
 
 def compare(survey, net: Preconditioner, test_seed: int, iters: int, recipe: str = "anomaly",
-            min_decrease: float = 0.0, plain=None):
+            min_decrease: float = 0.0, plain=None, patience: int = 0):
     """Plain and learned FWI on one held-out model: the lowest model error
     the plain run reaches in `iters` epochs is the target; returns the seconds
     each method needs to reach it with both histories (pass `plain` to reuse
@@ -359,7 +361,7 @@ def compare(survey, net: Preconditioner, test_seed: int, iters: int, recipe: str
     # not fall monotonically)
     target = min(h[1] for h in plain["history"][1:])
     learned = run_fwi(m, ex0, wlt, dobs, survey, iters, vtrue, net=net, target_error=target,
-                      min_decrease=min_decrease)
+                      min_decrease=min_decrease, patience=patience)
     return {"target_error": target, "initial_error": plain["history"][0][1],
             "plain_s": time_to_error(plain["history"], target),
             "learned_s": time_to_error(learned["history"], target),

@@ -226,3 +226,37 @@ def test_stream_matches_reference_large_grid(cuda, ref, kern, bz, depth):
     d = torch.zeros((s.nt, s.ng), device="cuda")
     m.FwiForwardModeling(t(torch, wlt), d, 3)
     np.testing.assert_array_equal(d.cpu().numpy(), M.fwi_forward(wlt, 3))
+
+
+def test_graph_loops_bit_exact_and_timed(cuda):
+    # the same batched forward and gradient with the time loops replayed as
+    # CUDA graphs (second and later calls) and launched one by one
+    import time
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    torch = cuda
+    s = sv.config("fwi").scaled(nt=600, ns=6, sxbeg=40, jsx=70)
+    v = sv.layered_model(s.nx, s.nz, seed=5)
+    out = {}
+    for graphs in (False, True):
+        m = S.Damp4t10d.from_survey(s, arith=S.ARITH_FAST)
+        m.set_graphs(graphs)
+        vel = t(torch, m.expandDomain(v))
+        m.bindVelocity(vel)
+        w = t(torch, S.ricker_wavelet(s.nt, s.fm, s.dt))
+        d = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
+        ids = list(range(s.ns))
+        m.forward_batch(w, d, ids)          # first use: direct launches
+        grad = torch.zeros_like(vel)
+        m.gradient_batch(w, d * 1.01, ids, grad)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            m.forward_batch(w, d, ids)
+            m.gradient_batch(w, d * 1.01, ids, grad)
+        torch.cuda.synchronize()
+        out[graphs] = (d.cpu().numpy(), grad.cpu().numpy(), (time.perf_counter() - t0) / 3)
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    np.testing.assert_array_equal(out[True][1], out[False][1])
+    print(f"forward + gradient, 6 shots of 533 x 193, nt 600: launches {out[False][2] * 1e3:.1f} ms, "
+          f"graphs {out[True][2] * 1e3:.1f} ms")
