@@ -101,13 +101,23 @@ Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, f
 
 // the handle owns no stream: work goes to the caller's (default: legacy stream 0)
 Propagator::~Propagator() {
-  for (cudaGraphExec_t &g : gexec_)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto &c : gcache_)
+    for (LoopGraph &g : c)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
   if (cap_) cudaStreamDestroy(cap_);
 }
 
+void Propagator::loop_key_common(std::vector<long long> &k) const {
+  const long long v[] = {nxpad, nzpad, pitch, fstride, bsize, bx0, nt, arith, strip_format, stream_kernel,
+                         stream_bz, stream_xchunk, stream_depth, stream_shot_major, fuse ? 1 : 0,
+                         reinterpret_cast<long long>(illum), illum_every, vel_stride_,
+                         reinterpret_cast<long long>(damp_x_.get()), reinterpret_cast<long long>(damp_z_.get()),
+                         reinterpret_cast<long long>(d_err_.get())};
+  k.insert(k.end(), std::begin(v), std::end(v));
+}
+
 template <typename F>
-void Propagator::run_loop(int which, double points_per_step, F &&body) {
+void Propagator::run_loop(int which, double points_per_step, const std::vector<long long> &key, F &&body) {
   const bool use = graphs && loop_warm_[which] && points_per_step <= kGraphMaxPoints &&
                    !step_timer().enabled.load(std::memory_order_relaxed);
   loop_warm_[which] = true;
@@ -115,6 +125,13 @@ void Propagator::run_loop(int which, double points_per_step, F &&body) {
     body();
     return;
   }
+  std::vector<LoopGraph> &cache = gcache_[which];
+  for (size_t i = 0; i < cache.size(); i++)
+    if (cache[i].key == key) {
+      if (i) std::swap(cache[i], cache[0]);   // most recent first
+      SWFWI_CUDA(cudaGraphLaunch(cache[0].exec, st_));
+      return;
+    }
   if (!cap_) SWFWI_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
   cudaStream_t user = st_;
   cudaGraph_t g = nullptr;
@@ -130,18 +147,17 @@ void Propagator::run_loop(int which, double points_per_step, F &&body) {
   }
   st_ = user;
   SWFWI_CUDA(cudaStreamEndCapture(cap_, &g));
-  if (gexec_[which]) {
-    cudaGraphExecUpdateResultInfo info;
-    if (cudaGraphExecUpdate(gexec_[which], g, &info) != cudaSuccess) {
-      (void)cudaGetLastError();   // a different topology: instantiate anew
-      cudaGraphExecDestroy(gexec_[which]);
-      gexec_[which] = nullptr;
-    }
-  }
-  cudaError_t e = gexec_[which] ? cudaSuccess : cudaGraphInstantiate(&gexec_[which], g, 0);
+  LoopGraph e;
+  e.key = key;
+  cudaError_t err = cudaGraphInstantiate(&e.exec, g, 0);
   cudaGraphDestroy(g);
-  SWFWI_CUDA(e);
-  SWFWI_CUDA(cudaGraphLaunch(gexec_[which], st_));
+  SWFWI_CUDA(err);
+  if (cache.size() >= kGraphCache) {
+    cudaGraphExecDestroy(cache.back().exec);
+    cache.pop_back();
+  }
+  cache.insert(cache.begin(), std::move(e));
+  SWFWI_CUDA(cudaGraphLaunch(cache[0].exec, st_));
 }
 
 void Propagator::set_stream(cudaStream_t s) { st_ = s; }
@@ -546,7 +562,16 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
   w.p1.zero(st_);
   int ar = sizeof(T) == 8 ? (int)ARITH_F64 : arith;
   long long bstride = (long long)nt * bsize;
-  run_loop(0, (double)n * nxpad * nzpad, [&] {
+  std::vector<long long> key = {
+      (long long)sizeof(T), n, reinterpret_cast<long long>(src.pos), src.per_shot,
+      reinterpret_cast<long long>(src.slot_shot), reinterpret_cast<long long>(vals), it_stride, slot_stride,
+      i_stride, reinterpret_cast<long long>(rec.pos), rec.per_shot, reinterpret_cast<long long>(rec.slot_shot),
+      ngrec, reinterpret_cast<long long>(dcal), save_strips ? 1 : 0, reinterpret_cast<long long>(velrcp),
+      reinterpret_cast<long long>(p0), reinterpret_cast<long long>(p1),
+      reinterpret_cast<long long>(w.strips.get()), reinterpret_cast<long long>(w.qstrips.get()),
+      reinterpret_cast<long long>(w.qscale.get())};
+  loop_key_common(key);
+  run_loop(0, (double)n * nxpad * nzpad, key, [&] {
   for (int it = 0; it < nt; it++) {
     // addSource -> stepForward -> swap -> recordSeis / writeBndry
     // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
@@ -570,8 +595,10 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
     }
   }
   });
-  // leave the final (current, next) pair for a backward sweep
-  if (p0 != w.p0.get() + kStreamCoff) std::swap(w.p0, w.p1);
+  // leave the final (current, next) pair for a backward sweep: every step
+  // swaps the pair once (decided by nt alone, since a replayed graph does
+  // not run the loop's host code)
+  if (nt % 2 == 1) std::swap(w.p0, w.p1);
 }
 
 template <typename T>
@@ -592,6 +619,16 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   // kStreamCoff on: (slot j) j*fstride + kStreamCoff + [0, nxpad*pitch)
   // stays inside the slot's fstride floats
   const int npts = nxpad * pitch;
+  std::vector<long long> key = {
+      (long long)sizeof(T), n, reinterpret_cast<long long>(src.pos), src.per_shot,
+      reinterpret_cast<long long>(src.slot_shot), reinterpret_cast<long long>(vals), it_stride, slot_stride,
+      i_stride, reinterpret_cast<long long>(rec.pos), rec.per_shot, reinterpret_cast<long long>(rec.slot_shot),
+      ngrec, reinterpret_cast<long long>(vsrc), reinterpret_cast<long long>(velrcp),
+      reinterpret_cast<long long>(sp0), reinterpret_cast<long long>(sp1), reinterpret_cast<long long>(gp0),
+      reinterpret_cast<long long>(gp1), reinterpret_cast<long long>(w.image.get()),
+      reinterpret_cast<long long>(w.strips.get()), reinterpret_cast<long long>(w.qstrips.get()),
+      reinterpret_cast<long long>(w.qscale.get()), reinterpret_cast<long long>(w.src_lines.get()),
+      reinterpret_cast<long long>(w.rec_lines.get()), (long long)(dt * 1e9)};
   const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
                      (int)rec_lines->size() == n && injectable(*src_lines) && injectable(*rec_lines);
   if (fused) {
@@ -600,10 +637,14 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
     // the next residual
     w.src_lines.upload(*src_lines, st_);
     w.rec_lines.upload(*rec_lines, st_);
+    key.push_back(1);   // fused
+    key.push_back(reinterpret_cast<long long>(w.src_lines.get()));
+    key.push_back(reinterpret_cast<long long>(w.rec_lines.get()));
     float *image = reinterpret_cast<float *>(w.image.get()) + kStreamCoff;
     launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)(nt - 1) * ngrec, (long long)nt * ngrec, 1, +1,
                      st_);
-    run_loop(1, (double)n * nxpad * nzpad, [&] {
+    loop_key_common(key);
+    run_loop(1, (double)n * nxpad * nzpad, key, [&] {
     for (int it = nt - 1; it >= 0; it--) {
       launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad, nzpad, bx0,
                            pitch, st_);
@@ -639,7 +680,9 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
     });
     return;
   }
-  run_loop(1, (double)n * nxpad * nzpad, [&] {
+  key.push_back(0);   // separate launches
+  loop_key_common(key);
+  run_loop(1, (double)n * nxpad * nzpad, key, [&] {
   for (int it = nt - 1; it >= 0; it--) {
     // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
     // subSource; receiver addSource -> stepForward -> swap; image.

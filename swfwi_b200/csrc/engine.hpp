@@ -202,13 +202,23 @@ class Propagator {
   template <typename T>
   void ensure_work(Work<T> &w, int n, bool strips);
   // Runs body (launches on st_ only, no allocation or synchronisation):
-  // directly, or captured into a graph on a private stream and launched on
-  // st_.  which: 0 forward loop, 1 backward loop (cached executable each).
+  // directly, or as a CUDA graph launched on st_.  which: 0 forward loop,
+  // 1 backward loop.  key lists everything the loop's launches depend on
+  // (pointers, sizes, settings); a cached graph with the same key is
+  // relaunched without running body, else body is captured on a private
+  // stream into a new graph (up to kGraphCache per loop kind).
   template <typename F>
-  void run_loop(int which, double points_per_step, F &&body);
+  void run_loop(int which, double points_per_step, const std::vector<long long> &key, F &&body);
+  struct LoopGraph {
+    std::vector<long long> key;
+    cudaGraphExec_t exec = nullptr;
+  };
+  static constexpr size_t kGraphCache = 4;
   cudaStream_t cap_ = nullptr;
-  cudaGraphExec_t gexec_[2] = {nullptr, nullptr};
+  std::vector<LoopGraph> gcache_[2];
   bool loop_warm_[2] = {false, false};
+  // settings every loop launch depends on, for graph keys
+  void loop_key_common(std::vector<long long> &k) const;
   // copies between the caller's [nxpad][nzpad] layout and pitched rows
   template <typename T>
   void to_pitched(T *dst, const T *src);
