@@ -115,14 +115,16 @@ __global__ void __launch_bounds__(128) k_conv3x3(const bf16 *__restrict__ in, in
   }
 }
 
-// Weight gradient of one tap: dw[co][tap][ci] += sum_p dz[p][co] x[p + tap][ci].
+// Weight gradient of one tap over one chunk of pixels:
+// part[chunk][co][tap][ci] = sum_{p in chunk} dz[p][co] x[p + tap][ci].
 // GEMM M = output channels (16 per warp, 64 per CTA), N = input channels
 // (8*NJ), K = pixels (32 per stage, staged transposed in shared memory so
-// that fragment pairs run along pixels).  FP32 atomics into dw at the end.
+// that fragment pairs run along pixels).  The chunks are summed afterwards
+// in a fixed order (k_reduce_rows): training is bit-reproducible.
 template <int NJ>
 __global__ void __launch_bounds__(128) k_conv3x3_wgrad(const bf16 *__restrict__ dz, int cout,
                                                        const bf16 *__restrict__ x,
-                                                       float *__restrict__ dw, int N, int H, int W,
+                                                       float *__restrict__ part, int N, int H, int W,
                                                        int pix_per_cta) {
   constexpr int CIN = 8 * NJ, KS = 32, LD = 40;
   __shared__ __align__(16) uint16_t zt[64][LD];
@@ -186,14 +188,24 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad(const bf16 *__restrict__ 
     __syncthreads();
   }
   if (!mw) return;
+  float *dw = part + (long long)blockIdx.x * cout * 9 * CIN;
   const int coa = co0 + warp * 16 + g, cob = coa + 8;
 #pragma unroll
   for (int j = 0; j < NJ; j++) {
     const int ci = j * 8 + 2 * t;
-    atomicAdd(dw + ((long long)coa * 9 + tap) * CIN + ci, acc[j][0]);
-    atomicAdd(dw + ((long long)coa * 9 + tap) * CIN + ci + 1, acc[j][1]);
-    atomicAdd(dw + ((long long)cob * 9 + tap) * CIN + ci, acc[j][2]);
-    atomicAdd(dw + ((long long)cob * 9 + tap) * CIN + ci + 1, acc[j][3]);
+    *reinterpret_cast<float2 *>(dw + ((long long)coa * 9 + tap) * CIN + ci) = make_float2(acc[j][0], acc[j][1]);
+    *reinterpret_cast<float2 *>(dw + ((long long)cob * 9 + tap) * CIN + ci) = make_float2(acc[j][2], acc[j][3]);
+  }
+}
+
+// out[i] = sum over r = 0..rows-1, in order, of part[r * len + i]
+__global__ void k_reduce_rows(const float *__restrict__ part, int rows, long long len,
+                              float *__restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+       i += (long long)gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int r = 0; r < rows; r++) s += part[(long long)r * len + i];
+    out[i] = s;
   }
 }
 
@@ -326,9 +338,10 @@ __global__ void k_out_bwd_dx(const float *__restrict__ dy, const float *__restri
   }
 }
 
-// out[c] += sum_p a[p][c] * (wgt ? wgt[p] : 1); C divides the block size.
+// part[block][c] = sum over the block's pixels of a[p][c] * (wgt ? wgt[p] :
+// 1); C divides the block size.  Summed over blocks by k_reduce_rows.
 __global__ void k_chan_dot(const bf16 *__restrict__ a, const float *__restrict__ wgt, long long P,
-                           int C, float *__restrict__ out) {
+                           int C, float *__restrict__ part) {
   __shared__ float red[kEw];
   const int c = threadIdx.x % C, lp = threadIdx.x / C, ps = kEw / C;
   float s = 0.0f;
@@ -341,17 +354,25 @@ __global__ void k_chan_dot(const bf16 *__restrict__ a, const float *__restrict__
   if (threadIdx.x < C) {
     float tsum = 0.0f;
     for (int k = 0; k < ps; k++) tsum += red[k * C + threadIdx.x];
-    atomicAdd(out + threadIdx.x, tsum);
+    part[(long long)blockIdx.x * C + threadIdx.x] = tsum;
   }
 }
 
-__global__ void k_sum(const float *__restrict__ a, long long n, float *__restrict__ out) {
+// part[block] = the block's sum of a (fixed order)
+__global__ void k_sum(const float *__restrict__ a, long long n, float *__restrict__ part) {
+  __shared__ float red[kEw / 32];
   float s = 0.0f;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     s += a[i];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < kEw / 32; w++) t += red[w];
+    part[blockIdx.x] = t;
+  }
 }
 
 // dy = scale (y - t); loss += (y - t)^2 (FP64)
@@ -409,11 +430,11 @@ __global__ void k_to_bf16(const float *__restrict__ a, bf16 *__restrict__ b, lon
     b[i] = __float2bfloat16_rn(a[i]);
 }
 
-// Interior statistics: s[0] += sum a^2, s[1] += sum b, s[2] += sum b^2,
-// s[3] = max c (c >= 0; its FP64 bits order as integers).
+// Interior statistics, per block: part[block][0..3] = sum a^2, sum b,
+// sum b^2, max c (c >= 0); k_stats_final adds the blocks in order.
 __global__ void k_stats(const float *__restrict__ a, const float *__restrict__ b,
                         const float *__restrict__ c, int nzpad, int x0, int z0, int nx, int nz,
-                        double *__restrict__ s) {
+                        double *__restrict__ part) {
   double sa = 0, sb = 0, sb2 = 0, mc = 0;
   const long long total = (long long)nx * nz;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
@@ -430,12 +451,41 @@ __global__ void k_stats(const float *__restrict__ a, const float *__restrict__ b
     sb2 += __shfl_down_sync(0xffffffffu, sb2, o);
     mc = fmax(mc, __shfl_down_sync(0xffffffffu, mc, o));
   }
+  __shared__ double red[kEw / 32][4];
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(s, sa);
-    atomicAdd(s + 1, sb);
-    atomicAdd(s + 2, sb2);
-    atomicMax(reinterpret_cast<unsigned long long *>(s + 3), (unsigned long long)__double_as_longlong(mc));
+    red[threadIdx.x >> 5][0] = sa;
+    red[threadIdx.x >> 5][1] = sb;
+    red[threadIdx.x >> 5][2] = sb2;
+    red[threadIdx.x >> 5][3] = mc;
   }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+    for (int w = 0; w < kEw / 32; w++) {
+      t0 += red[w][0];
+      t1 += red[w][1];
+      t2 += red[w][2];
+      t3 = fmax(t3, red[w][3]);
+    }
+    part[4 * blockIdx.x] = t0;
+    part[4 * blockIdx.x + 1] = t1;
+    part[4 * blockIdx.x + 2] = t2;
+    part[4 * blockIdx.x + 3] = t3;
+  }
+}
+
+__global__ void k_stats_final(const double *__restrict__ part, int blocks, double *__restrict__ s) {
+  double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+  for (int i = 0; i < blocks; i++) {
+    t0 += part[4 * i];
+    t1 += part[4 * i + 1];
+    t2 += part[4 * i + 2];
+    t3 = fmax(t3, part[4 * i + 3]);
+  }
+  s[0] = t0;
+  s[1] = t1;
+  s[2] = t2;
+  s[3] = t3;
 }
 
 __global__ void k_features(const float *__restrict__ gr, const float *__restrict__ vel,
@@ -510,14 +560,32 @@ void conv_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *ou
   noted();
 }
 
+constexpr long long kWgradChunks = 128;   // pixel chunks of a weight gradient (at most)
+constexpr int kRedBlocks = 256;           // blocks of the channel sums
+
+long long wgrad_pix_per_chunk(long long P) {
+  return 32 * std::max(1LL, (P + 32 * kWgradChunks - 1) / (32 * kWgradChunks));
+}
+
 template <int NJ>
-void wgrad_go(const bf16 *dz, int cout, const bf16 *x, float *dw, int N, int H, int W,
+void wgrad_go(const bf16 *dz, int cout, const bf16 *x, float *dw, float *part, int N, int H, int W,
               cudaStream_t st) {
   const long long P = (long long)N * H * W;
-  const long long chunks_wanted = 128;
-  long long ppc = 32 * std::max(1LL, (P + 32 * chunks_wanted - 1) / (32 * chunks_wanted));
-  dim3 grid((unsigned)((P + ppc - 1) / ppc), 9, (cout + 63) / 64);
-  k_conv3x3_wgrad<NJ><<<grid, 128, 0, st>>>(dz, cout, x, dw, N, H, W, (int)ppc);
+  const long long ppc = wgrad_pix_per_chunk(P);
+  const unsigned chunks = (unsigned)((P + ppc - 1) / ppc);
+  dim3 grid(chunks, 9, (cout + 63) / 64);
+  k_conv3x3_wgrad<NJ><<<grid, 128, 0, st>>>(dz, cout, x, part, N, H, W, (int)ppc);
+  noted();
+  const long long len = (long long)cout * 9 * 8 * NJ;
+  k_reduce_rows<<<blocks_for(len), kEw, 0, st>>>(part, (int)chunks, len, dw);
+  noted();
+}
+
+// Channel sums into out[C] (overwritten), in a fixed order.
+void chan_sum(const bf16 *a, const float *wgt, long long P, int C, float *out, float *part, cudaStream_t st) {
+  k_chan_dot<<<kRedBlocks, kEw, 0, st>>>(a, wgt, P, C, part);
+  noted();
+  k_reduce_rows<<<1, kEw, 0, st>>>(part, kRedBlocks, C, out);
   noted();
 }
 
@@ -542,16 +610,24 @@ void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, v
   }
 }
 
-void launch_conv3x3_wgrad(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, int N, int H,
-                          int W, cudaStream_t st) {
+size_t conv3x3_wgrad_scratch(int cout, int cin, int N, int H, int W) {
+  const long long P = (long long)N * H * W;
+  const long long ppc = wgrad_pix_per_chunk(P);
+  return (size_t)((P + ppc - 1) / ppc) * cout * 9 * cin;
+}
+
+void launch_conv3x3_wgrad(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, float *scratch,
+                          size_t scratch_floats, int N, int H, int W, cudaStream_t st) {
   SWFWI_REQUIRE(cout > 0 && cout % 16 == 0, "conv widths must be multiples of 16");
+  SWFWI_REQUIRE(scratch && scratch_floats >= conv3x3_wgrad_scratch(cout, cin, N, H, W),
+                "weight gradient scratch too small");
   switch (cin) {
-    case 16: wgrad_go<2>(dz, cout, x, dw, N, H, W, st); break;
-    case 32: wgrad_go<4>(dz, cout, x, dw, N, H, W, st); break;
-    case 48: wgrad_go<6>(dz, cout, x, dw, N, H, W, st); break;
-    case 64: wgrad_go<8>(dz, cout, x, dw, N, H, W, st); break;
-    case 96: wgrad_go<12>(dz, cout, x, dw, N, H, W, st); break;
-    case 128: wgrad_go<16>(dz, cout, x, dw, N, H, W, st); break;
+    case 16: wgrad_go<2>(dz, cout, x, dw, scratch, N, H, W, st); break;
+    case 32: wgrad_go<4>(dz, cout, x, dw, scratch, N, H, W, st); break;
+    case 48: wgrad_go<6>(dz, cout, x, dw, scratch, N, H, W, st); break;
+    case 64: wgrad_go<8>(dz, cout, x, dw, scratch, N, H, W, st); break;
+    case 96: wgrad_go<12>(dz, cout, x, dw, scratch, N, H, W, st); break;
+    case 128: wgrad_go<16>(dz, cout, x, dw, scratch, N, H, W, st); break;
     default: throw Error(SWFWI_ERR_BAD_ARG, "weight gradient: input width must be 16/32/48/64/96/128");
   }
 }
@@ -596,7 +672,7 @@ Preconditioner::Preconditioner(const int widths[4]) {
   v_.resize(nparam_);
   wbf_.resize(nparam_);
   wflip_.resize(maxw);
-  red_.resize(8);
+  red_.resize(8 + 4 * 256);   // loss, statistics and their per-block partials
   // He-uniform conv weights, zero biases, small output layer (seeded)
   std::vector<float> h(nparam_, 0.0f);
   std::mt19937 gen(12345u);
@@ -708,9 +784,9 @@ void Preconditioner::conv_bwd(int l, const bf16 *in, const bf16 *out, const floa
   const long long P = (long long)N_ * H * W;
   k_relu_mask<<<blocks_for(P * s.cout), kEw, 0, st_>>>(dY, out, dz_.get(), P * s.cout);
   noted();
-  k_chan_dot<<<blocks_for(P * s.cout), kEw, 0, st_>>>(dz_.get(), nullptr, P, s.cout, grads_.get() + s.b_off);
-  noted();
-  launch_conv3x3_wgrad(dz_.get(), s.cout, in, s.cin, grads_.get() + s.w_off, N_, H, W, st_);
+  chan_sum(dz_.get(), nullptr, P, s.cout, grads_.get() + s.b_off, part_.get(), st_);
+  launch_conv3x3_wgrad(dz_.get(), s.cout, in, s.cin, grads_.get() + s.w_off, part_.get(), part_.size(), N_, H, W,
+                       st_);
   if (dX) {
     k_flip<<<blocks_for((long long)s.cout * 9 * s.cin), kEw, 0, st_>>>(wbf_.get() + s.w_off, wflip_.get(),
                                                                         s.cout, s.cin);
@@ -735,14 +811,24 @@ double Preconditioner::backward(const float *t) {
   dS1_.resize(P1 * c1);
   dS2_.resize(P2 * c2);
   dz_.resize(big);
+  size_t need = (size_t)kRedBlocks * 64;
+  {
+    const int hw[4][2] = {{H, W}, {H1, W1}, {H2, W2}, {H3, W3}};
+    const int level[kConvs] = {0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0};
+    for (int l = 0; l < kConvs; l++)
+      need = std::max(need, conv3x3_wgrad_scratch(conv_[l].cout, conv_[l].cin, N, hw[level[l]][0],
+                                                  hw[level[l]][1]));
+  }
+  part_.resize(need);
   grads_.zero(st_);
   red_.zero(st_);
   k_mse<<<blocks_for(P0), kEw, 0, st_>>>(y_.get(), t, dy_.get(), P0, 2.0f / (float)P0, red_.get());
   noted();
   // output layer
-  k_chan_dot<<<blocks_for(P0 * c0), kEw, 0, st_>>>(u0_.get(), dy_.get(), P0, c0, grads_.get() + out_w_);
+  chan_sum(u0_.get(), dy_.get(), P0, c0, grads_.get() + out_w_, part_.get(), st_);
+  k_sum<<<kRedBlocks, kEw, 0, st_>>>(dy_.get(), P0, part_.get());
   noted();
-  k_sum<<<blocks_for(P0), kEw, 0, st_>>>(dy_.get(), P0, grads_.get() + out_b_);
+  k_reduce_rows<<<1, kEw, 0, st_>>>(part_.get(), kRedBlocks, 1, grads_.get() + out_b_);
   noted();
   k_out_bwd_dx<<<blocks_for(P0 * c0), kEw, 0, st_>>>(dy_.get(), params_.get() + out_w_, dA_.get(), P0, c0);
   noted();
@@ -810,16 +896,23 @@ double Preconditioner::train_step(const float *x, const float *t, int N, int H, 
   return loss;
 }
 
+void Preconditioner::stats(const float *a, const float *b, const float *c, int nzpad, int x0, int z0, int nx,
+                           int nz) {
+  constexpr int blocks = 256;
+  red_.resize(8 + 4 * blocks);
+  k_stats<<<blocks, kEw, 0, st_>>>(a, b, c, nzpad, x0, z0, nx, nz, red_.get() + 8);
+  noted();
+  k_stats_final<<<1, 1, 0, st_>>>(red_.get() + 8, blocks, red_.get());
+  noted();
+}
+
 void Preconditioner::features(const float *grad, const float *vel, const float *illum, int nxpad,
                               int nzpad, int bx0, int bxn, int bz0, int bzn, float *x3) {
   SWFWI_REQUIRE(grad && vel && x3, "null field");
   const int nx = nxpad - bx0 - bxn, nz = nzpad - bz0 - bzn;
   SWFWI_REQUIRE(nx > 0 && nz > 0, "empty interior");
   const int Hp = roundup8(nx), Wp = roundup8(nz);
-  red_.zero(st_);
-  k_stats<<<blocks_for((long long)nx * nz), kEw, 0, st_>>>(grad, vel, illum, nzpad, bx0, bz0, nx, nz,
-                                                             red_.get());
-  noted();
+  stats(grad, vel, illum, nzpad, bx0, bz0, nx, nz);
   k_features<<<blocks_for((long long)Hp * Wp), kEw, 0, st_>>>(grad, vel, illum, nzpad, bx0, bz0, nx, nz, Hp,
                                                                 Wp, red_.get(), x3);
   noted();
@@ -831,10 +924,7 @@ void Preconditioner::target(const float *dv, int nxpad, int nzpad, int bx0, int 
   const int nx = nxpad - bx0 - bxn, nz = nzpad - bz0 - bzn;
   SWFWI_REQUIRE(nx > 0 && nz > 0, "empty interior");
   const int Hp = roundup8(nx), Wp = roundup8(nz);
-  red_.zero(st_);
-  k_stats<<<blocks_for((long long)nx * nz), kEw, 0, st_>>>(dv, nullptr, nullptr, nzpad, bx0, bz0, nx, nz,
-                                                             red_.get());
-  noted();
+  stats(dv, nullptr, nullptr, nzpad, bx0, bz0, nx, nz);
   k_target<<<blocks_for((long long)Hp * Wp), kEw, 0, st_>>>(dv, nzpad, bx0, bz0, nx, nz, Hp, Wp, red_.get(), t);
   noted();
 }

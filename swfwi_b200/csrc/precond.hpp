@@ -95,10 +95,13 @@ class Preconditioner {
   // backward scratch
   DevBuf<float> dy_, dA_, dB_, dS0_, dS1_, dS2_, dLow_, dCat_;
   DevBuf<__nv_bfloat16> dz_;
+  DevBuf<float> part_;   // per-chunk / per-block partial sums of the gradients
   DevBuf<double> red_;
   DevBuf<float> feat_, outimg_;
 
   void refresh_bf16();
+  // interior statistics of a, b, c into red_[0..3] (fixed summation order)
+  void stats(const float *a, const float *b, const float *c, int nzpad, int x0, int z0, int nx, int nz);
   void conv_fwd(int l, const __nv_bfloat16 *in, __nv_bfloat16 *out, long long P, int H, int W);
   // dY (FP32, layer output grad) -> parameter grads; dX (FP32, may be null)
   void conv_bwd(int l, const __nv_bfloat16 *in, const __nv_bfloat16 *out, const float *dY, float *dX,
@@ -109,8 +112,12 @@ class Preconditioner {
 void launch_conv3x3(const __nv_bfloat16 *in, int cin, const __nv_bfloat16 *w, const float *bias,
                     void *out, bool out_f32, bool accum, int cout, int N, int H, int W,
                     cudaStream_t st);
+// dw [cout][3][3][cin] (overwritten) from per-chunk partials in scratch
+// (at least conv3x3_wgrad_scratch floats), summed in a fixed order.
+size_t conv3x3_wgrad_scratch(int cout, int cin, int N, int H, int W);
 void launch_conv3x3_wgrad(const __nv_bfloat16 *dz, int cout, const __nv_bfloat16 *x, int cin,
-                          float *dw, int N, int H, int W, cudaStream_t st);
+                          float *dw, float *scratch, size_t scratch_floats, int N, int H, int W,
+                          cudaStream_t st);
 // Illumination: illum[x*nzpad + z] += sum over n slots of p^2 (pitched
 // fields at fstride).
 void launch_illum_accum(float *illum, const float *p, long long fstride, int n, int nxpad, int nzpad,

@@ -197,3 +197,19 @@ def test_learned_epoch_falls_back_and_keeps_decrease(cuda):
     ess = S.EssFwiFramework(m, g["exvel_init"], s.vmin, s.vmax, s.nita, s.maxdv, g["wlt"], g["dobs"])
     with pytest.raises(S.SwfwiError):
         ess.setPreconditioner(net)
+
+
+def test_training_is_bit_reproducible(cuda):
+    # gradients are summed in a fixed order (no atomics): two trainings from
+    # the same start on the same data give the same weights bit for bit
+    torch = cuda
+    rng = np.random.default_rng(21)
+    x = torch.from_numpy(rng.standard_normal((3, 24, 40, 3)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((3, 24, 40)).astype(np.float32)).cuda()
+    finals = []
+    for _ in range(2):
+        net, _ = make_net()
+        for _ in range(5):
+            net.train_step(x, t, 1e-3)
+        finals.append(net.params())
+    np.testing.assert_array_equal(finals[0], finals[1])
