@@ -1,9 +1,11 @@
 """Autotuner for the streaming stencil's launch shape.
 
-The streaming step (``stream.cuh``) has four knobs that do not change its
-results: which kernel (streaming, or warp-specialised streaming with a copy
-warp), output depths per CTA, rows per CTA, rows in flight ahead of the
-compute and the launch order (shots slowest or fastest).  ``tune`` times short batched forward runs of a survey for each
+The streaming step (``stream.cuh``) has knobs that do not change its
+results: which kernel (streaming; warp-specialised with a copy warp, with
+two rows per step, or with the previous field read from global memory;
+independent consumer warps), output depths per CTA, rows per CTA, rows in
+flight ahead of the compute and the launch order (shots slowest or
+fastest).  ``tune`` times short batched forward runs of a survey for each
 candidate with the library's CUDA-event step timing and returns the fastest;
 ``apply`` sets it on a propagator.
 """
@@ -23,6 +25,9 @@ def candidates(nz: int):
     for bz, rows, depth, order in itertools.product((120, 248, 376), (48, 64, 128), (3, 7), (False, True)):
         yield {"kernel": 1, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": order}
+    for bz, rows, depth in itertools.product((248, 376), (48, 64, 128), (3, 7)):
+        yield {"kernel": 4, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
+               "shots_slowest": False}
     for bz, rows, depth in itertools.product((248, 376), (48, 64, 128), (3, 7)):
         yield {"kernel": 3, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": False}

@@ -205,8 +205,8 @@ int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on) {
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest) {
   return guarded([&] {
-    SWFWI_REQUIRE(kernel >= 0 && kernel <= 3, "kernel must be 0, 1, 2 or 3");
-    if (kernel == 3) {
+    SWFWI_REQUIRE(kernel >= 0 && kernel <= 4, "kernel must be 0, 1, 2, 3 or 4");
+    if (kernel == 3 || kernel == 4) {
       SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,
                     "band depth must be 120, 248 or 376");
       SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");

@@ -73,7 +73,8 @@ class Propagator {
   cudaStream_t stream() const { return st_; }
   int arith = ARITH_REF;
   int strip_format = SWFWI_STRIP_F32;
-  int stream_kernel = 1;      // 0: streaming step, 1: warp-specialised, 2: independent warps
+  int stream_kernel = 1;      // 0: streaming, 1: warp-specialised, 2: independent warps,
+                              // 3: two rows per step, 4: prev / 1/vt from global memory
   int stream_bz = 376;        // output depths per CTA (120, 248; 376 warp-specialised only)
   int stream_xchunk = 64;     // rows per CTA
   int stream_depth = 3;       // rows ahead (3 or 5; warp-specialised 3 or 7)

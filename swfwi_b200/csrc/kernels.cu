@@ -668,7 +668,7 @@ static void stream_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStr
 template <int ARITH, bool DAMPED, int NW, int D, int EPI>
 static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
   constexpr int BZ = 128 * NW - 8;
-  constexpr size_t smem = ws_smem_bytes<NW, D>();
+  constexpr size_t smem = ws_smem_bytes<NW, D, EPI>();
   static bool attr_set = false;   // raise the dynamic shared memory limit once
   if (!attr_set) {
     cudaFuncSetAttribute(fd_step_ws<ARITH, DAMPED, NW, D, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -682,10 +682,14 @@ static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
 }
 
 template <int ARITH, bool DAMPED, int NW, int D>
-static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st, bool global_prev) {
   const Epilogue &e = a.epi;
   const int mode = (e.sub || e.image) ? 2 : (e.inj ? 3 : 0);
   if (mode == 2 && e.inj) throw Error(SWFWI_ERR_BAD_ARG, "mixed fused epilogue parts");
+  if (global_prev) {
+    if (mode) throw Error(SWFWI_ERR_BAD_ARG, "the global-prev step has no fused epilogue");
+    return ws_launch<ARITH, DAMPED, NW, D, 4>(a, nslots, st);
+  }
   if constexpr (NW == 3) {
     if (mode == 2) return ws_launch<ARITH, DAMPED, NW, D, 2>(a, nslots, st);
     if (mode == 3) return ws_launch<ARITH, DAMPED, NW, D, 3>(a, nslots, st);
@@ -696,27 +700,27 @@ static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
 }
 
 template <int ARITH, bool DAMPED, int D>
-static void ws_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
-  if (bz >= 376) ws_t<ARITH, DAMPED, 3, D>(a, nslots, st);
-  else if (bz >= 248) ws_t<ARITH, DAMPED, 2, D>(a, nslots, st);
-  else ws_t<ARITH, DAMPED, 1, D>(a, nslots, st);
+static void ws_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st, bool gp) {
+  if (bz >= 376) ws_t<ARITH, DAMPED, 3, D>(a, nslots, st, gp);
+  else if (bz >= 248) ws_t<ARITH, DAMPED, 2, D>(a, nslots, st, gp);
+  else ws_t<ARITH, DAMPED, 1, D>(a, nslots, st, gp);
 }
 
 template <int ARITH, bool DAMPED>
-static void ws_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
-  if (depth >= 7) ws_nw<ARITH, DAMPED, 7>(bz, a, nslots, st);
-  else ws_nw<ARITH, DAMPED, 3>(bz, a, nslots, st);
+static void ws_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st, bool gp) {
+  if (depth >= 7) ws_nw<ARITH, DAMPED, 7>(bz, a, nslots, st, gp);
+  else ws_nw<ARITH, DAMPED, 3>(bz, a, nslots, st, gp);
 }
 
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
-                    cudaStream_t st) {
+                    cudaStream_t st, bool global_prev) {
   if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
   if (arith == ARITH_REF) {
-    if (damped) ws_d<ARITH_REF, true>(depth, bz, a, nslots, st);
-    else ws_d<ARITH_REF, false>(depth, bz, a, nslots, st);
+    if (damped) ws_d<ARITH_REF, true>(depth, bz, a, nslots, st, global_prev);
+    else ws_d<ARITH_REF, false>(depth, bz, a, nslots, st, global_prev);
   } else {
-    if (damped) ws_d<ARITH_FAST, true>(depth, bz, a, nslots, st);
-    else ws_d<ARITH_FAST, false>(depth, bz, a, nslots, st);
+    if (damped) ws_d<ARITH_FAST, true>(depth, bz, a, nslots, st, global_prev);
+    else ws_d<ARITH_FAST, false>(depth, bz, a, nslots, st, global_prev);
   }
   note_launch();
 }

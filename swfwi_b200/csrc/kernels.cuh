@@ -70,9 +70,10 @@ void launch_step(int arith, bool damped, bool vel_is_rcp, int tx, const StepArgs
 void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamArgs &a,
                         int nslots, cudaStream_t st);
 // Warp-specialised streaming step (stream_ws.cuh): bz = 120, 248 or 376
-// output depths per CTA (1-3 consumer warps), depth = 3 or 7 rows ahead.
+// output depths per CTA (1-3 consumer warps), depth = 3 or 7 rows ahead;
+// global_prev: the previous field and 1/vt come from global memory.
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
-                    cudaStream_t st);
+                    cudaStream_t st, bool global_prev = false);
 // Streaming step with independent consumer warps (stream_wi.cuh): bz = 240,
 // 360 or 480 output depths per CTA (2-4 consumer warps of 120), depth = 3
 // or 7 rows ahead.

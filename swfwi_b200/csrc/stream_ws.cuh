@@ -59,23 +59,32 @@ struct Smem {
 
 }  // namespace ws_detail
 
-// D rows ahead: the prev/velocity ring has D + 1 slots (D = 3 or 7).
-template <int NW, int D>
+// D rows ahead: the prev/velocity ring has D + 1 slots (D = 3 or 7); the
+// variant EPI 4 has no such ring.
+template <int NW, int D, int EPI = 0>
 constexpr size_t ws_smem_bytes() {
-  return ws_detail::Smem<NW * 32, D + 1>::bytes;
+  return ws_detail::Smem<NW * 32, EPI == 4 ? 0 : D + 1>::bytes;
 }
 
 // EPI: also run part of a.epi at the output points with the new values
 // before they are stored: 2 = source subtraction and imaging (source
-// back-step); 3 = next injection (receiver step).
+// back-step); 3 = next injection (receiver step).  EPI 4: the plain step
+// with the previous field and 1/vt read by the consumers from global memory
+// (each value is used once, at its output point; the loads are issued at
+// the start of the step so their latency overlaps the u2 work) instead of
+// staged in a shared-memory ring: 12 KB less shared memory per CTA, room
+// for a sixth CTA per SM.
 template <int ARITH, bool DAMPED, int NW, int D, int EPI = 0>
-__global__ void __launch_bounds__((NW + 1) * 32, EPI ? (ARITH == ARITH_REF ? 4 : 5) : 1)
+__global__ void __launch_bounds__((NW + 1) * 32,
+                                  (EPI == 2 || EPI == 3) ? (ARITH == ARITH_REF ? 4 : 5) : (EPI == 4 ? 6 : 1))
 fd_step_ws(StreamArgs a) {
   using namespace ws_detail;
   constexpr int NT = NW * 32;      // consumer threads
+  constexpr bool GPV = EPI == 4;   // prev / 1/vt from global memory
   constexpr int NP = D + 1;
   static_assert(NP == 4 || NP == 8, "the prev/vel ring must divide the current ring");
-  using L = Smem<NT, NP>;
+  constexpr int NPR = GPV ? 0 : NP;   // prev/vel ring rows allocated
+  using L = Smem<NT, NPR>;
   constexpr int BZ = L::BZ, WC = L::WC, WP = L::WP, NC = L::NC;
   extern __shared__ __align__(128) unsigned char smem[];
   float(*cring)[WC] = reinterpret_cast<float(*)[WC]>(smem + L::c_off);
@@ -85,7 +94,7 @@ fd_step_ws(StreamArgs a) {
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::b_off);
   uint64_t *emptyc = full + NC;
   uint64_t *emptyp = emptyc + NC;
-  int *s_fail = reinterpret_cast<int *>(emptyp + NP);
+  int *s_fail = reinterpret_cast<int *>(emptyp + NPR);
 
   const int tid = threadIdx.x;
   const int shot = a.shot_major ? blockIdx.z : blockIdx.x;
@@ -103,7 +112,7 @@ fd_step_ws(StreamArgs a) {
       mbar_init(&full[i], 1);
       mbar_init(&emptyc[i], 1);
     }
-    for (int i = 0; i < NP; i++) mbar_init(&emptyp[i], 1);
+    for (int i = 0; i < NPR; i++) mbar_init(&emptyp[i], 1);
     fence_mbar_init();
     *s_fail = 0;
   }
@@ -125,10 +134,10 @@ fd_step_ws(StreamArgs a) {
         *(volatile int *)s_fail = 1;
         break;
       }
-      const bool pv = k >= 12;
+      const bool pv = !GPV && k >= 12;
       const int ps = (k - 12) & (NP - 1);
       if (pv && k - 12 >= NP &&
-          !mbar_wait(&emptyp[ps], (uint32_t)((((k - 12) / NP) + 1) & 1))) {
+          !mbar_wait(&emptyp[ps & (NPR > 0 ? NPR - 1 : 0)], (uint32_t)((((k - 12) / NP) + 1) & 1))) {
         atomicExch(a.err, 1);
         *(volatile int *)s_fail = 1;
         break;
@@ -136,10 +145,12 @@ fd_step_ws(StreamArgs a) {
       uint64_t *fb = &full[k & (NC - 1)];
       mbar_expect_tx(fb, cbytes + (pv ? 2u * pbytes : 0u));
       bulk_g2s(&cring[k & (NC - 1)][0], curr + (long long)(xa - 6 + k) * P, cbytes, fb);
-      if (pv) {
-        long long off = (long long)(xa - 12 + k) * P;
-        bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
-        bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
+      if constexpr (!GPV) {
+        if (pv) {
+          long long off = (long long)(xa - 12 + k) * P;
+          bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
+          bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
+        }
       }
     }
     return;
@@ -172,7 +183,7 @@ fd_step_ws(StreamArgs a) {
   int hit_d = -1, hit_x = -1, hit_i = 0, hit_di = 0, hit_dx = 0, hit_left = 0;
   const float *hit_vals = nullptr;
   int hit_stride = 0;
-  if constexpr (EPI != 0) {
+  if constexpr (EPI == 2 || EPI == 3) {
     const float *vals = EPI == 2 ? a.epi.sub : a.epi.inj;
     if (vals && outgroup) {
       const PtLine l = a.epi.src[shot];
@@ -216,7 +227,18 @@ fd_step_ws(StreamArgs a) {
     // fused imaging: this step's receiver field and image values, loaded
     // early so their latency overlaps the update
     float4 gimg = make_float4(0.f, 0.f, 0.f, 0.f), vimg = gimg;
-    if constexpr (EPI != 0) {
+    float4 p4g = gimg, r4g = gimg;
+    if constexpr (GPV) {
+      // every outgroup lane's 4 depths lie inside the pitched row (halo and
+      // pad included), 16-byte aligned
+      if (has_out && outgroup) {
+        const long long row = (long long)(xa - 12 + k) * P + zg;
+        p4g = ld4g(a.prev + (long long)shot * a.shot_stride + row);
+        r4g = __ldg(reinterpret_cast<const float4 *>(
+            a.rcp + (long long)(shot / a.shots_per_vel) * a.vel_stride + row));
+      }
+    }
+    if constexpr (EPI == 2 || EPI == 3) {
       if (EPI == 2 && a.epi.image && has_out && outgroup) {
         const long long o = (long long)shot * a.shot_stride + (long long)(xa - 12 + k) * P + zg;
         if (fullgroup) {
@@ -276,9 +298,11 @@ fd_step_ws(StreamArgs a) {
     if (t == 0) {
       if (has_u2) mbar_arrive(&emptyc[cs(-10)]);
       // (stage 11 carries no prev/vel rows: the first release is at step 13)
-      if (k >= 13) {
-        if constexpr (PH >= 0) mbar_arrive(&emptyp[(PH - 13) & (NP - 1)]);
-        else mbar_arrive(&emptyp[(k - 13) & (NP - 1)]);
+      if constexpr (!GPV) {
+        if (k >= 13) {
+          if constexpr (PH >= 0) mbar_arrive(&emptyp[(PH - 13) & (NP - 1)]);
+          else mbar_arrive(&emptyp[(k - 13) & (NP - 1)]);
+        }
       }
     }
     if (has_out && outgroup) {
@@ -287,8 +311,14 @@ fd_step_ws(StreamArgs a) {
       const float *uc = &u2r[us(-1)][4 * t];
       const float *up = &u2r[us(0)][4 * t];
       float4 c4 = ld4(&cring[cs(-6)][8 + 4 * t]);
-      float4 p4 = ld4(&pring[ps][4 * t]);
-      float4 r4 = ld4(&vring[ps][4 * t]);
+      float4 p4, r4;
+      if constexpr (GPV) {
+        p4 = p4g;
+        r4 = r4g;
+      } else {
+        p4 = ld4(&pring[ps][4 * t]);
+        r4 = ld4(&vring[ps][4 * t]);
+      }
       float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
       float ucl = uc[-1], ucr = uc[4];
       float o[4];
@@ -325,7 +355,7 @@ fd_step_ws(StreamArgs a) {
                                   get(um4, i), get(up4, i), delta);
         }
       }
-      if constexpr (EPI != 0) {
+      if constexpr (EPI == 2 || EPI == 3) {
         if (hit_left > 0 && xa - 12 + k == hit_x) {
           const float v = hit_vals[(long long)hit_i * hit_stride];
 #pragma unroll

@@ -29,7 +29,8 @@ def test_calgradient_ess_bit_exact(cuda):
 
 
 @pytest.mark.parametrize("tuning", [None, (1, 248, 7, 3, 1), (2, 360, 64, 3, 0), (2, 240, 5, 7, 1),
-                                    (3, 376, 64, 7, 0), (3, 248, 9, 3, 1)])
+                                    (3, 376, 64, 7, 0), (3, 248, 9, 3, 1), (4, 376, 64, 3, 0),
+                                    (4, 248, 9, 7, 1)])
 def test_gradient_batch_matches_reference_loop(cuda, tuning):
     # the per-shot loop of FwiFramework::epoch: gradient bit-exact, the
     # objective summed in FP64 (the reference sums in float); with the
