@@ -293,6 +293,20 @@ int swfwi_fwi_set_velocity(swfwi_fwi *h, const float *exvel);
 /* sfWriteVel (damp4t10d.cpp:254-265) without the file: interior velocity in
  * m/s, host [nx][nz]. */
 int swfwi_fwi_write_vel(swfwi_fwi *h, float *vel);
+/* EssFwiRegu (src/unused/essfwiregu.cpp:667-776) on an encoded framework:
+ * every objective adds lx Wx2 + lz Wz2 of the padded transformed model
+ * (ReguFactor, src/unused/ReguFactor.cpp), the gradient adds the factor's
+ * gradient before the mask and is not depth-scaled, and the step is taken
+ * along the gradient itself.  lx = lz = 0 (default) is the plain encoded
+ * epoch. */
+int swfwi_fwi_set_regularization(swfwi_fwi *h, float lx, float lz);
+/* ReguFactor on a DEVICE model vel [nx][nz]: term (host, FP64 sums of the
+ * float squares; the reference sums in float) and the gradient written, or
+ * added when accumulate = 1, into grad (DEVICE) exactly as the reference's
+ * loops leave it.  Synchronises. */
+int swfwi_regu_term(const float *vel, int nx, int nz, float lx, float lz, double *term, void *stream);
+int swfwi_regu_gradient(const float *vel, int nx, int nz, float lx, float lz, float *grad, int accumulate,
+                        void *stream);
 /* last epoch's step length and trial record: alpha[4], obj[4] (host) */
 int swfwi_fwi_last_line_search(const swfwi_fwi *h, float *alpha, float *obj);
 

@@ -95,6 +95,7 @@ class RefLib:
             "ref_cal_objective": [_fp, C.c_int],
             "ref_parabola_vertex": [C.c_float] * 7 + [_fp, _fp],
             "ref_ricker": [_fp, C.c_int, C.c_float, C.c_float, C.c_float],
+            "ref_regu": [_fp, C.c_int, C.c_int, C.c_float, C.c_float, _fp, _fp],
             "ref_random_codes": [C.c_int, C.c_int, C.c_int, _ip],
             "ref_ess_fwi_run": [vp, _fp, _fp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, _fp, _fp],
             "ref_fwi_run": [vp, _fp, _fp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, _fp, _fp],
@@ -158,6 +159,16 @@ class RefLib:
         w = np.zeros(nt, np.float32)
         self.lib.ref_ricker(fptr(w), nt, fm, dt, amp)
         return w
+
+    def regu(self, vel: np.ndarray, lx: float, lz: float):
+        """ReguFactor (src/unused/ReguFactor.cpp) on vel [nx][nz]: (term,
+        gradient [nx][nz])."""
+        v = np.ascontiguousarray(vel, np.float32)
+        nx, nz = v.shape
+        term = np.zeros(1, np.float32)
+        g = np.zeros_like(v)
+        self.lib.ref_regu(fptr(v), nx, nz, lx, lz, fptr(term), fptr(g))
+        return float(term[0]), g
 
     def random_codes(self, seed, ns, skip=0):
         c = np.zeros(ns, np.int32)

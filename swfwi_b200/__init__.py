@@ -139,6 +139,9 @@ _SIGS = {
     "swfwi_precond_propose": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "swfwi_fwi_set_preconditioner": [_vp, _vp],
     "swfwi_fwi_collect_illumination": [_vp, C.c_int],
+    "swfwi_fwi_set_regularization": [_vp, C.c_float, C.c_float],
+    "swfwi_regu_term": [_vp, C.c_int, C.c_int, C.c_float, C.c_float, _dp, _vp],
+    "swfwi_regu_gradient": [_vp, C.c_int, C.c_int, C.c_float, C.c_float, _vp, C.c_int, _vp],
     "swfwi_fwi_set_learned_min_decrease": [_vp, C.c_float],
     "swfwi_fwi_set_learned_patience": [_vp, C.c_int],
     "swfwi_fwi_get_gradient": [_vp, _fp],
@@ -378,6 +381,21 @@ class EnkfAnalyze:
         mean = torch.empty(vels.shape[1:], dtype=torch.float32, device=vels.device)
         enkf_mean(mean, vels)
         return mean
+
+
+def regu_term(vel, lx: float, lz: float, stream=None) -> float:
+    """ReguFactor::getReguTerm (src/unused/ReguFactor.cpp:19-27) of a CUDA
+    model [nx][nz]: lx Wx2 + lz Wz2 (FP64 sums)."""
+    nx, nz = vel.shape
+    out = C.c_double()
+    _check(lib().swfwi_regu_term(_ptr(vel), nx, nz, lx, lz, C.byref(out), _stream(stream)))
+    return out.value
+
+
+def regu_gradient(vel, lx: float, lz: float, grad, accumulate: bool = False, stream=None) -> None:
+    """ReguFactor::getReguGradient (:67-108) into (or added to) grad."""
+    nx, nz = vel.shape
+    _check(lib().swfwi_regu_gradient(_ptr(vel), nx, nz, lx, lz, _ptr(grad), int(accumulate), _stream(stream)))
 
 
 def cal_objective_static(r, out, stream=None) -> None:
@@ -711,3 +729,8 @@ class FwiFramework(_Framework):
 class EssFwiFramework(_Framework):
     """Encoded simultaneous-source FWI (src/essfwi/essfwiframework.h)."""
     encoded = 1
+
+    def setRegularization(self, lambda_x: float, lambda_z: float):
+        """EssFwiRegu (src/unused/essfwiregu.h): epochs with the first-difference
+        regularisation lx Wx2 + lz Wz2 (0, 0: the plain encoded epoch)."""
+        _check(lib().swfwi_fwi_set_regularization(self.h, lambda_x, lambda_z))

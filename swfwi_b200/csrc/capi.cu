@@ -792,6 +792,32 @@ int swfwi_fwi_set_learned_patience(swfwi_fwi *h, int rejections) {
   });
 }
 
+int swfwi_fwi_set_regularization(swfwi_fwi *h, float lx, float lz) {
+  return guarded([&] { R(h).set_regularization(lx, lz); });
+}
+
+int swfwi_regu_term(const float *vel, int nx, int nz, float lx, float lz, double *term, void *stream) {
+  return guarded([&] {
+    SWFWI_REQUIRE(vel && term && nx > 0 && nz > 0, "bad regularisation arguments");
+    DevBuf<double> sc(regu_scratch_doubles());
+    launch_regu_term(vel, nx, nz, lx, lz, sc.get(), as_stream(stream));
+    check_launch();
+    double h[3];
+    SWFWI_CUDA(cudaMemcpyAsync(h, sc.get(), sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream)));
+    SWFWI_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    *term = h[2];
+  });
+}
+
+int swfwi_regu_gradient(const float *vel, int nx, int nz, float lx, float lz, float *grad, int accumulate,
+                        void *stream) {
+  return guarded([&] {
+    SWFWI_REQUIRE(vel && grad && nx > 0 && nz > 0, "bad regularisation arguments");
+    launch_regu_grad(vel, nx, nz, lx, lz, grad, accumulate != 0, as_stream(stream));
+    check_launch();
+  });
+}
+
 int swfwi_fwi_collect_illumination(swfwi_fwi *h, int on) {
   return guarded([&] { R(h).set_collect_illumination(on != 0); });
 }

@@ -203,8 +203,87 @@ void FwiRunner::update_grad(int iter) {
 }
 
 void FwiRunner::epoch(int iter) {
-  if (encoded_) ess_epoch(iter);
+  if (encoded_ && regu_) regu_epoch(iter);
+  else if (encoded_) ess_epoch(iter);
   else plain_epoch(iter);
+}
+
+void FwiRunner::set_regularization(float lx, float lz) {
+  SWFWI_REQUIRE(encoded_, "regularisation applies to the encoded-source framework");
+  SWFWI_REQUIRE(lx >= 0.0f && lz >= 0.0f && std::isfinite(lx) && std::isfinite(lz),
+                "regularisation weights must be finite and non-negative");
+  regu_lx_ = lx;
+  regu_lz_ = lz;
+  regu_ = lx > 0.0f || lz > 0.0f;
+}
+
+// ReguFactor::getReguTerm of a padded model (FP64 sums, returned as the
+// float the reference adds to its objective).
+float FwiRunner::regu_term(const float *vel) {
+  regu_scratch_.resize(regu_scratch_doubles());
+  double *sc = regu_scratch_.get();
+  launch_regu_term(vel, p_.nxpad, p_.nzpad, regu_lx_, regu_lz_, sc, p_.stream());
+  double h[3];
+  SWFWI_CUDA(cudaMemcpyAsync(h, sc, sizeof(h), cudaMemcpyDeviceToHost, p_.stream()));
+  SWFWI_CUDA(cudaStreamSynchronize(p_.stream()));
+  return (float)h[2];
+}
+
+// EssFwiRegu::epoch (src/unused/essfwiregu.cpp:667-776).  The reference
+// restores the source field from disk checkpoints every 50 steps (hello,
+// :217-349); this restores it from the boundary strips like calgradient.
+// The step length is the framework's UpdateSteplenOp search over the
+// regularised objective (calculate_obj_val :405-449 adds the trial model's
+// term).
+void FwiRunner::regu_epoch(int iter) {
+  cudaStream_t st = p_.stream();
+  p_.bind_velocity(vel_.get());
+  const int nt = p_.nt, ns = p_.ns, ng = p_.ng;
+  long long dn = (long long)nt * ng;
+  std::vector<int> codes = codes_gen_.gen_plus1_minus1(ns);
+  codes_.upload(codes, st);
+  encsrc_.resize((size_t)nt * ns);
+  encobs_.resize(dn);
+  dcal_.resize(dn);
+  vsrc_.resize(dn);
+  res_.resize(dn);
+  launch_encode_source(encsrc_.get(), wlt_.get(), codes_.get(), nt, ns, st);
+  launch_encode_obs(encobs_.get(), dobs_.get(), codes_.get(), dn, ns, st);
+  p_.ess_forward(encsrc_.get(), dcal_.get());
+  p_.remove_direct_arrival(encobs_.get(), -1);
+  p_.remove_direct_arrival(dcal_.get(), -1);
+  launch_residual(res_.get(), encobs_.get(), 0, dcal_.get(), dn, 1, st);
+  float obj1 = (float)sumsq(res_.get(), dn);
+  obj1 += regu_term(vel_.get());
+  if (iter == 0) init_obj = obj1;
+  launch_trans_vsrc(vsrc_.get(), res_.get(), nt, ng, 1, st);
+  g_.zero(st);
+  p_.calgradient_ess(encsrc_.get(), vsrc_.get(), g_.get());
+  launch_regu_grad(vel_.get(), p_.nxpad, p_.nzpad, regu_lx_, regu_lz_, g_.get(), true, st);
+  p_.mask_gradient(g_.get());
+  SWFWI_CUDA(cudaMemcpyAsync(dir_.get(), g_.get(), sizeof(float) * n_, cudaMemcpyDeviceToDevice, st));
+
+  launch_max_alpha(reinterpret_cast<float *>(scratch_.get()), vel_.get(), dir_.get(), n_, p_.dt,
+                   p_.dx, search.maxdv, st);
+  float a2max = 0;
+  SWFWI_CUDA(cudaMemcpyAsync(&a2max, scratch_.get(), sizeof(float), cudaMemcpyDeviceToHost, st));
+  SWFWI_CUDA(cudaStreamSynchronize(st));
+  float a3max = 2 * a2max;
+  auto f = [&](float alpha) -> float {
+    launch_update_vel(trial_.get(), vel_.get(), dir_.get(), n_, alpha, vmin_t_, vmax_t_, st);
+    p_.ess_forward(encsrc_.get(), dcal_.get(), trial_.get());
+    p_.remove_direct_arrival(dcal_.get(), -1, trial_.get());
+    launch_residual(res_.get(), encobs_.get(), 0, dcal_.get(), dn, 1, st);
+    float v = (float)sumsq(res_.get(), dn);
+    return v + regu_term(trial_.get());
+  };
+  float objv = 0;
+  float step = search.calsteplen(f, obj1, a3max, objv);
+  update_obj = objv;
+  launch_update_vel(vel_.get(), vel_.get(), dir_.get(), n_, step, vmin_t_, vmax_t_, st);
+  launch_refill_boundary(vel_.get(), p_.nxpad, p_.nzpad, p_.bz0, p_.bzn, p_.bx0, p_.bxn, st);
+  p_.bind_velocity(vel_.get());
+  SWFWI_CUDA(cudaStreamSynchronize(st));
 }
 
 // FwiFramework::epoch (fwiframework.cpp:269-356) with the documented

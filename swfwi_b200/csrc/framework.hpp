@@ -70,6 +70,12 @@ class FwiRunner {
   // Accumulate the source illumination during the gradient's forward sweep
   // (always on while a network is set).
   void set_collect_illumination(bool on) { collect_illum_ = on; }
+  // EssFwiRegu (src/unused/essfwiregu.cpp:667-776) for an encoded
+  // framework: each objective adds lx Wx2 + lz Wz2 of the model
+  // (ReguFactor, src/unused/ReguFactor.cpp), the gradient adds the factor's
+  // gradient before the mask, it is not depth-scaled, and the direction is
+  // the gradient itself (gradUpdator :66-68).  lx = lz = 0 turns it off.
+  void set_regularization(float lx, float lz);
   void get_gradient(float *host);       // the last epoch's gradient
   void get_illumination(float *host);   // the last epoch's illumination
   int last_step_learned = 0, learned_tried = 0, learned_accepted = 0;
@@ -95,6 +101,11 @@ class FwiRunner {
   bool collect_illum_ = false;
   bool restart_cg_ = false;
   bool try_learned_step(float obj1);
+  float regu_lx_ = 0.0f, regu_lz_ = 0.0f;
+  DevBuf<double> regu_scratch_;
+  bool regu_ = false;
+  void regu_epoch(int iter);
+  float regu_term(const float *vel);
   DevBuf<double> scratch_;
   RandomCodes codes_gen_;
   std::vector<int> ids_;

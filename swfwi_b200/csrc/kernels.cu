@@ -917,4 +917,105 @@ template void launch_image<float>(float *, long long, const float *, const float
 template void launch_image<double>(double *, long long, const double *, const double *, long long,
                                    int, int, float, cudaStream_t);
 
+// ---------------------------------------------------------------- regularisation
+// ReguFactor (src/unused/ReguFactor.cpp) on p [nx][nz].  Sums: per-block FP64
+// partials of the float squares (r * r in float, as :43 and :61) of the x and
+// z first differences, added in a fixed order; the reference adds them in
+// float in loop order.
+namespace {
+constexpr int kReguBlocks = 256;
+
+__global__ void k_regu_sums(const float *__restrict__ p, int nx, int nz, double *__restrict__ part) {
+  double sx = 0.0, sz = 0.0;
+  const long long total = (long long)nx * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(e / nz), iz = (int)(e - (long long)ix * nz);
+    const float v = p[e];
+    if (ix < nx - 1) {
+      const float r = __fsub_rn(p[e + nz], v);
+      sx += (double)__fmul_rn(r, r);
+    }
+    if (iz < nz - 1) {
+      const float r = __fsub_rn(p[e + 1], v);
+      sz += (double)__fmul_rn(r, r);
+    }
+  }
+  __shared__ double red[2][kThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_down_sync(0xffffffffu, sx, o);
+    sz += __shfl_down_sync(0xffffffffu, sz, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = sx;
+    red[1][threadIdx.x >> 5] = sz;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < kThreads / 32; w++) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    part[2 * blockIdx.x] = a;
+    part[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// out: Wx2, Wz2, lx * Wx2 + lz * Wz2 (getReguTerm :19-27)
+__global__ void k_regu_final(const double *__restrict__ part, int blocks, float lx, float lz,
+                             double *__restrict__ out) {
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < blocks; i++) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  out[0] = a;
+  out[1] = b;
+  out[2] = (double)lx * a + (double)lz * b;
+}
+
+// getReguGradient (:67-108) element by element as its loops leave it: the z
+// loop writes into the x-term array, so every element above the last depth
+// holds its z term; the last depth holds the x term (0 on the last row).
+// g = (accumulate ? g + term : term), each operation one float rounding.
+__global__ void k_regu_grad(const float *__restrict__ p, int nx, int nz, float lx, float lz,
+                            float *__restrict__ g, int accumulate) {
+  const float cx = __fmul_rn(2.0f, lx), cz = __fmul_rn(2.0f, lz);
+  const long long total = (long long)nx * nz;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(e / nz), iz = (int)(e - (long long)ix * nz);
+    const float v = p[e];
+    float r = 0.0f;
+    if (iz < nz - 1) {
+      const float d = iz == 0 ? __fsub_rn(v, p[e + 1])
+                              : __fsub_rn(__fsub_rn(__fmul_rn(2.0f, v), p[e + 1]), p[e - 1]);
+      r = __fmul_rn(cz, d);
+    } else if (ix < nx - 1) {
+      const float d = ix == 0 ? __fsub_rn(v, p[e + nz])
+                              : __fsub_rn(__fsub_rn(__fmul_rn(2.0f, v), p[e + nz]), p[e - nz]);
+      r = __fmul_rn(cx, d);
+    }
+    r = __fadd_rn(r, 0.0f);   // + the (all-zero) second term array
+    g[e] = accumulate ? __fadd_rn(g[e], r) : r;
+  }
+}
+}  // namespace
+
+size_t regu_scratch_doubles() { return 3 + 2 * (size_t)kReguBlocks; }
+
+void launch_regu_term(const float *p, int nx, int nz, float lx, float lz, double *scratch, cudaStream_t st) {
+  k_regu_sums<<<kReguBlocks, kThreads, 0, st>>>(p, nx, nz, scratch + 3);
+  note_launch();
+  k_regu_final<<<1, 1, 0, st>>>(scratch + 3, kReguBlocks, lx, lz, scratch);
+  note_launch();
+}
+
+void launch_regu_grad(const float *p, int nx, int nz, float lx, float lz, float *g, bool accumulate,
+                      cudaStream_t st) {
+  k_regu_grad<<<grid_for((long long)nx * nz), kThreads, 0, st>>>(p, nx, nz, lx, lz, g, accumulate ? 1 : 0);
+  note_launch();
+}
+
 }  // namespace swfwi

@@ -157,4 +157,12 @@ void launch_encode_obs(float *encobs, const float *dobs, const int *codes, long 
 void launch_f32_to_f64(double *out, const float *in, long long n, cudaStream_t st);
 void launch_f64_to_f32(float *out, const double *in, long long n, cudaStream_t st);
 
+// ReguFactor (src/unused/ReguFactor.cpp) on p [nx][nz] (device):
+// scratch[0..2] = Wx2, Wz2, lx Wx2 + lz Wz2 in FP64 (scratch holds
+// regu_scratch_doubles()); the gradient written (or added) into g.
+size_t regu_scratch_doubles();
+void launch_regu_term(const float *p, int nx, int nz, float lx, float lz, double *scratch, cudaStream_t st);
+void launch_regu_grad(const float *p, int nx, int nz, float lx, float lz, float *g, bool accumulate,
+                      cudaStream_t st);
+
 }  // namespace swfwi

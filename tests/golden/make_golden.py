@@ -135,8 +135,28 @@ def main():
     ve, objs_e = M3.ess_fwi_run(wlt, dobs, 2, s.nita, s.maxdv, 1500.0, 4700.0)
     np.savez_compressed(os.path.join(HERE, "small_epochs.npz"), fwi_vel=vf, fwi_objs=objs_f, ess_vel=ve,
                         ess_objs=objs_e)
+    regu_fixture(R)
     print("fixtures written to", HERE)
 
 
+def regu_fixture(R=None):
+    """ReguFactor (src/unused/ReguFactor.cpp) on the small survey's padded
+    initial model and on a seeded ragged grid: term and gradient."""
+    R = R or oracle.RefLib()
+    g = np.load(os.path.join(HERE, "small_survey.npz"))
+    v = g["exvel_init"]
+    t1, g1 = R.regu(v, 0.3, 0.7)
+    rng = np.random.default_rng(17)
+    w = rng.uniform(0.2, 3.0, (13, 7)).astype(np.float32)
+    t2, g2 = R.regu(w, 1.5, 0.25)
+    np.savez_compressed(os.path.join(HERE, "regu.npz"), term_small=np.float32(t1), grad_small=g1,
+                        lx_small=np.float32(0.3), lz_small=np.float32(0.7), ragged=w, term_ragged=np.float32(t2),
+                        grad_ragged=g2, lx_ragged=np.float32(1.5), lz_ragged=np.float32(0.25))
+
+
 if __name__ == "__main__":
-    main()
+    import sys
+    if "--regu" in sys.argv:
+        regu_fixture()
+    else:
+        main()
