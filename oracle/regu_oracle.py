@@ -6,9 +6,10 @@ It follows src/unused/ReguFactor.cpp (class ReguFactor):
 
 * getWx2 (:30-47): sum over ix < nx-1, iz < nz of (p[ix+1][iz] - p[ix][iz])^2,
   getWz2 (:49-65): sum over ix < nx, iz < nz-1 of (p[ix][iz+1] - p[ix][iz])^2,
-  getReguTerm (:19-27): lx * Wx2 + lz * Wz2.  The reference sums in float in
-  loop order; this restatement sums in float64 (the sums are compared within
-  a tolerance, like the objective).
+  getReguTerm (:19-27): lx * Wx2 + lz * Wz2.  Each difference and square is
+  formed in float as in the reference's loop body; the reference then sums
+  in float in loop order, this restatement in float64 (the sums are compared
+  within a tolerance, like the objective).
 * getReguGradient (:67-108), element by element in float, exactly as the
   loops leave it: the x loop writes 2 lx (p - p[x+1]) at ix = 0 and
   2 lx (2p - p[x+1] - p[x-1]) for 0 < ix < nx-1; the z loop then writes into
@@ -22,9 +23,13 @@ import numpy as np
 
 
 def regu_term(p: np.ndarray, lx: float, lz: float) -> float:
-    p = np.asarray(p, np.float64)
-    wx2 = float(((p[1:, :] - p[:-1, :]) ** 2).sum())
-    wz2 = float(((p[:, 1:] - p[:, :-1]) ** 2).sum())
+    # each difference and its square in float, as the reference's loop body;
+    # the sum in float64
+    p = np.asarray(p, np.float32)
+    rx = (p[1:, :] - p[:-1, :]).astype(np.float32)
+    rz = (p[:, 1:] - p[:, :-1]).astype(np.float32)
+    wx2 = float((rx * rx).astype(np.float32).astype(np.float64).sum())
+    wz2 = float((rz * rz).astype(np.float32).astype(np.float64).sum())
     return float(np.float32(lx)) * wx2 + float(np.float32(lz)) * wz2
 
 
