@@ -25,6 +25,12 @@ workload.
 
 Multi-GPU: replicas only (the workload runs on one GPU; N ranks run N
 independent copies, value = all ranks' point-updates / max time).
+
+Other modes: --mode tune (the autotuner's table), --mode kernel (a short
+96-shot batched forward, the small case for ncu), --mode learned (FWI
+wall-clock to equal model error, learned preconditioner vs plain, on seeded
+gradient + anomaly models of 240 x 80 with held-out test models), --mode
+network (the preconditioner's kernels alone).
 """
 from __future__ import annotations
 
