@@ -316,6 +316,9 @@ int swfwi_fwi_last_line_search(const swfwi_fwi *h, float *alpha, float *obj);
  * launches and, when enabled, CUDA-event timing of every stencil launch on
  * its own stream with its algorithmic work (interior point-updates; bytes =
  * 12 per point-update plus 4 per point per velocity model read).
+ * kernel_launches counts launches issued from the host: a time loop replayed
+ * as a CUDA graph (swfwi_damp4t10d_set_graphs) is counted when captured, not
+ * again per replay; stencil timing turns the replay off.
  * ---------------------------------------------------------------------- */
 typedef struct {
   long long kernel_launches;
