@@ -4,7 +4,7 @@
 //
 // The network has no counterpart in the reference; it sits beside the
 // plain FWI epoch (src/fwi/fwiframework.cpp:269-356), which stays both the
-// fallback and the judge of every proposed step.
+// fallback and the arbiter of every proposed step.
 //
 // Architecture (4 levels, widths c0..c3, default 16/32/64/64):
 //   x (3 channels, zero-padded to 16)

@@ -14,7 +14,7 @@ Attached to a plain ``FwiFramework`` (``setPreconditioner``), each epoch
 first searches along the network's direction with the plain step-length
 search and keeps that step only when the search confirms an objective
 decrease; otherwise it takes the plain CG step.  Plain FWI thus stays both
-the fallback and the judge of every learned step.
+the fallback and the arbiter of every learned step.
 
 The network has no counterpart in the reference (src/fwi/fwiframework.cpp
 is the plain method it sits beside).
