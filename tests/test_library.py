@@ -100,3 +100,31 @@ def test_bad_arguments_are_rejected_without_gpu():
     # null device pointers are refused before any launch
     assert lib.swfwi_fd4t10s_damp_zjh_2d_vtrans(None, None, None, None, 100, 100, 36, None) == 1
     assert b"null" in lib.swfwi_last_error()
+
+
+def test_header_is_c99_and_links(tmp_path):
+    # the boundary is a C ABI: the header compiles as strict C99 and a C
+    # program links against the library and calls a host entry point
+    import swfwi_b200
+    src = tmp_path / "abi.c"
+    src.write_text(
+        '#include "swfwi_gpu.h"\n'
+        "#include <stdio.h>\n"
+        "int main(void) {\n"
+        "  float w[16];\n"
+        "  int s = swfwi_ricker_wavelet(w, 16, 10.0f, 0.002f, 1.0f);\n"
+        "  if (s != SWFWI_OK) return 1;\n"
+        "  s = swfwi_ricker_wavelet(w, 0, 10.0f, 0.002f, 1.0f);\n"
+        '  printf("%d %s\\n", s, swfwi_status_string(s));\n'
+        "  return s == SWFWI_ERR_BAD_ARG ? 0 : 2;\n"
+        "}\n")
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(swfwi_b200.LIB_PATH)
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                         "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                         "-L", libdir, "-lswfwi_b200", "-Wl,-rpath," + libdir],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert run.returncode == 0, (run.stdout, run.stderr)
+    assert "bad argument" in run.stdout
