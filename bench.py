@@ -53,6 +53,23 @@ CONFIG = "batched"
 CPU_SAMPLE_NT = 1500
 
 
+def max_over_ranks(x: float, dist=None, device="cuda") -> float:
+    """The largest value of a per-rank scalar over all ranks (a job's time
+    is its slowest rank's); dist None: one rank."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(updates_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job Gpts/s of N replicas: every rank's point-updates over the
+    slowest rank's time."""
+    return updates_per_rank * world / seconds_max / 1e9
+
+
 def env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -484,13 +501,9 @@ def main():
     ms = ev0.elapsed_time(ev1)
     st = S.stats_read()
     S.stats_enable_step_timing(False)
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist)
     updates_rank = st["step_point_updates"]
-    value = updates_rank * world / (ms_max * 1e-3) / 1e9
+    value = replica_value(updates_rank, world, ms_max * 1e-3)
 
     # dominant kernel: the stencil step, timed per launch with CUDA events
     peak, peak_kind = measured_peaks()
@@ -500,7 +513,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                 "frac": step_gbs / peak, "peak_basis": peak_kind,
                 "traffic": (tpp * per_launch_pts) if tpp else None,
-                "kernel": {0: "fd_step_stream", 1: "fd_step_ws", 2: "fd_step_wi"}.get(tuning.get("kernel", 1)),
+                "kernel": {0: "fd_step_stream", 1: "fd_step_ws", 2: "fd_step_wi", 3: "fd_step_ws2",
+                           4: "fd_step_ws (global prev)"}.get(tuning.get("kernel", 1)),
                 "launches": st["step_launches"],
                 "avg_launch_us": st["step_ms"] * 1e3 / max(st["step_launches"], 1),
                 "bytes_per_launch": st["step_bytes"] / max(st["step_launches"], 1),
@@ -525,12 +539,9 @@ def main():
         dt = time.perf_counter() - t0
         st2 = S.stats_read()
         S.stats_enable_step_timing(False)
-        if dist is not None:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = max_over_ranks(dt, dist)
         h2d = exi_p.numel() * 4 + wlt_p.numel() * 4 + dobs_h.numel() * 4
-        e2e = {"value": st2["step_point_updates"] * world / dt / 1e9, "unit": "Gpts/s",
+        e2e = {"value": replica_value(st2["step_point_updates"], world, dt), "unit": "Gpts/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(grad_p.numel() * 4 + 8 * ns),
                "ms_per_step": dt / args.e2e_steps * 1e3}
         m.bindVelocity(exi)
