@@ -307,6 +307,12 @@ int swfwi_fwi_set_regularization(swfwi_fwi *h, float lx, float lz);
 int swfwi_regu_term(const float *vel, int nx, int nz, float lx, float lz, double *term, void *stream);
 int swfwi_regu_gradient(const float *vel, int nx, int nz, float lx, float lz, float *grad, int accumulate,
                         void *stream);
+/* Failure-detection self-test: one thread waits, with the stencil kernels'
+ * bounded mbarrier wait (about 2^31 cycles, a second), on a barrier nothing
+ * arrives at; the wait gives up, raises the error flag, and the call returns
+ * SWFWI_ERR_TIMEOUT as a stalled stencil launch would.  The context stays
+ * usable.  Returns SWFWI_OK only if the wait did not give up (a fault). */
+int swfwi_selftest_bounded_wait(void *stream);
 /* last epoch's step length and trial record: alpha[4], obj[4] (host) */
 int swfwi_fwi_last_line_search(const swfwi_fwi *h, float *alpha, float *obj);
 

@@ -147,6 +147,7 @@ _SIGS = {
     "swfwi_fwi_get_gradient": [_vp, _fp],
     "swfwi_fwi_get_illumination": [_vp, _fp],
     "swfwi_fwi_learned_stats": [_vp, _ip, _ip, _ip],
+    "swfwi_selftest_bounded_wait": [_vp],
     "swfwi_stats_reset": [],
     "swfwi_stats_enable_step_timing": [C.c_int],
     "swfwi_stats_read": [C.POINTER(Stats)],
