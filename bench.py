@@ -37,7 +37,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import tempfile
@@ -51,6 +50,7 @@ sys.path.insert(0, ROOT)
 METRIC = "FD Gpts/s (% HBM roofline); FWI wall-clock to equal model L2, learned vs plain"
 CONFIG = "batched"
 CPU_SAMPLE_NT = 1500
+CPU_SAMPLE_NT_ASBUILT = 600
 
 
 def max_over_ranks(x: float, dist=None, device="cuda") -> float:
@@ -86,15 +86,16 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic_per_point():
-    """DRAM bytes per stencil point-update from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "fd_step_batched_traffic.md")
-    try:
-        txt = open(path).read()
-    except OSError:
-        return None
-    m = re.search(r"dram_bytes_per_point_update:\s*([0-9.]+)", txt)
-    return float(m.group(1)) if m else None
+# DRAM bytes per point-update of each stencil kernel on the 96-shot
+# workload's launch (993 x 343 padded, 31,172,256 point-updates), from one
+# ncu capture: (dram__bytes_read.sum + dram__bytes_write.sum) / point-updates.
+# Kernel 1: 288.79 MB + 88.67 MB (profiles/fd_step_ws_96shots_993x343_fast.md);
+# kernel 5: 293.74 MB + 88.59 MB (profiles/fd_step_rq_96shots_993x343_fast.md).
+STENCIL_TRAFFIC_B_PER_PT = {1: 12.11, 5: 12.27}
+
+
+def traffic_per_point(kernel):
+    return STENCIL_TRAFFIC_B_PER_PT.get(kernel)
 
 
 def backward_steps(nt: int, dt: float) -> int:
@@ -183,9 +184,12 @@ def setup_workload(torch, arith, nt=0):
     return s, m, exi, exi_h, wlt, wlt_h, dobs, ids
 
 
-def cpu_reference_sample(nt_sample=CPU_SAMPLE_NT, repeats=1):
+def cpu_reference_sample(nt_sample=CPU_SAMPLE_NT, repeats=1, asbuilt=False):
     """The reference's gradient loop on one shot of the workload with the
-    time axis cut to nt_sample steps, OpenMP over all host cores."""
+    time axis cut to nt_sample steps, OpenMP over all host cores (asbuilt:
+    the reference as its own build compiles it, pass 1 of the damped step
+    serial).  Also returns what the GPU needs to recompute the same sample
+    and the reference's gradient and objective to check it against."""
     import oracle
     from swfwi_b200 import survey as sv
     if not oracle.available():
@@ -194,7 +198,7 @@ def cpu_reference_sample(nt_sample=CPU_SAMPLE_NT, repeats=1):
     off, gx, _ = s.spreads
     n0 = int(off[1] - off[0])
     ss = s.scaled(nt=nt_sample, ns=1, ng=n0, gxbeg=int(gx[0]), spreads=None)
-    R = oracle.RefLib()
+    R = oracle.RefLib(asbuilt=asbuilt)
     M = R.model(ss)
     vtrue = sv.layered_model(s.nx, s.nz, seed=2024)
     vinit = sv.smooth(vtrue, 15.0).astype(np.float32)
@@ -205,15 +209,38 @@ def cpu_reference_sample(nt_sample=CPU_SAMPLE_NT, repeats=1):
     pts = (M.nxpad - 12) * (M.nzpad - 12)
     updates = pts * (2 * ss.nt + 2 * backward_steps(ss.nt, ss.dt))
     times = []
+    grad = obj = None
     for _ in range(repeats):
         t0 = time.perf_counter()
-        M.fwi_gradient(wlt, dobs)
+        grad, obj = M.fwi_gradient(wlt, dobs)
         times.append(time.perf_counter() - t0)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"seconds": min(times), "updates": updates, "cores": cores,
+    return {"seconds": min(times), "updates": updates, "cores": _cores(),
             "sample": f"one shot ({n0} receivers), nt={ss.nt}, full {M.nxpad}x{M.nzpad} padded grid, "
                       f"reference gradient loop (FwiForwardModeling, mute, residual, transVsrc, "
-                      f"calgradient, scale/mask)"}
+                      f"calgradient, scale/mask)" + (", as built (pass 1 serial)" if asbuilt else ""),
+            "survey": ss, "vinit": vinit, "wlt": wlt, "dobs": dobs, "grad": grad, "obj": obj}
+
+
+def parity_of_sample(torch, arith, tuning, info):
+    """The product's gradient of the CPU-baseline sample (the same shot,
+    velocity, wavelet and observed data) against the reference's gradient
+    of it: relative L2 and objective difference."""
+    import swfwi_b200 as S
+    ss = info["survey"]
+    m = S.Damp4t10d.from_survey(ss, arith=arith)
+    m.set_tuning(**tuning)
+    vel = torch.from_numpy(m.expandDomain(info["vinit"])).cuda()
+    m.bindVelocity(vel)
+    gr = torch.zeros(vel.shape, device="cuda")
+    obj = m.gradient_batch(torch.from_numpy(np.ascontiguousarray(info["wlt"])).cuda(),
+                           torch.from_numpy(np.ascontiguousarray(info["dobs"])).cuda(), [0], gr)
+    g = gr.cpu().numpy().astype(np.float64)
+    want = np.asarray(info["grad"], np.float64)
+    e = float(np.linalg.norm(g - want) / np.linalg.norm(want))
+    eo = float(abs(float(obj.sum()) - info["obj"]) / abs(info["obj"]))
+    return {"case": "the CPU baseline's sample: " + info["sample"], "grad_rel_l2": e, "objective_rel": eo,
+            "tolerance": {"grad_rel_l2": 1e-4, "objective_rel": 1e-4},
+            "ok": bool(e < 1e-4 and eo < 1e-4)}
 
 
 def run_reference(args):
@@ -281,6 +308,205 @@ def run_kernel_mode(args):
     print(json.dumps({"mode": "kernel", "shots": ss.ns, "nt": ss.nt,
                       "checksum": float(dcal.abs().sum().item())}))
     return 0
+
+
+# ---------------------------------------------------------------- the other workload configurations
+def _timed(torch, fn):
+    """Wall seconds of fn() between two device synchronisations."""
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = fn()
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, r
+
+
+def _cpu_timed(fn):
+    t0 = time.perf_counter()
+    r = fn()
+    return time.perf_counter() - t0, r
+
+
+def record_fwi_iteration(torch, arith, tuning, cpu):
+    """Plain FWI, one iteration: 20 shots of 151 x 461 (193 x 533 padded),
+    nt 2000, dt 2 ms, 10 Hz: the batched gradient of all shots, the
+    step-length search with its trial forwards, the velocity update
+    (FwiFramework::epoch, fwiframework.cpp:269-356).  GPU seconds are the
+    second epoch's (the first allocates).  The reference CPU seconds are
+    extrapolated from its own per-shot units timed at full nt on the host
+    cores: 20 x (one shot's gradient loop + trials x one shot's forward),
+    trials = the trial objectives this run's search evaluated."""
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    s = sv.config("fwi")
+    vt = sv.layered_model(s.nx, s.nz, seed=2024)
+    vi = sv.smooth(vt, 15.0).astype(np.float32)
+    m = S.Damp4t10d.from_survey(s, arith=arith)
+    m.set_tuning(**tuning)
+    ext, exi = m.expandDomain(vt), m.expandDomain(vi)
+    wlt = S.ricker_wavelet(s.nt, s.fm, s.dt)
+    vel = torch.from_numpy(ext).cuda()
+    m.bindVelocity(vel)
+    dobs = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
+    m.forward_batch(torch.from_numpy(wlt).cuda(), dobs, np.arange(s.ns, dtype=np.int32))
+    f = S.FwiFramework(m, exi, s.vmin, s.vmax, s.nita, s.maxdv, wlt, dobs.cpu().numpy())
+    t_first, _ = _timed(torch, lambda: f.epoch(0))
+    t_iter, _ = _timed(torch, lambda: f.epoch(1))
+    trials = f.lastTrials()
+    rec = {"workload": "plain FWI iteration: 20 shots, 151x461 (193x533 padded), nt 2000, dt 2 ms, 10 Hz, "
+                       "gradient + step-length search + velocity update",
+           "gpu_s": t_iter, "gpu_first_epoch_s": t_first, "trials": trials,
+           "objective": f.getInitObj(), "objective_after": f.getUpdateObj()}
+    if cpu:
+        import oracle
+        if oracle.available():
+            R = oracle.RefLib()
+            ss = s.scaled(ns=1, sxbeg=int(s.src_x()[s.ns // 2]))
+            M = R.model(ss)
+            M.expand_domain(vt)
+            d1 = M.fwi_forward(wlt, 0)
+            M.expand_domain(vi)
+            tg, _ = _cpu_timed(lambda: M.fwi_gradient(wlt, d1[None]))
+            tf, _ = _cpu_timed(lambda: M.fwi_forward(wlt, 0))
+            cpu_s = s.ns * (tg + trials * tf)
+            rec["cpu"] = {"s": cpu_s, "kind": "reference", "cores": _cores(),
+                          "basis": f"extrapolated: 20 x (one shot's gradient loop {tg:.2f} s + {trials} x one "
+                                   f"shot's forward {tf:.2f} s), each timed once at full nt"}
+            rec["speedup_vs_cpu"] = cpu_s / t_iter
+    return rec
+
+
+def record_encoded(torch, arith, tuning, iters):
+    """Encoded-source FWI: the 96 shots of 301 x 921 (nt 4000, dt 1 ms,
+    15 Hz, common receiver line) as one supershot with +-1 codes re-drawn
+    every iteration (EssFwiFramework::epoch, essfwiframework.cpp:191-239).
+    `iters` iterations are timed (the 50-iteration run is their mean x 50).
+    The gradient's error against the FP64 GPU run of the same scheme is
+    stated for FP32, FP16 and BF16 boundary strips, on one supershot."""
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    s = sv.config("encoded")
+    vt = sv.layered_model(s.nx, s.nz, seed=2024)
+    vi = sv.smooth(vt, 15.0).astype(np.float32)
+    m = S.Damp4t10d.from_survey(s, arith=arith)
+    m.set_tuning(**tuning)
+    ext, exi = m.expandDomain(vt), m.expandDomain(vi)
+    wlt_h = S.ricker_wavelet(s.nt, s.fm, s.dt)
+    wlt = torch.from_numpy(wlt_h).cuda()
+    vel = torch.from_numpy(ext).cuda()
+    m.bindVelocity(vel)
+    dobs = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
+    m.forward_batch(wlt, dobs, np.arange(s.ns, dtype=np.int32))
+    velinit = torch.from_numpy(exi).cuda()
+    m.bindVelocity(velinit)
+    # the gradient of one supershot against FP64
+    codes = torch.from_numpy(S.random_codes(1, s.ns)).cuda()
+    encsrc = torch.empty((s.nt, s.ns), device="cuda")
+    S.encode_source(encsrc, wlt, codes)
+    encobs = torch.empty((s.nt, s.ng), device="cuda")
+    S.encode_obs(encobs, dobs, codes)
+    dcal = torch.zeros((s.nt, s.ng), device="cuda")
+    m.EssForwardModeling(encsrc, dcal)
+    vsrc = torch.empty_like(dcal)
+    S.trans_vsrc(vsrc, (encobs - dcal).contiguous())
+    g64 = torch.zeros(exi.shape, dtype=torch.float64, device="cuda")
+    t64, _ = _timed(torch, lambda: m.calgradient_ess_f64(velinit, encsrc.double(), vsrc.double(), g64))
+    errs = {}
+    for name, fmt in (("f32", S.STRIP_F32), ("f16", S.STRIP_F16), ("bf16", S.STRIP_BF16)):
+        m.set_strip_format(fmt)
+        g = torch.zeros(exi.shape, device="cuda")
+        m.calgradient_ess(encsrc, vsrc, g)
+        errs[name] = float(((g.double() - g64).norm() / g64.norm()).item())
+    m.set_strip_format(S.STRIP_F32)
+    dobs_h = dobs.cpu().numpy()
+    del dobs, encobs
+    f = S.EssFwiFramework(m, exi, s.vmin, s.vmax, s.nita, s.maxdv, wlt_h, dobs_h)
+    t_first, _ = _timed(torch, lambda: f.epoch(0))
+    ts = []
+    for it in range(1, iters + 1):
+        t, _ = _timed(torch, lambda: f.epoch(it))
+        ts.append(t)
+    per = sum(ts) / len(ts)
+    return {"workload": "encoded-source FWI: 96 shots of 301x921 (993x343 padded) as one supershot, nt 4000, "
+                        "dt 1 ms, 15 Hz, codes re-drawn each iteration",
+            "iterations_timed": len(ts), "s_per_iteration": per, "fifty_iterations_s": 50 * per,
+            "gpu_first_epoch_s": t_first, "trials_last": f.lastTrials(),
+            "gradient_rel_l2_vs_f64": errs, "f64_gradient_s": t64,
+            "strips": "FP32 during the timed iterations; FP16/BF16 scaled strips in the error figures"}
+
+
+def record_enkf(torch, arith, tuning, cpu, members=64):
+    """Ensemble Kalman FWI analysis: 201 x 461 (243 x 533 padded), 20 m,
+    nt 3000, dt 2 ms, 16 shots encoded into one supershot per member
+    (EnkfAnalyze::calGainMatrix's HA loop, enkfanalyze.cpp:207-236) for 64
+    members = initial model + Gaussian random fields (200 m, 100 m/s);
+    observed data with Gaussian noise at 1 % of each trace's RMS.  Timed:
+    the batched member forward (HA), the FP64 gain (cross products,
+    factorisation, products) and the member update."""
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    from swfwi_b200.enfwi import vel_recover, vel_trans
+    s = sv.config("enkf")
+    vt = sv.layered_model(s.nx, s.nz, seed=2024)
+    vi = sv.smooth(vt, 15.0).astype(np.float32)
+    m = S.Damp4t10d.from_survey(s, arith=arith)
+    m.set_tuning(**tuning)
+    ext, exi = m.expandDomain(vt), m.expandDomain(vi)
+    wlt_h = S.ricker_wavelet(s.nt, s.fm, s.dt)
+    wlt = torch.from_numpy(wlt_h).cuda()
+    vel = torch.from_numpy(ext).cuda()
+    m.bindVelocity(vel)
+    dobs = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
+    m.forward_batch(wlt, dobs, np.arange(s.ns, dtype=np.int32))
+    g = torch.Generator(device="cuda").manual_seed(7)
+    rms = dobs.pow(2).mean(dim=1, keepdim=True).sqrt()
+    dobs += 0.01 * rms * torch.randn(dobs.shape, device="cuda", generator=g)
+    v0 = vel_recover(exi, s.dx, s.dt)
+    nxpad, nzpad = exi.shape
+    vels = np.stack([vel_trans(v0 + sv.gaussian_random_field(nxpad, nzpad, s.dx, 200.0, 100.0, seed=100 + i),
+                               s.dx, s.dt) for i in range(members)])
+    vels = torch.from_numpy(vels).cuda()
+    ea = S.EnkfAnalyze(m, wlt, dobs, sigfac=0.5)
+    codes = torch.from_numpy(S.random_codes(2, s.ns)).cuda()
+    encsrc = torch.empty((s.nt, s.ns), device="cuda")
+    S.encode_source(encsrc, wlt, codes)
+    encobs = torch.empty((s.nt, s.ng), device="cuda")
+    S.encode_obs(encobs, dobs, codes)
+    d = encobs.t().contiguous().reshape(-1)
+    hona = torch.empty((members, s.ng * s.nt), device="cuda")
+    m.ess_forward_members(encsrc, vels, hona)            # warm-up
+    t_ha, _ = _timed(torch, lambda: m.ess_forward_members(encsrc, vels, hona))
+    t_gain, (t4, sigma, clip) = _timed(torch, lambda: S.enkf_gain_matrix(hona, d, None, 0.5, 0.0, 1))
+    t_upd, _ = _timed(torch, lambda: S.enkf_update(vels.reshape(members, -1), t4, s.dx, s.dt))
+    rows = s.ng * s.nt
+    pts = (nxpad - 12) * (nzpad - 12) * s.nt * members
+    rec = {"workload": f"EnKF analysis: {members} members x one 16-shot supershot of 201x461 (243x533 padded), "
+                       "nt 3000, dt 2 ms; FP32 member modelling, FP64 analysis",
+           "members": members, "ha_s": t_ha, "ha_gpts": pts / t_ha / 1e9,
+           "gain_s": t_gain, "update_s": t_upd, "clip": int(clip),
+           "cross_products_gflop": 6.0 * members * members * rows / 1e9,
+           "gain_fp64_gflops": 6.0 * members * members * rows / t_gain / 1e9}
+    if cpu:
+        import oracle
+        if oracle.available():
+            R = oracle.RefLib()
+            ntc = 600
+            ss = s.scaled(nt=ntc)
+            M = R.model(ss)
+            M.bind_velocity(exi)
+            enc = np.ascontiguousarray(np.outer(S.ricker_wavelet(ntc, s.fm, s.dt),
+                                                S.random_codes(2, s.ns)).astype(np.float32))
+            tf, _ = _cpu_timed(lambda: M.ess_forward(enc))
+            cpu_ha = tf * (s.nt / ntc) * members
+            rec["cpu"] = {"ha_s": cpu_ha, "kind": "reference", "cores": _cores(),
+                          "basis": f"extrapolated: {members} members x the reference's EssForwardModeling of "
+                                   f"one member timed at nt {ntc} ({tf:.2f} s) x {s.nt}/{ntc}; the "
+                                   "reference's analysis needs MPI and LAPACK and is not timed"}
+            rec["ha_speedup_vs_cpu"] = cpu_ha / t_ha
+    return rec
+
+
+def _cores():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
 
 def network_flops(layers, N, H, W):
@@ -413,6 +639,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the records of the other workloads (plain FWI iteration, encoded-source "
+                         "FWI, EnKF analysis)")
+    ap.add_argument("--ess-iters", type=int, default=3, help="timed encoded-source FWI iterations")
     ap.add_argument("--mode", default="bench", choices=["bench", "kernel", "tune", "learned", "network"],
                     help="kernel: short 96-shot batched forward (the small case for ncu); "
                          "tune: print the autotuner's table; learned: FWI wall-clock to equal model "
@@ -509,12 +739,12 @@ def main():
     peak, peak_kind = measured_peaks()
     step_gbs = st["step_bytes"] / (st["step_ms"] * 1e-3) / 1e9 if st["step_ms"] > 0 else 0.0
     per_launch_pts = st["step_point_updates"] / max(st["step_launches"], 1)
-    tpp = profile_traffic_per_point()
+    tpp = traffic_per_point(tuning.get("kernel", 1))
     roofline = {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                 "frac": step_gbs / peak, "peak_basis": peak_kind,
                 "traffic": (tpp * per_launch_pts) if tpp else None,
                 "kernel": {0: "fd_step_stream", 1: "fd_step_ws", 2: "fd_step_wi", 3: "fd_step_ws2",
-                           4: "fd_step_ws (global prev)"}.get(tuning.get("kernel", 1)),
+                           4: "fd_step_ws (global prev)", 5: "fd_step_rq"}.get(tuning.get("kernel", 1)),
                 "launches": st["step_launches"],
                 "avg_launch_us": st["step_ms"] * 1e3 / max(st["step_launches"], 1),
                 "bytes_per_launch": st["step_bytes"] / max(st["step_launches"], 1),
@@ -546,7 +776,7 @@ def main():
                "ms_per_step": dt / args.e2e_steps * 1e3}
         m.bindVelocity(exi)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             info = cpu_reference_sample()
@@ -554,9 +784,26 @@ def main():
                 cpu = {"value": info["updates"] / info["seconds"] / 1e9, "unit": "Gpts/s",
                        "cores": info["cores"], "kind": "reference", "sample": info["sample"],
                        "seconds": info["seconds"]}
+                parity = parity_of_sample(torch, arith, tuning, info)
+                ab = cpu_reference_sample(nt_sample=CPU_SAMPLE_NT_ASBUILT, asbuilt=True)
+                cpu["as_built"] = {"value": ab["updates"] / ab["seconds"] / 1e9, "unit": "Gpts/s",
+                                   "cores": ab["cores"], "sample": ab["sample"], "seconds": ab["seconds"]}
         except Exception as e:   # the baseline is reported, never required
             cpu = {"value": None, "unit": "Gpts/s", "cores": 0, "kind": "reference",
                    "sample": f"failed: {e}"}
+
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = {}
+        for key, fn in (("fwi_iteration_151x461", lambda: record_fwi_iteration(torch, arith, tuning,
+                                                                                not args.no_cpu_baseline)),
+                        ("encoded_fwi_301x921", lambda: record_encoded(torch, arith, tuning, args.ess_iters)),
+                        ("enkf_201x461", lambda: record_enkf(torch, arith, tuning, not args.no_cpu_baseline))):
+            try:
+                configs[key] = fn()
+            except Exception as e:   # reported, never required
+                configs[key] = {"failed": f"{type(e).__name__}: {e}"}
+            torch.cuda.synchronize()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
@@ -571,8 +818,8 @@ def main():
                            "l2": "inputs larger than L2 (strips 14 GB, fields 0.5 GB): no flush",
                            "parallelism": f"replicas{world}",
                            "objective_last_step": float(np.sum(objs)) if objs is not None else None},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(st["kernel_launches"]), "clocks": clocks}
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,
+                "gpu_launches": int(st["kernel_launches"]), "clocks": clocks, "configs": configs}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

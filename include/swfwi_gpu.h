@@ -226,6 +226,12 @@ int swfwi_damp4t10d_calgradient_fwi(swfwi_damp4t10d *h, const float *wlt, const 
  * double (device); grad accumulates. */
 int swfwi_damp4t10d_calgradient_fwi_f64(swfwi_damp4t10d *h, const float *vel, const double *wlt,
                                         const double *vsrc, double *grad, int shot_id);
+/* FP64 run of the encoded-source gradient scheme (essfwiframework.cpp:
+ * 114-173; double fields, exact strips): vel float transformed velocity,
+ * encsrc [nt][ns], vsrc [nt][ng] and grad double (device); grad
+ * accumulates. */
+int swfwi_damp4t10d_calgradient_ess_f64(swfwi_damp4t10d *h, const float *vel, const double *encsrc,
+                                        const double *vsrc, double *grad);
 /* FP64 forward modelling of one shot (double dcal, device). */
 int swfwi_damp4t10d_fwi_forward_modeling_f64(swfwi_damp4t10d *h, const float *vel,
                                              const double *wlt, double *dcal, int shot_id);
@@ -315,6 +321,10 @@ int swfwi_regu_gradient(const float *vel, int nx, int nz, float lx, float lz, fl
 int swfwi_selftest_bounded_wait(void *stream);
 /* last epoch's step length and trial record: alpha[4], obj[4] (host) */
 int swfwi_fwi_last_line_search(const swfwi_fwi *h, float *alpha, float *obj);
+/* Trial objectives the last epoch's step-length search evaluated (each a
+ * forward sweep over all shots, or over the supershot; refineAlpha and
+ * calsteplen of updatesteplenop.cpp:88-265). */
+int swfwi_fwi_last_trials(const swfwi_fwi *h, int *trials);
 
 /* ------------------------------------------------------------------------
  * Measurement (no counterpart in the reference, which prints wall-clock
@@ -364,9 +374,10 @@ int swfwi_encode_obs(float *encobs, const float *dobs, const int *codes, long lo
  * t4 (host, out): the n x n gain HA'^T U SSqInv U^T (D - HA), column-major
  *   (t4[col*n + row]) like the reference's Matrix;
  * clip (host, out, optional): clipPosition of the singular values.
- * The SVD is taken through the n x n cross product band^T band (cyclic
- * Jacobi in double on the host); the three n x n products over the rows are
- * one fused FP64 pass on the device.  Synchronises the stream. */
+ * Everything runs on the device: the three n x n products over the rows in
+ * one fused FP64 pass, then the SVD through the n x n cross product
+ * band^T band (parallel-ordered Jacobi in FP64 in one CTA), clipPosition
+ * and the n x n products.  Synchronises the stream. */
 int swfwi_enkf_gain_matrix(const float *hona, const float *dobs, const double *z, long long rows,
                            int n, float sigfac, double *sigma, unsigned long long seed, double *t4,
                            int *clip, void *stream);
@@ -376,6 +387,16 @@ int swfwi_enkf_gain_matrix(const float *hona, const float *dobs, const double *z
  * (A' t4)_i).  t4 host, column-major as returned above.  Synchronises. */
 int swfwi_enkf_update(float *vels, long long model_size, int n, const double *t4, float dx, float dt,
                       void *stream);
+/* The analysis in one call (EnkfAnalyze::analyze after calGainMatrix,
+ * enkfanalyze.cpp:57-111 and 185-341): the gain of swfwi_enkf_gain_matrix
+ * stays in device memory and moves the members vels [n][model_size]
+ * (DEVICE) in place as swfwi_enkf_update does; nothing returns to the host
+ * between the two.  sigma as above; t4_out (HOST, optional) receives the
+ * gain, column-major; clip (host, optional).  A non-finite gain returns
+ * SWFWI_ERR_NONFINITE and leaves the members unchanged.  Synchronises. */
+int swfwi_enkf_analyze(const float *hona, const float *dobs, const double *z, long long rows, int n,
+                       float sigfac, double *sigma, unsigned long long seed, float *vels,
+                       long long model_size, float dx, float dt, double *t4_out, int *clip, void *stream);
 /* createAMean (enkfanalyze.cpp:568-580): mean [model_size] DEVICE = the
  * members' float sum in member order / n. */
 int swfwi_enkf_mean(float *mean, const float *vels, long long model_size, int n, void *stream);

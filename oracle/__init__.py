@@ -28,6 +28,18 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 
+def reference_tree() -> str | None:
+    """The reference checkout the oracle recipe compiles (``oracle/Makefile``
+    decides: REF, else $SWFWI_REFERENCE, else its default); None when that
+    tree is absent, as on a machine that only runs the prebuilt oracle."""
+    try:
+        out = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], check=True, capture_output=True,
+                             text=True).stdout.strip()
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    return out if out and os.path.isdir(os.path.join(out, "src")) else None
+
+
 def build(reference: str | None = None) -> None:
     """Compile the oracle libraries (needs the reference tree; run where it exists)."""
     cmd = ["make", "-C", HERE, "-j8"]

@@ -86,6 +86,7 @@ _SIGS = {
     "swfwi_damp4t10d_calgradient_ess": [_vp, _vp, _vp, _vp],
     "swfwi_damp4t10d_calgradient_fwi": [_vp, _vp, _vp, _vp, C.c_int],
     "swfwi_damp4t10d_calgradient_fwi_f64": [_vp, _vp, _vp, _vp, _vp, C.c_int],
+    "swfwi_damp4t10d_calgradient_ess_f64": [_vp, _vp, _vp, _vp, _vp],
     "swfwi_damp4t10d_fwi_forward_modeling_f64": [_vp, _vp, _vp, _vp, C.c_int],
     "swfwi_update_grad": [_vp, _vp, _vp, C.c_int, C.c_int, _vp],
     "swfwi_cal_max_alpha": [_vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float, _fp, _fp, _vp],
@@ -110,6 +111,8 @@ _SIGS = {
     "swfwi_enkf_gain_matrix": [_vp, _vp, _vp, C.c_longlong, C.c_int, C.c_float, _dp, C.c_ulonglong, _dp,
                                _ip, _vp],
     "swfwi_enkf_update": [_vp, C.c_longlong, C.c_int, _dp, C.c_float, C.c_float, _vp],
+    "swfwi_enkf_analyze": [_vp, _vp, _vp, C.c_longlong, C.c_int, C.c_float, _dp, C.c_ulonglong, _vp,
+                           C.c_longlong, C.c_float, C.c_float, _dp, _ip, _vp],
     "swfwi_enkf_mean": [_vp, _vp, C.c_longlong, C.c_int, _vp],
     "swfwi_parabola_vertex": [C.c_float] * 7 + [_fp, _fp],
     "swfwi_ricker_wavelet": [_fp, C.c_int, C.c_float, C.c_float, C.c_float],
@@ -123,6 +126,7 @@ _SIGS = {
     "swfwi_fwi_get_velocity": [_vp, _fp],
     "swfwi_fwi_write_vel": [_vp, _fp],
     "swfwi_fwi_last_line_search": [_vp, _fp, _fp],
+    "swfwi_fwi_last_trials": [_vp, _ip],
     "swfwi_precond_create": [C.POINTER(_vp), _ip],
     "swfwi_precond_destroy": [_vp],
     "swfwi_precond_num_params": [_vp, C.POINTER(C.c_longlong)],
@@ -336,6 +340,21 @@ def enkf_update(vels, t4, dx: float, dt: float, stream=None) -> None:
                                    _stream(stream)))
 
 
+def enkf_analyze(hona, dobs, vels, dx: float, dt: float, z=None, sigfac: float = 0.0, sigma: float = 0.0,
+                 seed: int = 1, stream=None):
+    """Gain and member update in one device-side call: vels [n][...] float32
+    CUDA moved in place.  Returns (t4 numpy [n][n] indexed [row, col],
+    sigma, clip)."""
+    n, rows = hona.shape
+    t4 = np.zeros((n, n), np.float64)
+    sg = C.c_double(sigma)
+    clip = C.c_int(0)
+    _check(lib().swfwi_enkf_analyze(_ptr(hona), _ptr(dobs), _ptr(z) if z is not None else None, rows, n, sigfac,
+                                    C.byref(sg), seed, _ptr(vels), vels.numel() // n, dx, dt,
+                                    t4.ctypes.data_as(_dp), C.byref(clip), _stream(stream)))
+    return t4.T.copy(), sg.value, clip.value
+
+
 def enkf_mean(mean, vels, stream=None) -> None:
     n = vels.shape[0]
     _check(lib().swfwi_enkf_mean(_ptr(mean), _ptr(vels), vels.numel() // n, n, _stream(stream)))
@@ -356,6 +375,12 @@ class EnkfAnalyze:
     def calGainMatrix(self, vels, codes, z=None):
         """vels [N][nxpad][nzpad] CUDA members; codes [ns] +-1 ints.  Returns
         (t4 [N][N] numpy, clip)."""
+        hona, d = self._encoded(vels, codes)
+        t4, self.sigma, clip = enkf_gain_matrix(hona, d, z, self.sigfac, self.sigma, self.seed)
+        self.seed += 1
+        return t4, clip
+
+    def _encoded(self, vels, codes):
         import torch
         nxpad, nzpad, ns, ng, nt = self.fm.dims()
         c = torch.as_tensor(np.asarray(codes, np.int32), device=self.wlt.device)
@@ -364,17 +389,17 @@ class EnkfAnalyze:
         encobs = torch.empty((nt, ng), dtype=torch.float32, device=self.wlt.device)
         encode_obs(encobs, self.dobs, c)
         d = encobs.t().contiguous().reshape(-1)             # matrix_transpose: row ig*nt + it
-        n = vels.shape[0]
-        hona = torch.empty((n, ng * nt), dtype=torch.float32, device=self.wlt.device)
+        hona = torch.empty((vels.shape[0], ng * nt), dtype=torch.float32, device=self.wlt.device)
         self.fm.ess_forward_members(encsrc, vels, hona)
-        t4, self.sigma, clip = enkf_gain_matrix(hona, d, z, self.sigfac, self.sigma, self.seed)
-        self.seed += 1
-        return t4, clip
+        return hona, d
 
     def analyze(self, vels, codes, z=None):
-        """One analysis: gain, then every member moved in place."""
-        t4, clip = self.calGainMatrix(vels, codes, z)
-        enkf_update(vels.reshape(vels.shape[0], -1), t4, self.fm.dx, self.fm.dt)
+        """One analysis: gain, then every member moved in place, the gain
+        never leaving the device in between."""
+        hona, d = self._encoded(vels, codes)
+        t4, self.sigma, clip = enkf_analyze(hona, d, vels, self.fm.dx, self.fm.dt, z, self.sigfac, self.sigma,
+                                            self.seed)
+        self.seed += 1
         return t4, clip
 
     def createAMean(self, vels):
@@ -402,7 +427,14 @@ def regu_gradient(vel, lx: float, lz: float, grad, accumulate: bool = False, str
 def cal_objective_static(r, out, stream=None) -> None:
     """Sums of squares of each row of r ([nslots][n] float32, CUDA) into out
     ([nslots] float64, CUDA) without allocating device memory."""
+    import torch
+    if not (isinstance(r, torch.Tensor) and r.is_cuda and r.dtype == torch.float32 and r.dim() == 2
+            and r.is_contiguous()):
+        raise SwfwiError(1, "r must be a contiguous 2-D float32 CUDA tensor")
     nslots, n = r.shape
+    if not (isinstance(out, torch.Tensor) and out.is_cuda and out.dtype == torch.float64
+            and out.is_contiguous() and out.numel() >= nslots):
+        raise SwfwiError(1, "out must be a contiguous float64 CUDA tensor of at least nslots elements")
     _check(lib().swfwi_cal_objective_static(_ptr(r), n, nslots, _ptr(out), _stream(stream)))
 
 
@@ -480,7 +512,7 @@ class Damp4t10d:
         STRIP_BF16 (scaled 16-bit)."""
         _check(lib().swfwi_damp4t10d_set_strip_format(self.h, fmt))
 
-    def set_tuning(self, kernel: int = 1, band_depth: int = 376, rows_per_cta: int = 64,
+    def set_tuning(self, kernel: int = 5, band_depth: int = 120, rows_per_cta: int = 48,
                    rows_in_flight: int = 3, shots_slowest: bool = False):
         """Launch shape of the stencil (results do not change)."""
         _check(lib().swfwi_damp4t10d_set_tuning(self.h, kernel, band_depth, rows_per_cta, rows_in_flight,
@@ -624,6 +656,10 @@ class Damp4t10d:
         _check(lib().swfwi_damp4t10d_calgradient_fwi_f64(self.h, _ptr(vel), _ptr(wlt64), _ptr(vsrc64),
                                                          _ptr(grad64), shot_id))
 
+    def calgradient_ess_f64(self, vel, encsrc64, vsrc64, grad64):
+        _check(lib().swfwi_damp4t10d_calgradient_ess_f64(self.h, _ptr(vel), _ptr(encsrc64), _ptr(vsrc64),
+                                                         _ptr(grad64)))
+
     def FwiForwardModeling_f64(self, vel, wlt64, dcal64, shot_id: int):
         _check(lib().swfwi_damp4t10d_fwi_forward_modeling_f64(self.h, _ptr(vel), _ptr(wlt64), _ptr(dcal64),
                                                               shot_id))
@@ -720,6 +756,12 @@ class _Framework:
         o = np.zeros(4, np.float32)
         _check(lib().swfwi_fwi_last_line_search(self.h, a.ctypes.data_as(_fp), o.ctypes.data_as(_fp)))
         return a, o
+
+    def lastTrials(self) -> int:
+        """Trial objectives (forward sweeps) of the last epoch's step search."""
+        n = C.c_int()
+        _check(lib().swfwi_fwi_last_trials(self.h, C.byref(n)))
+        return n.value
 
 
 class FwiFramework(_Framework):

@@ -1,11 +1,11 @@
 """Autotuner for the streaming stencil's launch shape.
 
 The streaming step (``stream.cuh``) has knobs that do not change its
-results: which kernel (streaming; warp-specialised with a copy warp, with
-two rows per step, or with the previous field read from global memory;
-independent consumer warps), output depths per CTA, rows per CTA, rows in
-flight ahead of the compute and the launch order (shots slowest or
-fastest).  ``tune`` times short batched forward runs of a survey for each
+results: which kernel (register-queue warps, each a self-contained TMA
+pipeline; warp-specialised with a copy warp, with two rows per step, or
+with the previous field read from global memory; independent consumer
+warps), output depths per CTA, rows per task, rows in flight ahead of the
+compute and the launch order (shots slowest or fastest).  ``tune`` times short batched forward runs of a survey for each
 candidate with the library's CUDA-event step timing and returns the fastest;
 ``apply`` sets it on a propagator.
 """
@@ -15,13 +15,17 @@ import itertools
 
 import numpy as np
 
-DEFAULT = {"kernel": 1, "band_depth": 376, "rows_per_cta": 64, "rows_in_flight": 3,
+DEFAULT = {"kernel": 5, "band_depth": 120, "rows_per_cta": 48, "rows_in_flight": 3,
            "shots_slowest": False}
 
 
 def candidates(nz: int):
-    """Both kernels' band depths crossed with chunk lengths, prefetch depths
-    and launch orders."""
+    """The register-queue kernel's task lengths and prefetch depths, the
+    warp-specialised kernel's band depths, chunk lengths and prefetch
+    depths."""
+    for rows, depth in itertools.product((24, 32, 48, 64), (3, 7)):
+        yield {"kernel": 5, "band_depth": 120, "rows_per_cta": rows, "rows_in_flight": depth,
+               "shots_slowest": False}
     for bz, rows, depth, order in itertools.product((120, 248, 376), (48, 64, 128), (3, 7), (False, True)):
         yield {"kernel": 1, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": order}

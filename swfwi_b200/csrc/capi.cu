@@ -205,8 +205,11 @@ int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on) {
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest) {
   return guarded([&] {
-    SWFWI_REQUIRE(kernel >= 0 && kernel <= 4, "kernel must be 0, 1, 2, 3 or 4");
-    if (kernel == 3 || kernel == 4) {
+    SWFWI_REQUIRE(kernel >= 0 && kernel <= 5, "kernel must be 0, 1, 2, 3, 4 or 5");
+    if (kernel == 5) {
+      SWFWI_REQUIRE(band_depth == 120, "band depth must be 120 (one warp a task)");
+      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
+    } else if (kernel == 3 || kernel == 4) {
       SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,
                     "band depth must be 120, 248 or 376");
       SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
@@ -478,6 +481,14 @@ int swfwi_damp4t10d_calgradient_fwi_f64(swfwi_damp4t10d *h, const float *vel, co
   });
 }
 
+int swfwi_damp4t10d_calgradient_ess_f64(swfwi_damp4t10d *h, const float *vel, const double *encsrc,
+                                        const double *vsrc, double *grad) {
+  return guarded([&] {
+    SWFWI_REQUIRE(P(h).nxpad > 0, "model size unknown");
+    P(h).calgradient_ess_f64(vel, encsrc, vsrc, grad);
+  });
+}
+
 int swfwi_damp4t10d_fwi_forward_modeling_f64(swfwi_damp4t10d *h, const float *vel,
                                              const double *wlt, double *dcal, int shot_id) {
   return guarded([&] {
@@ -648,6 +659,13 @@ int swfwi_stats_read(swfwi_stats *out) {
     out->step_ms = ms;
     out->step_point_updates = pts;
     out->step_bytes = b;
+  });
+}
+
+int swfwi_fwi_last_trials(const swfwi_fwi *h, int *trials) {
+  return guarded([&] {
+    SWFWI_REQUIRE(trials, "null output");
+    *trials = R(h).search.trials;
   });
 }
 

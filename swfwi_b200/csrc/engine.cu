@@ -289,7 +289,8 @@ void Propagator::set_dims(int nxpad_, int nzpad_) {
   fstride = round_up((long long)nxpad * pitch + 2 * kStreamCoff, 64);
   damp_x_.resize(nxpad);
   damp_z_.resize(nzpad);
-  launch_damp_tables(damp_x_.get(), damp_z_.get(), nxpad, nzpad, bx0, st_);
+  coef_x_.resize(nxpad);
+  launch_damp_tables(damp_x_.get(), damp_z_.get(), coef_x_.get(), nxpad, nzpad, bx0, st_);
   bsize = strip_size(nxpad, nzpad, bx0);
   rcp_for_ = nullptr;
   upload_geometry();
@@ -357,6 +358,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.curr = static_cast<const float *>(curr);
   a.rcp = static_cast<const float *>(velrcp);
   a.damp_x = damp_x_.get();
+  a.coef_x = coef_x_.get();
   a.ramp = bx0;   // launch_damp_tables ramp length
   a.epi = epi ? *epi : Epilogue{};
   a.damp_z = damp_z_.get();
@@ -373,7 +375,8 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
     // the fused step is the warp-specialised kernel with 376-deep bands
     if (stream_kernel != 1) a.xchunk = 64;
     launch_ws_step(ar, damped, 376, (stream_kernel == 1 || stream_kernel == 4) ? stream_depth : 3, a, n, st_);
-  } else if (stream_kernel == 3) launch_ws2_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  } else if (stream_kernel == 5) launch_rq_step(ar, damped, stream_depth, a, n, st_);
+  else if (stream_kernel == 3) launch_ws2_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   else if (stream_kernel == 2) launch_wi_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   else if (stream_kernel == 1) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   else if (stream_kernel == 4) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_, true);
@@ -603,10 +606,10 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
 }
 
 template <typename T>
-void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
+bool Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                               long long slot_stride, int i_stride, PointSet rec, int ngrec,
                               const T *vsrc, const void *velrcp, const std::vector<PtLine> *src_lines,
-                              const std::vector<PtLine> *rec_lines) {
+                              const std::vector<PtLine> *rec_lines, bool sum_images) {
   size_t f = (size_t)n * fstride;
   w.g0.resize(f);
   w.g1.resize(f);
@@ -679,9 +682,10 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
       if (last) break;
     }
     });
-    return;
+    return false;
   }
-  key.push_back(0);   // separate launches
+  const bool summed = sum_images && sizeof(T) == 4 && ar == ARITH_FAST;
+  key.push_back(summed ? 2 : 0);   // separate launches (2: one summed image)
   loop_key_common(key);
   run_loop(1, (double)n * nxpad * nzpad, key, [&] {
   for (int it = nt - 1; it >= 0; it--) {
@@ -707,9 +711,14 @@ void Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
     if ((double)t > 0.4) scale = 1.0f;
     else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
     else break;
-    launch_image<T>(w.image.get() + kStreamCoff, fstride, sp0, gp0, fstride, n, npts, scale, st_);
+    if (summed)
+      launch_image_sum(reinterpret_cast<float *>(w.image.get()) + kStreamCoff, reinterpret_cast<const float *>(sp0),
+                       reinterpret_cast<const float *>(gp0), fstride, n, npts, scale, st_);
+    else
+      launch_image<T>(w.image.get() + kStreamCoff, fstride, sp0, gp0, fstride, n, npts, scale, st_);
   }
   });
+  return summed;
 }
 
 template <typename T>
@@ -836,10 +845,12 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
                           ngmax, k, st_);
     launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);
     launch_trans_vsrc(w_.vsrc.get(), w_.res.get(), nt, ngmax, k, st_);
-    run_backward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.vsrc.get(), rcp, lines ? &sl : nullptr,
-                        lines ? &rl : nullptr);
-    launch_finalize_gradient(grad, w_.image.get() + kStreamCoff, fstride, k, nxpad, nzpad, bx0, pitch,
-                             (accumulate || c0 > 0) ? 1 : 0, st_);
+    // FAST arithmetic images all shots of the batch into one image (one
+    // read-modify-write a step for the whole batch)
+    const bool summed = run_backward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.vsrc.get(), rcp,
+                                            lines ? &sl : nullptr, lines ? &rl : nullptr, arith == ARITH_FAST);
+    launch_finalize_gradient(grad, w_.image.get() + kStreamCoff, fstride, summed ? 1 : k, nxpad, nzpad, bx0,
+                             pitch, (accumulate || c0 > 0) ? 1 : 0, st_);
     if (obj) {
       SWFWI_CUDA(cudaMemcpyAsync(obj + c0, w_.obj.get(), sizeof(double) * k, cudaMemcpyDeviceToHost,
                                  st_));
@@ -930,6 +941,22 @@ void Propagator::calgradient_fwi_f64(const float *vel, const double *wlt, const 
   to_pitched(wd_.image.get() + kStreamCoff, grad);
   run_forward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, nullptr, true, r64.get() + kStreamCoff);
   run_backward<double>(wd_, 1, src, wlt, 1, 0, 0, rec, ng, vsrc, r64.get() + kStreamCoff);
+  from_pitched(grad, wd_.image.get() + kStreamCoff);
+  SWFWI_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Propagator::calgradient_ess_f64(const float *vel, const double *encsrc, const double *vsrc,
+                                     double *grad) {
+  SWFWI_REQUIRE(vel && encsrc && vsrc && grad, "null pointer");
+  DevBuf<double> r64((size_t)nxpad * pitch + 2 * kStreamCoff);
+  launch_to_f64_reciprocal(r64.get() + kStreamCoff, vel, nxpad, nzpad, pitch, st_);
+  PointSet src{d_src_pos_p_.get(), ns, nullptr};
+  PointSet rec{d_geo_pos_p_.get(), ng, nullptr};
+  wd_.image.resize((size_t)fstride);
+  wd_.image.zero(st_);
+  to_pitched(wd_.image.get() + kStreamCoff, grad);
+  run_forward<double>(wd_, 1, src, encsrc, ns, 0, 1, rec, ng, nullptr, true, r64.get() + kStreamCoff);
+  run_backward<double>(wd_, 1, src, encsrc, ns, 0, 1, rec, ng, vsrc, r64.get() + kStreamCoff);
   from_pitched(grad, wd_.image.get() + kStreamCoff);
   SWFWI_CUDA(cudaStreamSynchronize(st_));
 }

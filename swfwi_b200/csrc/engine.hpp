@@ -73,10 +73,11 @@ class Propagator {
   cudaStream_t stream() const { return st_; }
   int arith = ARITH_REF;
   int strip_format = SWFWI_STRIP_F32;
-  int stream_kernel = 1;      // 0: streaming, 1: warp-specialised, 2: independent warps,
-                              // 3: two rows per step, 4: prev / 1/vt from global memory
-  int stream_bz = 376;        // output depths per CTA (120, 248; 376 warp-specialised only)
-  int stream_xchunk = 64;     // rows per CTA
+  int stream_kernel = 5;      // 0: streaming, 1: warp-specialised, 2: independent warps,
+                              // 3: two rows per step, 4: prev / 1/vt from global memory,
+                              // 5: register-queue warps
+  int stream_bz = 120;        // output depths per CTA (120, 248; 376 warp-specialised only)
+  int stream_xchunk = 48;     // rows per CTA (per warp task for kernel 5)
   int stream_depth = 3;       // rows ahead (3 or 5; warp-specialised 3 or 7)
   int stream_shot_major = 0;  // launch order: 0 = shots fastest
   bool fuse = false;          // fused time loops where they apply
@@ -142,6 +143,7 @@ class Propagator {
   void calgradient_fwi(const float *wlt, const float *vsrc, float *grad, int shot_id);
   void calgradient_fwi_f64(const float *vel, const double *wlt, const double *vsrc, double *grad,
                            int shot_id);
+  void calgradient_ess_f64(const float *vel, const double *encsrc, const double *vsrc, double *grad);
   void fwi_forward_f64(const float *vel, const double *wlt, double *dcal, int shot_id);
 
   // Max shots per batch that fit the device memory budget.
@@ -164,6 +166,7 @@ class Propagator {
   long long vel_stride_ = 0;    // floats between slots' velocity reciprocals (0: one model)
   DevBuf<int> d_err_;
   DevBuf<float> damp_x_, damp_z_;   // per-axis sponge ramps (streaming step)
+  DevBuf<float2> coef_x_;           // each row's FAST ramp coefficients (streaming step)
   // positions in the caller's layout (x*nzpad + z) ...
   DevBuf<int> d_src_pos_, d_geo_pos_;
   // ... and in the propagator's pitched layout (x*pitch + z)
@@ -195,11 +198,13 @@ class Propagator {
   template <typename T>
   // With per-slot horizontal lines, FP32 fields and fusion on: the source
   // back-step also subtracts the source and images, the receiver step also
-  // injects the next residual.
-  void run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
+  // injects the next residual.  sum_images (FAST arithmetic, separate
+  // launches only): every slot images into slot 0's image, one pass per
+  // step.  Returns true when the images were summed that way.
+  bool run_backward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                     long long slot_stride, int i_stride, PointSet rec, int ngrec, const T *vsrc,
                     const void *velrcp, const std::vector<PtLine> *src_lines = nullptr,
-                    const std::vector<PtLine> *rec_lines = nullptr);
+                    const std::vector<PtLine> *rec_lines = nullptr, bool sum_images = false);
   template <typename T>
   void ensure_work(Work<T> &w, int n, bool strips);
   // Runs body (launches on st_ only, no allocation or synchronisation):

@@ -67,8 +67,13 @@ struct Tried {
 };
 }  // namespace
 
-float StepSearch::calsteplen(const std::function<float(float)> &f, float obj_val1,
+float StepSearch::calsteplen(const std::function<float(float)> &fobj, float obj_val1,
                              float max_alpha3, float &objval) {
+  trials = 0;
+  auto f = [&](float a) {
+    trials++;
+    return fobj(a);
+  };
   // initAlpha23 (updatesteplenop.cpp:273-285)
   const float minAlpha = 1.0E-7f, resetAlpha = 1.0E-4f;
   if (!preserved_init) {

@@ -36,8 +36,10 @@ struct StepSearch {
   float maxdv = 0;
   bool preserved_init = false;
   float preserved_alpha = 0;
-  // last search, for inspection
+  // last search, for inspection: its (alpha, objective) triple and vertex,
+  // and how many trial objectives (forward sweeps over all shots) it ran
   float alpha[4] = {0, 0, 0, 0}, obj[4] = {0, 0, 0, 0};
+  int trials = 0;
   // calsteplen: returns the step; objval receives its objective
   float calsteplen(const std::function<float(float)> &f, float obj_val1, float max_alpha3,
                    float &objval);

@@ -10,10 +10,10 @@
 namespace swfwi {
 
 std::atomic<long long> g_kernel_launches{0};
+void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
 namespace {
 constexpr int kThreads = 256;
-inline void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 inline unsigned grid_for(long long n, int threads = kThreads) {
   long long g = (n + threads - 1) / threads;
   return (unsigned)(g < 1 ? 1 : (g > 2147483647LL ? 2147483647LL : g));
@@ -159,6 +159,47 @@ __global__ void k_image(T *image, long long image_stride, const T *s, const T *r
       g[i] = g[i] - a[i] * b[i] * (double)scale;
     }
   }
+}
+
+// All slots' cross-correlations into one image (FAST arithmetic):
+// image[p] -= (sum over slots, in slot order, of s*r) * scale, four points
+// a thread; one image read-modify-write for all slots.  n % 4 == 0 and
+// every array 16-byte aligned.
+__global__ void __launch_bounds__(kThreads)
+k_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, long long n4,
+            float scale) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n4;
+       q += (long long)gridDim.x * blockDim.x) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 *a = reinterpret_cast<const float4 *>(s) + q;
+    const float4 *b = reinterpret_cast<const float4 *>(r) + q;
+    const long long st4 = shot_stride / 4;
+#pragma unroll 8
+    for (int slot = 0; slot < nslots; slot++) {
+      const float4 x = __ldcs(a + slot * st4), y = __ldcs(b + slot * st4);
+      acc.x = fmaf(x.x, y.x, acc.x);
+      acc.y = fmaf(x.y, y.y, acc.y);
+      acc.z = fmaf(x.z, y.z, acc.z);
+      acc.w = fmaf(x.w, y.w, acc.w);
+    }
+    float4 *g = reinterpret_cast<float4 *>(image) + q;
+    float4 v = *g;
+    v.x = __fsub_rn(v.x, __fmul_rn(acc.x, scale));
+    v.y = __fsub_rn(v.y, __fmul_rn(acc.y, scale));
+    v.z = __fsub_rn(v.z, __fmul_rn(acc.z, scale));
+    v.w = __fsub_rn(v.w, __fmul_rn(acc.w, scale));
+    *g = v;
+  }
+}
+
+void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int n,
+                      float scale, cudaStream_t st) {
+  if (n % 4 != 0 || shot_stride % 4 != 0 || (reinterpret_cast<uintptr_t>(image) | reinterpret_cast<uintptr_t>(s) |
+                                              reinterpret_cast<uintptr_t>(r)) % 16 != 0)
+    throw Error(SWFWI_ERR_BAD_ARG, "summed image: sizes and arrays must be 16-byte aligned");
+  const long long n4 = n / 4;
+  k_image_sum<<<grid_for(n4), kThreads, 0, st>>>(image, s, r, shot_stride, nslots, n4, scale);
+  note_launch();
 }
 
 template <typename T>
@@ -625,20 +666,21 @@ void launch_to_f64_reciprocal(double *out, const float *in, int nx, int nz, int 
 // Sponge ramps of fd4t10s-damp-zjh.c:64-80 split by axis: dist_x[ix] is the
 // left/right ramp (0 inside), dist_z[iz] the bottom ramp (-1 above it, where
 // the left/right one applies).
-__global__ void k_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb) {
+__global__ void k_damp_tables(float *dist_x, float *dist_z, float2 *coef_x, int nx, int nz, int nb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nx) {
     float d = 0.0f;
     if (i < nb) d = __fdiv_rn((float)(nb - i), (float)nb);
     if (i >= nx - nb) d = __fdiv_rn((float)(i - (nx - nb) + 1), (float)nb);
     dist_x[i] = d;
+    if (coef_x) coef_x[i] = fast_damp_coef(d);
   }
   if (i < nz) dist_z[i] = i >= nz - nb ? __fdiv_rn((float)(i - (nz - nb) + 1), (float)nb) : -1.0f;
 }
 
-void launch_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb, cudaStream_t st) {
+void launch_damp_tables(float *dist_x, float *dist_z, float2 *coef_x, int nx, int nz, int nb, cudaStream_t st) {
   int n = nx > nz ? nx : nz;
-  k_damp_tables<<<grid_for(n), kThreads, 0, st>>>(dist_x, dist_z, nx, nz, nb);
+  k_damp_tables<<<grid_for(n), kThreads, 0, st>>>(dist_x, dist_z, coef_x, nx, nz, nb);
   note_launch();
 }
 
@@ -858,6 +900,10 @@ k_strip_write_q(uint16_t *q, long long q_slot_stride, float *scale, long long sc
   for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wmax[w]);
   int e = 0;
   if (m > 0.f && m <= 3.0e38f) frexpf(m, &e);   // m < 2^e
+  // a step whose largest |value| is subnormal would need a scale of 2^-140
+  // or so, whose inverse overflows (and 0 * inf is NaN): such values are
+  // kept at the scale 2^-114 (they encode as 0 or as 16-bit subnormals)
+  e = max(e, -100);
   const float s = ldexpf(1.0f, e - 14), inv = ldexpf(1.0f, 14 - e);
   if (threadIdx.x == 0) scale[(long long)slot * scale_slot_stride] = s;
   uint16_t *qs = q + (long long)slot * q_slot_stride;

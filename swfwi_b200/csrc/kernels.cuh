@@ -13,6 +13,8 @@ namespace swfwi {
 
 // Kernel launches issued by this library (all launchers count).
 extern std::atomic<long long> g_kernel_launches;
+// Counts one launch in g_kernel_launches.
+void note_launch();
 
 // ---- wavefield point operations (batched over shot slots) --------------
 // A "slot" is one wavefield in a batch; slot_shot maps it to a shot id
@@ -62,6 +64,14 @@ template <typename T>
 void launch_image(T *image, long long image_stride, const T *s, const T *r, long long shot_stride,
                   int nslots, int n, float scale, cudaStream_t st);
 
+// image -= (sum over slots of s[slot] * r[slot]) * scale: all slots'
+// cross-correlations into ONE image (FAST arithmetic; the slot terms are
+// added in slot order before the scale, so the bits differ from per-slot
+// images summed later).  n points from each array start, n % 4 == 0,
+// 16-byte aligned arrays and shot_stride.
+void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int n,
+                      float scale, cudaStream_t st);
+
 // One FD step for all slots: shared-memory tile form (any pitch, any
 // arithmetic) and streaming TMA form (float, 16-byte aligned pitched rows;
 // bz = 120 or 248 output depths per CTA, depth = 3 or 5 rows in flight).
@@ -83,11 +93,17 @@ void launch_wi_step(int arith, bool damped, int bz, int depth, const StreamArgs 
 // (stream_ws2.cuh): bz = 120, 248 or 376, depth = 3 or 7 rows ahead.
 void launch_ws2_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
                      cudaStream_t st);
+// Register-queue streaming step (stream_rq.cuh): one self-contained warp
+// pipeline (a one-warp CTA) per task of 120 output depths x a.xchunk rows
+// of one slot, depth = 3 or 7 stages ahead.
+void launch_rq_step(int arith, bool damped, int depth, const StreamArgs &a, int nslots, cudaStream_t st);
 // out[s][ig*nt + it] = in[s][it*ng + ig] for nslots seismograms
 // (matrix_transpose of common.cpp:14-24 with n1 = ng, n2 = nt).
 void launch_transpose_traces(float *out, const float *in, int nt, int ng, int nslots, cudaStream_t st);
-// Per-axis sponge ramps for the streaming step (see stream.cuh).
-void launch_damp_tables(float *dist_x, float *dist_z, int nx, int nz, int nb, cudaStream_t st);
+// Per-axis sponge ramps for the streaming step (see stream.cuh), and (if
+// coef_x is not null) each row's FAST update coefficients of the left/right
+// ramp, fast_damp_coef(dist_x[row]).
+void launch_damp_tables(float *dist_x, float *dist_z, float2 *coef_x, int nx, int nz, int nb, cudaStream_t st);
 
 // ---- per-iteration arithmetic --------------------------------------------
 // Mute windows of removeDirectArrival (damp4t10d.cpp:321-365) for one

@@ -31,6 +31,7 @@ extern "C" int swfwi_selftest_bounded_wait(void *stream) {
     DevBuf<int> err(1);
     SWFWI_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), st));
     k_selftest_mbar_timeout<<<1, 32, 0, st>>>(err.get());
+    note_launch();
     SWFWI_CUDA(cudaGetLastError());
     int h = 0;
     SWFWI_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));

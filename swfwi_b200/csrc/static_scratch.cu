@@ -9,16 +9,22 @@
 // same bits) with its partials in a file-scope device array that every GPU
 // loading this library holds until exit.
 //
-// The array's host-side name is not a device address, so the first call on
-// each device (with that device current) looks the address up with
-// cudaGetSymbolAddress and caches it; that first call should come before any
-// stream capture.  Every call shares the array and leaves its partials
+// The array's host-side name is not a device address, so the first call in
+// each CUDA context (with its device current) looks the address up with
+// cudaGetSymbolAddress and caches it under that context; that first call
+// should come before any stream capture.  A context created later on the
+// same device (after cudaDeviceReset, or a non-primary context) gets its
+// own lookup.  Every call shares the array and leaves its partials
 // there: each call overwrites all the partials it reads, so nothing has to
 // start at zero, but calls whose kernels overlap on the GPU (different
 // streams, or different host threads) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <map>
 #include <mutex>
+#include <utility>
 #include "common.hpp"
+#include "kernels.cuh"
 
 namespace swfwi {
 namespace {
@@ -65,20 +71,39 @@ __global__ void k_static_final(double *out, const double *partials) {
   if (threadIdx.x == 0) out[slot] = acc;
 }
 
-// Device address of the partials array, looked up once per device.
+// The current CUDA context (the driver's cuCtxGetCurrent, reached through
+// the runtime so the library needs no link against the driver library).
+CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext *);
+  static Fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<Fn>(p);
+  });
+  SWFWI_REQUIRE(fn != nullptr, "cuCtxGetCurrent is not available from the CUDA driver");
+  CUcontext c = nullptr;
+  SWFWI_REQUIRE(fn(&c) == CUDA_SUCCESS && c != nullptr, "no current CUDA context");
+  return c;
+}
+
+// Device address of the partials array, looked up once per context.
 double *partials_on_current_device() {
   static std::mutex mu;
-  static double *addr[128] = {nullptr};
+  static std::map<std::pair<int, CUcontext>, double *> addr;
   int dev = 0;
   SWFWI_CUDA(cudaGetDevice(&dev));
-  SWFWI_REQUIRE(dev >= 0 && dev < 128, "device index out of range");
+  SWFWI_CUDA(cudaFree(nullptr));   // makes the device's primary context current if none is
+  const std::pair<int, CUcontext> key(dev, current_context());
   std::lock_guard<std::mutex> g(mu);
-  if (!addr[dev]) {
-    void *p = nullptr;
-    SWFWI_CUDA(cudaGetSymbolAddress(&p, g_objective_partials));
-    addr[dev] = static_cast<double *>(p);
-  }
-  return addr[dev];
+  auto it = addr.find(key);
+  if (it != addr.end()) return it->second;
+  void *p = nullptr;
+  SWFWI_CUDA(cudaGetSymbolAddress(&p, g_objective_partials));
+  return addr[key] = static_cast<double *>(p);
 }
 
 }  // namespace
@@ -95,7 +120,9 @@ extern "C" int swfwi_cal_objective_static(const float *r, long long n_per_slot, 
     double *partials = partials_on_current_device();
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     k_static_partials<<<dim3(kStaticPartials, nslots), kThreads, 0, st>>>(partials, r, n_per_slot);
+    note_launch();
     k_static_final<<<nslots, kThreads, 0, st>>>(obj, partials);
+    note_launch();
     SWFWI_CUDA(cudaGetLastError());
   });
 }

@@ -61,6 +61,7 @@ struct Epilogue {
 
 struct StreamArgs {
   float *prev;            // field origins (see layout above)
+  const float2 *coef_x;   // FAST update coefficients of each row's left/right ramp, [nx]
   const float *curr;
   const float *rcp;       // 1/vt, same layout
   const float *damp_x;    // sponge ramp of each row (0 outside), [nx]
@@ -77,6 +78,16 @@ struct StreamArgs {
 };
 
 constexpr int kStreamCoff = 8;   // floats between a slot's start and its origin
+
+// FAST update coefficients of a sponge ramp distance: next = cf*c + pc*p
+// + inc with delta = 0.05 dist^2, cf = 2 - 2 delta + delta^2 (one fma),
+// pc = -(1 - 2 delta); (2, -1) where dist is 0 (no damping).
+__device__ __forceinline__ float2 fast_damp_coef(float dist) {
+  if (dist == 0.0f) return make_float2(2.0f, -1.0f);
+  const float delta = __fmul_rn(__fmul_rn(0.05f, dist), dist);
+  const float d2 = __fmul_rn(2.0f, delta);
+  return make_float2(fmaf(delta, delta, __fsub_rn(2.0f, d2)), -__fsub_rn(1.0f, d2));
+}
 
 namespace stream_detail {
 
@@ -218,17 +229,19 @@ __device__ __forceinline__ float update_pt(float c, float p, float r, float uc, 
     acc = __dadd_rn(acc, (double)t4);
     return __double2float_rn(acc);
   } else {
-    float lap = ((uzm + uzp) + (uxm + uxp)) - 4.0f * uc;
-    float q = r * (1.0f / 12.0f);
-    float inc = r * fmaf(q, lap, uc);
+    // every rounding spelled out, so each kernel evaluates the same
+    // sequence: lap = fma(-4, uc, s), base = fma(coef, c, p * pc)
+    const float lap = fmaf(-4.0f, uc, __fadd_rn(__fadd_rn(uzm, uzp), __fadd_rn(uxm, uxp)));
+    const float q = __fmul_rn(r, 1.0f / 12.0f);
+    const float inc = __fmul_rn(r, fmaf(q, lap, uc));
     float base;
     if (delta == 0.0f) {
-      base = fmaf(2.0f, c, -p);
+      base = fmaf(2.0f, c, __fmul_rn(p, -1.0f));
     } else {
-      float d2 = 2.0f * delta;
-      base = fmaf(2.0f - d2 + delta * delta, c, -(1.0f - d2) * p);
+      const float d2 = __fmul_rn(2.0f, delta);
+      base = fmaf(fmaf(delta, delta, __fsub_rn(2.0f, d2)), c, __fmul_rn(p, -__fsub_rn(1.0f, d2)));
     }
-    return base + inc;
+    return __fadd_rn(base, inc);
   }
 }
 
@@ -263,6 +276,21 @@ __device__ __forceinline__ float2 update_pair_fast(float2 c, float2 p, float2 r,
   const float2 q = __fmul2_rn(r, f2(1.0f / 12.0f, 1.0f / 12.0f));
   const float2 inc = __fmul2_rn(r, __ffma2_rn(q, lap, uc));
   const float2 base = __ffma2_rn(f2(2.0f, 2.0f), c, __fmul2_rn(p, f2(-1.0f, -1.0f)));
+  return __fadd2_rn(base, inc);
+}
+
+// FAST time update of a depth pair with sponge coefficients:
+// out = cf*c + pc*p + r*(uc + (r/12)*lap), lap = (sz + (uxm + uxp)) - 4 uc,
+// sz = uzm + uzp (the z neighbours' sum, formed by the caller).  Each lane
+// is evaluated as update_pt<ARITH_FAST> evaluates a point; cf = 2, pc = -1
+// where no sponge acts.
+__device__ __forceinline__ float2 update_pair_coef(float2 c, float2 p, float2 r, float2 uc, float2 sz, float2 uxm,
+                                                   float2 uxp, float2 cf, float2 pc) {
+  const float2 s = __fadd2_rn(sz, __fadd2_rn(uxm, uxp));
+  const float2 lap = __ffma2_rn(f2(-4.0f, -4.0f), uc, s);
+  const float2 q = __fmul2_rn(r, f2(1.0f / 12.0f, 1.0f / 12.0f));
+  const float2 inc = __fmul2_rn(r, __ffma2_rn(q, lap, uc));
+  const float2 base = __ffma2_rn(cf, c, __fmul2_rn(p, pc));
   return __fadd2_rn(base, inc);
 }
 

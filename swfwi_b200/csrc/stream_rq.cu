@@ -1,0 +1,52 @@
+// Launcher of the register-queue streaming step (stream_rq.cuh); its own
+// translation unit so it compiles beside kernels.cu.
+#include "common.hpp"
+#include "kernels.cuh"
+#include "stream_rq.cuh"
+
+namespace swfwi {
+
+namespace {
+
+template <int ARITH, bool DAMPED, int NW, int D>
+void rq_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+  constexpr size_t smem = rq_smem_bytes<NW, D>();
+  static bool attr_set = false;   // raise the dynamic shared memory limit once
+  if (!attr_set) {
+    cudaFuncSetAttribute(fd_step_rq<ARITH, DAMPED, NW, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_set = true;
+  }
+  const long long nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
+  const long long tasks = (long long)nslots * rq_detail::slices(a.nz) * nchunks;
+  const long long blocks = (tasks + NW - 1) / NW;
+  if (blocks > 0x7fffffffLL) throw Error(SWFWI_ERR_BAD_ARG, "too many stencil tasks for one launch");
+  fd_step_rq<ARITH, DAMPED, NW, D><<<(unsigned)blocks, NW * 32, smem, st>>>(a, nslots);
+}
+
+// One warp per CTA: the warps' tasks are independent, and a one-warp CTA
+// frees its slot as soon as its task ends (measured faster than 2-4 warps
+// per CTA, which also need more registers than the 20-warp occupancy
+// leaves).
+template <int ARITH, bool DAMPED>
+void rq_d(int depth, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (depth >= 7) rq_t<ARITH, DAMPED, 1, 7>(a, nslots, st);
+  else rq_t<ARITH, DAMPED, 1, 3>(a, nslots, st);
+}
+
+}  // namespace
+
+void launch_rq_step(int arith, bool damped, int depth, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
+  if (a.xchunk <= 0) throw Error(SWFWI_ERR_BAD_ARG, "rows per task must be positive");
+  if (arith == ARITH_REF) {
+    if (damped) rq_d<ARITH_REF, true>(depth, a, nslots, st);
+    else rq_d<ARITH_REF, false>(depth, a, nslots, st);
+  } else {
+    if (damped) rq_d<ARITH_FAST, true>(depth, a, nslots, st);
+    else rq_d<ARITH_FAST, false>(depth, a, nslots, st);
+  }
+  note_launch();
+}
+
+}  // namespace swfwi

@@ -172,6 +172,16 @@ fd_step_ws(StreamArgs a) {
       coldamp = coldamp || dz[i] >= 0.f;
     }
   }
+  // FAST sponge coefficients of this thread's depths in the bottom ramp
+  float cfz[4] = {2.f, 2.f, 2.f, 2.f}, pcz[4] = {-1.f, -1.f, -1.f, -1.f};
+  if constexpr (DAMPED && ARITH == ARITH_FAST) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const float2 c = fast_damp_coef(dz[i] >= 0.f ? dz[i] : 0.0f);
+      cfz[i] = c.x;
+      pcz[i] = c.y;
+    }
+  }
   const bool outgroup = t >= 1 && t < NT - 1 && zg < nz - 6 && zg + 3 >= 6;
   const bool fullgroup = zok[0] && zok[1] && zok[2] && zok[3];
   const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
@@ -344,6 +354,22 @@ fd_step_ws(StreamArgs a) {
                                     get(um4, i), get(up4, i), 0.0f);
           }
         }
+      } else if constexpr (ARITH == ARITH_FAST) {
+        // sponge coefficients: the bottom ramp overrides the row's
+        const float2 cx = a.coef_x[xa - 12 + k];
+        float cf[4], pc[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          cf[i] = dz[i] >= 0.f ? cfz[i] : cx.x;
+          pc[i] = dz[i] >= 0.f ? pcz[i] : cx.y;
+        }
+        const float2 a0 = update_pair_coef(lo2(c4), lo2(p4), lo2(r4), lo2(uc4),
+                                           f2(__fadd_rn(ucl, uc4.y), __fadd_rn(uc4.x, uc4.z)), lo2(um4), lo2(up4),
+                                           f2(cf[0], cf[1]), f2(pc[0], pc[1]));
+        const float2 b0 = update_pair_coef(hi2(c4), hi2(p4), hi2(r4), hi2(uc4),
+                                           f2(__fadd_rn(uc4.y, uc4.w), __fadd_rn(uc4.z, ucr)), hi2(um4), hi2(up4),
+                                           f2(cf[2], cf[3]), f2(pc[2], pc[3]));
+        o[0] = a0.x; o[1] = a0.y; o[2] = b0.x; o[3] = b0.y;
       } else {
 #pragma unroll
         for (int i = 0; i < 4; i++) {

@@ -49,7 +49,7 @@ void launch_ws2_step(int arith, bool damped, int bz, int depth, const StreamArgs
     if (damped) ws2_d<ARITH_FAST, true>(depth, bz, a, nslots, st);
     else ws2_d<ARITH_FAST, false>(depth, bz, a, nslots, st);
   }
-  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  note_launch();
 }
 
 }  // namespace swfwi

@@ -36,7 +36,7 @@ def ref():
     """The compiled reference (oracle/_ref); built here when the reference
     tree is present, skipped where it is neither built nor buildable."""
     import oracle
-    if not oracle.available() and os.path.isdir("/root/reference/src"):
+    if not oracle.available() and oracle.reference_tree():
         oracle.build()
     if not oracle.available():
         pytest.skip("oracle/_ref not built")
@@ -47,7 +47,7 @@ def ref():
 def fdo():
     import oracle
     if not os.path.exists(os.path.join(oracle.REF_DIR, "libfd_oracle.so")):
-        if os.path.isdir("/root/reference/src"):
+        if oracle.reference_tree():
             oracle.build()
         else:
             pytest.skip("oracle/_ref not built")

@@ -121,3 +121,31 @@ def test_enkf_analyze_pipeline_matches_oracle(cuda):
     want = E.analyze_update(vels.reshape(n, -1), want_t4, s.dx, s.dt).reshape(vels.shape)
     got = vg.cpu().numpy()
     assert (np.abs(got - want) / np.abs(want)).max() < 1e-5
+
+
+def test_analysis_in_one_call_matches_gain_then_update(cuda):
+    # the gain kept in device memory and applied at once gives the bits of
+    # the two-call form; a non-finite gain leaves the members unchanged
+    import swfwi_b200 as S
+    torch = cuda
+    n, rows, model = 40, 30000, 20000
+    dx, dt = 20.0, 0.002
+    hona, dobs, z = _case(n, rows, seed=11)
+    rng = np.random.default_rng(12)
+    vels = E.vel_trans((2500 + 200 * rng.standard_normal((n, model))).astype(np.float32), dx, dt)
+    h, d, zz = t(torch, hona), t(torch, dobs), t(torch, z)
+    t4a, sa, ca = S.enkf_gain_matrix(h, d, zz, sigfac=0.05)
+    va = t(torch, vels).clone()
+    S.enkf_update(va, t4a, dx, dt)
+    vb = t(torch, vels).clone()
+    t4b, sb, cb = S.enkf_analyze(h, d, vb, dx, dt, z=zz, sigfac=0.05)
+    assert sa == sb and ca == cb
+    np.testing.assert_array_equal(t4a, t4b)
+    np.testing.assert_array_equal(va.cpu().numpy(), vb.cpu().numpy())
+    bad = hona.copy()
+    bad[3, 17] = np.nan
+    vc = t(torch, vels).clone()
+    with pytest.raises(S.SwfwiError) as e:
+        S.enkf_analyze(t(torch, bad), d, vc, dx, dt, z=zz, sigfac=0.05, sigma=sa)
+    assert e.value.status == 4              # SWFWI_ERR_NONFINITE
+    np.testing.assert_array_equal(vc.cpu().numpy(), vels)

@@ -13,8 +13,11 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("arith", [0, 1])
 def test_fused_and_separate_paths_identical(cuda, arith):
-    # same kernels' arithmetic either way: bit-identical seismograms and
-    # gradients in REF and FAST
+    # same kernels' arithmetic either way: bit-identical seismograms, and
+    # gradients in REF; in FAST the separate path images every shot into
+    # one image (summed before the scale), so its gradient matches to
+    # rounding
+    from tests.conftest import rel_l2
     torch = cuda
     out = []
     for fuse in (True, False):
@@ -26,7 +29,10 @@ def test_fused_and_separate_paths_identical(cuda, arith):
         obj = m.gradient_batch(t(torch, g["wlt"]), t(torch, g["dobs"]), [0, 1, 2], gr)
         out.append((d.cpu().numpy(), gr.cpu().numpy(), obj))
     np.testing.assert_array_equal(out[0][0], out[1][0])
-    np.testing.assert_array_equal(out[0][1], out[1][1])
+    if arith == 0:
+        np.testing.assert_array_equal(out[0][1], out[1][1])
+    else:
+        assert rel_l2(out[1][1], out[0][1]) < 1e-6
     np.testing.assert_array_equal(out[0][2], out[1][2])
     if arith == 0:
         np.testing.assert_array_equal(out[0][0], golden("small_survey")["dcal"])

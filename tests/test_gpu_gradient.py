@@ -30,7 +30,8 @@ def test_calgradient_ess_bit_exact(cuda):
 
 @pytest.mark.parametrize("tuning", [None, (1, 248, 7, 3, 1), (2, 360, 64, 3, 0), (2, 240, 5, 7, 1),
                                     (3, 376, 64, 7, 0), (3, 248, 9, 3, 1), (4, 376, 64, 3, 0),
-                                    (4, 248, 9, 7, 1)])
+                                    (4, 248, 9, 7, 1), (5, 120, 64, 3, 0), (5, 120, 7, 7, 0),
+                                    (5, 120, 1, 3, 0)])
 def test_gradient_batch_matches_reference_loop(cuda, tuning):
     # the per-shot loop of FwiFramework::epoch: gradient bit-exact, the
     # objective summed in FP64 (the reference sums in float); with the
@@ -76,7 +77,7 @@ def test_fast_gradient_within_tolerance_and_f64(cuda, fdo):
     print(f"gradient rel-L2 vs FP64: REF {rel_l2(g['grad_shot1'], g64):.2e}  FAST {rel_l2(fast, g64):.2e}")
 
 
-@pytest.mark.parametrize("fmt,bound", [(1, 2e-3), (2, 2e-2)])
+@pytest.mark.parametrize("fmt,bound", [(1, 1e-4), (2, 1e-4)])
 def test_16bit_strips_gradient_error_vs_f64(cuda, fmt, bound):
     # scaled FP16 / BF16 boundary strips: the gradient's error against the
     # FP64 run of the same scheme, beside the FP32-strip gradient's
@@ -109,7 +110,7 @@ def test_16bit_strips_batched_gradient(cuda):
     m.set_strip_format(S.STRIP_F16)
     gr = torch.zeros(g["grad_sum"].shape, device="cuda")
     obj = m.gradient_batch(t(torch, g["wlt"]), t(torch, g["dobs"]), [0, 1, 2], gr)
-    assert rel_l2(gr.cpu().numpy(), g["grad_sum"]) < 2e-3
+    assert rel_l2(gr.cpu().numpy(), g["grad_sum"]) < 1e-4
     assert abs(obj.sum() - float(g["obj"])) / float(g["obj"]) < 1e-5
 
 

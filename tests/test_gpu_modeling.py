@@ -195,7 +195,9 @@ def test_errors_reported(cuda):
     (1, 376, 16, 3, 0), (1, 248, 33, 3, 1),
     (2, 240, 1, 3, 1), (2, 360, 64, 7, 0), (2, 480, 9, 3, 0), (2, 240, 33, 7, 0), (2, 360, 16, 3, 1),
     (3, 376, 64, 7, 0), (3, 376, 33, 3, 0), (3, 248, 1, 7, 1), (3, 120, 2, 3, 0), (3, 376, 17, 7, 1),
-    (4, 376, 64, 3, 0), (4, 376, 33, 7, 0), (4, 248, 1, 3, 1), (4, 120, 2, 7, 0), (4, 376, 17, 3, 1)])
+    (4, 376, 64, 3, 0), (4, 376, 33, 7, 0), (4, 248, 1, 3, 1), (4, 120, 2, 7, 0), (4, 376, 17, 3, 1),
+    (5, 120, 1, 3, 0), (5, 120, 9, 7, 0), (5, 120, 64, 3, 0), (5, 120, 33, 7, 0), (5, 120, 200, 3, 0),
+    (5, 120, 11, 3, 0), (5, 120, 12, 7, 0), (5, 120, 8, 3, 0), (5, 120, 16, 7, 0)])
 def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     # every band depth / chunk length of the streaming stencil gives the
     # reference's seismogram bit for bit
@@ -209,7 +211,8 @@ def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
 
 @pytest.mark.parametrize("kern,bz,depth", [(0, 120, 5), (0, 248, 3), (1, 120, 7), (1, 248, 3), (1, 376, 3),
                                            (1, 376, 7), (2, 240, 3), (2, 360, 7), (2, 480, 3), (3, 376, 7),
-                                           (3, 248, 3), (4, 376, 3), (4, 376, 7), (4, 248, 3)])
+                                           (3, 248, 3), (4, 376, 3), (4, 376, 7), (4, 248, 3),
+                                           (5, 120, 3), (5, 120, 7)])
 def test_stream_matches_reference_large_grid(cuda, ref, kern, bz, depth):
     # 921 x 301 (993 x 343 padded, pitch 344): several bands, a short last
     # band, many chunks
