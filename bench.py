@@ -743,8 +743,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                 "frac": step_gbs / peak, "peak_basis": peak_kind,
                 "traffic": (tpp * per_launch_pts) if tpp else None,
-                "kernel": {0: "fd_step_stream", 1: "fd_step_ws", 2: "fd_step_wi", 3: "fd_step_ws2",
-                           4: "fd_step_ws (global prev)", 5: "fd_step_rq"}.get(tuning.get("kernel", 1)),
+                "kernel": {1: "fd_step_ws", 5: "fd_step_rq"}.get(tuning.get("kernel", 5)),
                 "launches": st["step_launches"],
                 "avg_launch_us": st["step_ms"] * 1e3 / max(st["step_launches"], 1),
                 "bytes_per_launch": st["step_bytes"] / max(st["step_launches"], 1),

@@ -106,17 +106,13 @@ int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith);
  * write_bndry/read_bndry calls always use FP32. */
 int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
 /* Launch shape of the propagator's stencil (results do not depend on it):
- * kernel 0 = streaming step (band depth 120 or 248 = one or two warps,
- * rows ahead 3 or 5), kernel 1 = warp-specialised streaming step (band
- * depth 120, 248 or 376 = 1-3 consumer warps plus a copy warp, rows ahead 3
- * or 7), kernel 2 = streaming step with independent consumer warps (band
- * depth 240, 360 or 480 = 2-4 consumer warps plus a copy warp, rows ahead 3
- * or 7), kernel 3 = kernel 1 with two output rows per consumer step (band
- * depth 120, 248 or 376, rows ahead 3 or 7), kernel 4 = kernel 1 with the
- * previous field and 1/vt loaded from global memory by the consumers (no
- * shared-memory ring for them; band depth 120, 248 or 376, rows ahead 3 or
- * 7; the fused time loop keeps kernel 1); rows per CTA >= 1;
- * shots_slowest = 1 runs the CTAs of one shot together. */
+ * kernel 5 (default) = register-queue streaming step, one warp a task of
+ * 120 output depths x rows_per_cta rows, each warp its own TMA pipeline
+ * (band depth 120, rows ahead 3 or 7); kernel 1 = warp-specialised
+ * streaming step (band depth 120, 248 or 376 = 1-3 consumer warps plus a
+ * copy warp, rows ahead 3 or 7; the fused time loop always uses it);
+ * rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot together
+ * (kernel 1). */
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest);
 /* Fused backward time loop (default off): where sources and receivers form

@@ -205,26 +205,14 @@ int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on) {
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest) {
   return guarded([&] {
-    SWFWI_REQUIRE(kernel >= 0 && kernel <= 5, "kernel must be 0, 1, 2, 3, 4 or 5");
+    SWFWI_REQUIRE(kernel == 1 || kernel == 5, "kernel must be 1 or 5");
     if (kernel == 5) {
       SWFWI_REQUIRE(band_depth == 120, "band depth must be 120 (one warp a task)");
-      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
-    } else if (kernel == 3 || kernel == 4) {
-      SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,
-                    "band depth must be 120, 248 or 376");
-      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
-    } else if (kernel == 2) {
-      SWFWI_REQUIRE(band_depth == 240 || band_depth == 360 || band_depth == 480,
-                    "band depth must be 240, 360 or 480");
-      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
-    } else if (kernel == 0) {
-      SWFWI_REQUIRE(band_depth == 120 || band_depth == 248, "band depth must be 120 or 248");
-      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 5, "rows in flight must be 3 or 5");
     } else {
       SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,
                     "band depth must be 120, 248 or 376");
-      SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
     }
+    SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
     SWFWI_REQUIRE(rows_per_cta >= 1, "rows per CTA must be positive");
     P(h).stream_kernel = kernel;
     P(h).stream_bz = band_depth;

@@ -374,13 +374,12 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   if (epi) {
     // the fused step is the warp-specialised kernel with 376-deep bands
     if (stream_kernel != 1) a.xchunk = 64;
-    launch_ws_step(ar, damped, 376, (stream_kernel == 1 || stream_kernel == 4) ? stream_depth : 3, a, n, st_);
-  } else if (stream_kernel == 5) launch_rq_step(ar, damped, stream_depth, a, n, st_);
-  else if (stream_kernel == 3) launch_ws2_step(ar, damped, stream_bz, stream_depth, a, n, st_);
-  else if (stream_kernel == 2) launch_wi_step(ar, damped, stream_bz, stream_depth, a, n, st_);
-  else if (stream_kernel == 1) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
-  else if (stream_kernel == 4) launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_, true);
-  else launch_stream_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+    launch_ws_step(ar, damped, 376, stream_kernel == 1 ? stream_depth : 3, a, n, st_);
+  } else if (stream_kernel == 5) {
+    launch_rq_step(ar, damped, stream_depth, a, n, st_);
+  } else {
+    launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
+  }
   if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
 }
 

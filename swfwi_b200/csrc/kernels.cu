@@ -684,28 +684,6 @@ void launch_damp_tables(float *dist_x, float *dist_z, float2 *coef_x, int nx, in
   note_launch();
 }
 
-// ---------------------------------------------------------------- streaming step
-template <int ARITH, bool DAMPED, int NW, int D>
-static void stream_t(const StreamArgs &a, int nslots, cudaStream_t st) {
-  constexpr int BZ = 128 * NW - 8;
-  int nbands = (a.nz - 10 + BZ - 1) / BZ;
-  int nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
-  dim3 g = a.shot_major ? dim3(nbands, nchunks, nslots) : dim3(nslots, nbands, nchunks);
-  fd_step_stream<ARITH, DAMPED, NW, D><<<g, NW * 32, 0, st>>>(a);
-}
-
-template <int ARITH, bool DAMPED, int D>
-static void stream_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
-  if (bz >= 248) stream_t<ARITH, DAMPED, 2, D>(a, nslots, st);
-  else stream_t<ARITH, DAMPED, 1, D>(a, nslots, st);
-}
-
-template <int ARITH, bool DAMPED>
-static void stream_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
-  if (depth >= 5) stream_nw<ARITH, DAMPED, 5>(bz, a, nslots, st);
-  else stream_nw<ARITH, DAMPED, 3>(bz, a, nslots, st);
-}
-
 // ---------------------------------------------------------------- warp-specialised step
 template <int ARITH, bool DAMPED, int NW, int D, int EPI>
 static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
@@ -724,14 +702,10 @@ static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
 }
 
 template <int ARITH, bool DAMPED, int NW, int D>
-static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st, bool global_prev) {
+static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st) {
   const Epilogue &e = a.epi;
   const int mode = (e.sub || e.image) ? 2 : (e.inj ? 3 : 0);
   if (mode == 2 && e.inj) throw Error(SWFWI_ERR_BAD_ARG, "mixed fused epilogue parts");
-  if (global_prev) {
-    if (mode) throw Error(SWFWI_ERR_BAD_ARG, "the global-prev step has no fused epilogue");
-    return ws_launch<ARITH, DAMPED, NW, D, 4>(a, nslots, st);
-  }
   if constexpr (NW == 3) {
     if (mode == 2) return ws_launch<ARITH, DAMPED, NW, D, 2>(a, nslots, st);
     if (mode == 3) return ws_launch<ARITH, DAMPED, NW, D, 3>(a, nslots, st);
@@ -742,40 +716,27 @@ static void ws_t(const StreamArgs &a, int nslots, cudaStream_t st, bool global_p
 }
 
 template <int ARITH, bool DAMPED, int D>
-static void ws_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st, bool gp) {
-  if (bz >= 376) ws_t<ARITH, DAMPED, 3, D>(a, nslots, st, gp);
-  else if (bz >= 248) ws_t<ARITH, DAMPED, 2, D>(a, nslots, st, gp);
-  else ws_t<ARITH, DAMPED, 1, D>(a, nslots, st, gp);
+static void ws_nw(int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (bz >= 376) ws_t<ARITH, DAMPED, 3, D>(a, nslots, st);
+  else if (bz >= 248) ws_t<ARITH, DAMPED, 2, D>(a, nslots, st);
+  else ws_t<ARITH, DAMPED, 1, D>(a, nslots, st);
 }
 
 template <int ARITH, bool DAMPED>
-static void ws_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st, bool gp) {
-  if (depth >= 7) ws_nw<ARITH, DAMPED, 7>(bz, a, nslots, st, gp);
-  else ws_nw<ARITH, DAMPED, 3>(bz, a, nslots, st, gp);
+static void ws_d(int depth, int bz, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (depth >= 7) ws_nw<ARITH, DAMPED, 7>(bz, a, nslots, st);
+  else ws_nw<ARITH, DAMPED, 3>(bz, a, nslots, st);
 }
 
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
-                    cudaStream_t st, bool global_prev) {
+                    cudaStream_t st) {
   if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
   if (arith == ARITH_REF) {
-    if (damped) ws_d<ARITH_REF, true>(depth, bz, a, nslots, st, global_prev);
-    else ws_d<ARITH_REF, false>(depth, bz, a, nslots, st, global_prev);
+    if (damped) ws_d<ARITH_REF, true>(depth, bz, a, nslots, st);
+    else ws_d<ARITH_REF, false>(depth, bz, a, nslots, st);
   } else {
-    if (damped) ws_d<ARITH_FAST, true>(depth, bz, a, nslots, st, global_prev);
-    else ws_d<ARITH_FAST, false>(depth, bz, a, nslots, st, global_prev);
-  }
-  note_launch();
-}
-
-void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamArgs &a,
-                        int nslots, cudaStream_t st) {
-  if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
-  if (arith == ARITH_REF) {
-    if (damped) stream_d<ARITH_REF, true>(depth, bz, a, nslots, st);
-    else stream_d<ARITH_REF, false>(depth, bz, a, nslots, st);
-  } else {
-    if (damped) stream_d<ARITH_FAST, true>(depth, bz, a, nslots, st);
-    else stream_d<ARITH_FAST, false>(depth, bz, a, nslots, st);
+    if (damped) ws_d<ARITH_FAST, true>(depth, bz, a, nslots, st);
+    else ws_d<ARITH_FAST, false>(depth, bz, a, nslots, st);
   }
   note_launch();
 }

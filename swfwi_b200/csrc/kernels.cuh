@@ -72,27 +72,15 @@ void launch_image(T *image, long long image_stride, const T *s, const T *r, long
 void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int n,
                       float scale, cudaStream_t st);
 
-// One FD step for all slots: shared-memory tile form (any pitch, any
-// arithmetic) and streaming TMA form (float, 16-byte aligned pitched rows;
-// bz = 120 or 248 output depths per CTA, depth = 3 or 5 rows in flight).
+// One FD step for all slots: the shared-memory tile form (any pitch, any
+// arithmetic; stencil.cuh).
 void launch_step(int arith, bool damped, bool vel_is_rcp, int tx, const StepArgs &a, int nslots,
                  cudaStream_t st);
-void launch_stream_step(int arith, bool damped, int bz, int depth, const StreamArgs &a,
-                        int nslots, cudaStream_t st);
 // Warp-specialised streaming step (stream_ws.cuh): bz = 120, 248 or 376
 // output depths per CTA (1-3 consumer warps), depth = 3 or 7 rows ahead;
-// global_prev: the previous field and 1/vt come from global memory.
+// the fused epilogues of a.epi run with 376-deep bands.
 void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
-                    cudaStream_t st, bool global_prev = false);
-// Streaming step with independent consumer warps (stream_wi.cuh): bz = 240,
-// 360 or 480 output depths per CTA (2-4 consumer warps of 120), depth = 3
-// or 7 rows ahead.
-void launch_wi_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
                     cudaStream_t st);
-// Warp-specialised step with two output rows per consumer step
-// (stream_ws2.cuh): bz = 120, 248 or 376, depth = 3 or 7 rows ahead.
-void launch_ws2_step(int arith, bool damped, int bz, int depth, const StreamArgs &a, int nslots,
-                     cudaStream_t st);
 // Register-queue streaming step (stream_rq.cuh): one self-contained warp
 // pipeline (a one-warp CTA) per task of 120 output depths x a.xchunk rows
 // of one slot, depth = 3 or 7 stages ahead.

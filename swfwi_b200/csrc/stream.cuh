@@ -1,29 +1,16 @@
-// Streaming form of the acoustic step for sm_100a (same scheme and
-// arithmetics as stencil.cuh).
-//
-// A CTA of NW warps owns a band of BZ = 128*NW - 8 output depths (z,
-// contiguous) and a chunk of consecutive rows (x) of one shot, and walks the
-// chunk row by row:
-//  * thread 0 issues TMA bulk copies (cp.async.bulk global -> shared,
-//    completion on an mbarrier) D rows ahead: the current field's row with a
-//    12-cell margin each side into a 16-row ring, the previous field's and
-//    the velocity reciprocal's rows into (D+1)-row rings;
-//  * each thread owns 4 consecutive depths; every shared-memory access is a
-//    128-bit vector (z neighbours: 5 loads; x neighbours: 10 loads from the
-//    ring; u2 of three rows from a 4-row ring), outputs go out as 128-bit
-//    stores in place over prev;
-//  * one barrier per row (__syncwarp for a one-warp CTA) between writing u2
-//    and reading its z neighbours;
-//  * the sponge's damping comes from per-row and per-column ramp tables
-//    computed once, not per point.
-// Every mbarrier wait is bounded: on timeout the CTA raises an error flag,
-// waits (bounded) for its copies in flight and leaves.
+// Shared pieces of the streaming form of the acoustic step for sm_100a (same
+// scheme and arithmetics as stencil.cuh): the launch arguments, mbarrier and
+// TMA bulk-copy helpers, the per-point u2 and update of each arithmetic,
+// their packed FP32x2 FAST forms, and the line cursor of the fused
+// epilogues.  The kernels are stream_rq.cuh (register-queue warps) and
+// stream_ws.cuh (warp-specialised, with the fused epilogues).
 //
 // Layout: the field's origin is 8 floats into each slot (coff = 8), rows of
 // P floats (P % 8 == 0, P >= nz + 8); depth z of row x sits at origin +
-// x*P + z.  Band b starts at z0 = 4 + b*BZ, so every staged window
-// [z0-12, z0+BZ+12) and [z0-4, z0+BZ+4) and every 4-depth group starts on a
-// 16-byte boundary.
+// x*P + z.  Staged windows start at depths that are multiples of 4, so
+// every window and every 4-depth group starts on a 16-byte boundary.
+// Every mbarrier wait is bounded: on timeout a kernel raises an error flag,
+// waits (bounded) for its copies in flight and leaves.
 #pragma once
 #include <cstdint>
 #include "stencil.cuh"
@@ -348,164 +335,5 @@ struct LineCursor {
 };
 
 }  // namespace stream_detail
-
-template <int ARITH, bool DAMPED, int NW, int D>
-__global__ void __launch_bounds__(NW * 32)
-fd_step_stream(StreamArgs a) {
-  using namespace stream_detail;
-  constexpr int NT = NW * 32;
-  constexpr int BZ = 4 * NT - 8;  // output depths of the band
-  constexpr int WC = BZ + 24;     // current-field window [z0-12, z0+BZ+12)
-  constexpr int WP = BZ + 8;      // prev / velocity window [z0-4, z0+BZ+4)
-  constexpr int NC = 16;          // current-field ring (11 rows in use + D ahead)
-  constexpr int NP = D + 1;       // prev/vel ring and mbarriers
-  static_assert(D + 11 <= NC, "ring too short");
-  __shared__ __align__(128) float cring[NC][WC];
-  __shared__ __align__(128) float pring[NP][WP];
-  __shared__ __align__(128) float vring[NP][WP];
-  __shared__ __align__(16) float u2r[4][4 * NT];
-  __shared__ __align__(8) uint64_t bar[NP];
-  __shared__ int s_fail;
-
-  const int t = threadIdx.x;
-  const int shot = a.shot_major ? blockIdx.z : blockIdx.x;
-  const int band = a.shot_major ? blockIdx.x : blockIdx.y;
-  const int chunk = a.shot_major ? blockIdx.y : blockIdx.z;
-  const int nx = a.nx, nz = a.nz, P = a.pitch;
-  const int z0 = 4 + band * BZ;
-  const int zg = z0 - 4 + 4 * t;   // first depth of this thread's group
-  const int xa = 6 + chunk * a.xchunk;
-  const int xb = min(xa + a.xchunk, nx - 6);
-  if (xa >= xb) return;
-  const int K = xb - xa + 12;      // stages: current rows xa-6 .. xb+5
-  // window starts relative to the origin, in floats (>= -8) and byte counts
-  const int cz = z0 - 12, pz = z0 - 4;
-  const int clen = min(WC, P - kStreamCoff - cz), plen = min(WP, P - kStreamCoff - pz);
-  const uint32_t cbytes = (uint32_t)clen * 4u, pbytes = (uint32_t)plen * 4u;
-
-  const float *curr = a.curr + (long long)shot * a.shot_stride + cz;
-  float *prev = a.prev + (long long)shot * a.shot_stride;
-  const float *prevw = prev + pz;
-  const float *rcpw = a.rcp + (long long)(shot / a.shots_per_vel) * a.vel_stride + pz;
-
-  if (t == 0) {
-    for (int i = 0; i < NP; i++) mbar_init(&bar[i], 1);
-    fence_mbar_init();
-    s_fail = 0;
-  }
-  if constexpr (NW == 1) __syncwarp();
-  else __syncthreads();
-
-  auto issue = [&](int k) {
-    int slot = k % NP;
-    mbar_expect_tx(&bar[slot], cbytes + (k >= 12 ? 2u * pbytes : 0u));
-    bulk_g2s(&cring[k & (NC - 1)][0], curr + (long long)(xa - 6 + k) * P, cbytes, &bar[slot]);
-    if (k >= 12) {
-      long long off = (long long)(xa - 12 + k) * P;
-      bulk_g2s(&pring[slot][0], prevw + off, pbytes, &bar[slot]);
-      bulk_g2s(&vring[slot][0], rcpw + off, pbytes, &bar[slot]);
-    }
-  };
-  if (t == 0)
-    for (int k = 0; k < D && k < K; k++) issue(k);
-
-  // per-depth sponge ramps of this thread's 4 depths
-  float dz[4] = {-1.f, -1.f, -1.f, -1.f};
-  bool zok[4];
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    int z = zg + i;
-    zok[i] = z >= 6 && z < nz - 6;
-    if constexpr (DAMPED) dz[i] = (z >= 0 && z < nz) ? a.damp_z[z] : -1.f;
-  }
-  const bool outgroup = t >= 1 && t < NT - 1 && zg < nz - 6 && zg + 3 >= 6;
-  const bool fullgroup = zok[0] && zok[1] && zok[2] && zok[3];
-
-  int k = 0;
-  for (; k < K; k++) {
-    if (!mbar_wait(&bar[k % NP], (uint32_t)((k / NP) & 1))) {
-      atomicExch(a.err, 1);
-      s_fail = 1;
-    }
-    if (k >= 10) {
-      // u2 of row r = xa - 11 + k: rows r-5 .. r+5 are stages k-10 .. k
-      const float *rowc = &cring[(k - 5) & (NC - 1)][0];
-      float zn[20];
-      {
-        float4 v0 = ld4(rowc + 4 * t), v1 = ld4(rowc + 4 * t + 4), v2 = ld4(rowc + 4 * t + 8),
-               v3 = ld4(rowc + 4 * t + 12), v4 = ld4(rowc + 4 * t + 16);
-        zn[0] = v0.x; zn[1] = v0.y; zn[2] = v0.z; zn[3] = v0.w;
-        zn[4] = v1.x; zn[5] = v1.y; zn[6] = v1.z; zn[7] = v1.w;
-        zn[8] = v2.x; zn[9] = v2.y; zn[10] = v2.z; zn[11] = v2.w;
-        zn[12] = v3.x; zn[13] = v3.y; zn[14] = v3.z; zn[15] = v3.w;
-        zn[16] = v4.x; zn[17] = v4.y; zn[18] = v4.z; zn[19] = v4.w;
-      }
-      float4 xm4[6], xp4[6];
-#pragma unroll
-      for (int d = 1; d <= 5; d++) {
-        xm4[d] = ld4(&cring[(k - 5 - d) & (NC - 1)][8 + 4 * t]);
-        xp4[d] = ld4(&cring[(k - 5 + d) & (NC - 1)][8 + 4 * t]);
-      }
-      float u[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        float xm[6], xp[6];
-#pragma unroll
-        for (int d = 1; d <= 5; d++) {
-          xm[d] = get(xm4[d], i);
-          xp[d] = get(xp4[d], i);
-        }
-        xm[0] = xp[0] = 0.f;
-        u[i] = lap_pt<ARITH>(zn, i, xm, xp);
-      }
-      st4(&u2r[k & 3][4 * t], make_float4(u[0], u[1], u[2], u[3]));
-    }
-    if constexpr (NW == 1) __syncwarp();
-    else __syncthreads();
-    if (s_fail) break;
-    if (t == 0 && k + D < K) {
-      fence_proxy_async();
-      issue(k + D);
-    }
-    if (k >= 12 && outgroup) {
-      const int j = xa - 12 + k;   // output row; u2 rows j-1, j, j+1 are steps k-2, k-1, k
-      const float *um = &u2r[(k - 2) & 3][4 * t];
-      const float *uc = &u2r[(k - 1) & 3][4 * t];
-      const float *up = &u2r[k & 3][4 * t];
-      float4 c4 = ld4(&cring[(k - 6) & (NC - 1)][8 + 4 * t]);
-      float4 p4 = ld4(&pring[k % NP][4 * t]);
-      float4 r4 = ld4(&vring[k % NP][4 * t]);
-      float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
-      float ucl = uc[-1], ucr = uc[4];
-      float dxr = 0.f;
-      if constexpr (DAMPED) dxr = (j < a.ramp || j >= nx - a.ramp) ? a.damp_x[j] : 0.f;
-      float o[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        float delta = 0.f;
-        if constexpr (DAMPED) {
-          float dist = dz[i] >= 0.f ? dz[i] : dxr;
-          delta = __fmul_rn(__fmul_rn(0.05f, dist), dist);
-        }
-        float uzm = i == 0 ? ucl : get(uc4, i - 1);
-        float uzp = i == 3 ? ucr : get(uc4, i + 1);
-        o[i] = update_pt<ARITH>(get(c4, i), get(p4, i), get(r4, i), get(uc4, i), uzm, uzp,
-                                get(um4, i), get(up4, i), delta);
-      }
-      float *dst = prev + (long long)j * P + zg;
-      if (fullgroup) {
-        st4(dst, make_float4(o[0], o[1], o[2], o[3]));
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-          if (zok[i]) dst[i] = o[i];
-      }
-    }
-  }
-  if (s_fail && t == 0) {
-    // wait (bounded) for this CTA's copies still in flight before leaving
-    for (int i = k + 1; i < K && i < k + D; i++) mbar_wait(&bar[i % NP], (uint32_t)((i / NP) & 1));
-  }
-}
 
 }  // namespace swfwi

@@ -59,32 +59,23 @@ struct Smem {
 
 }  // namespace ws_detail
 
-// D rows ahead: the prev/velocity ring has D + 1 slots (D = 3 or 7); the
-// variant EPI 4 has no such ring.
+// D rows ahead: the prev/velocity ring has D + 1 slots (D = 3 or 7).
 template <int NW, int D, int EPI = 0>
 constexpr size_t ws_smem_bytes() {
-  return ws_detail::Smem<NW * 32, EPI == 4 ? 0 : D + 1>::bytes;
+  return ws_detail::Smem<NW * 32, D + 1>::bytes;
 }
 
 // EPI: also run part of a.epi at the output points with the new values
 // before they are stored: 2 = source subtraction and imaging (source
-// back-step); 3 = next injection (receiver step).  EPI 4: the plain step
-// with the previous field and 1/vt read by the consumers from global memory
-// (each value is used once, at its output point; the loads are issued at
-// the start of the step so their latency overlaps the u2 work) instead of
-// staged in a shared-memory ring: 12 KB less shared memory per CTA, room
-// for a sixth CTA per SM.
+// back-step); 3 = next injection (receiver step).
 template <int ARITH, bool DAMPED, int NW, int D, int EPI = 0>
-__global__ void __launch_bounds__((NW + 1) * 32,
-                                  (EPI == 2 || EPI == 3) ? (ARITH == ARITH_REF ? 4 : 5) : (EPI == 4 ? 6 : 1))
+__global__ void __launch_bounds__((NW + 1) * 32, (EPI == 2 || EPI == 3) ? (ARITH == ARITH_REF ? 4 : 5) : 1)
 fd_step_ws(StreamArgs a) {
   using namespace ws_detail;
   constexpr int NT = NW * 32;      // consumer threads
-  constexpr bool GPV = EPI == 4;   // prev / 1/vt from global memory
   constexpr int NP = D + 1;
   static_assert(NP == 4 || NP == 8, "the prev/vel ring must divide the current ring");
-  constexpr int NPR = GPV ? 0 : NP;   // prev/vel ring rows allocated
-  using L = Smem<NT, NPR>;
+  using L = Smem<NT, NP>;
   constexpr int BZ = L::BZ, WC = L::WC, WP = L::WP, NC = L::NC;
   extern __shared__ __align__(128) unsigned char smem[];
   float(*cring)[WC] = reinterpret_cast<float(*)[WC]>(smem + L::c_off);
@@ -94,7 +85,7 @@ fd_step_ws(StreamArgs a) {
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::b_off);
   uint64_t *emptyc = full + NC;
   uint64_t *emptyp = emptyc + NC;
-  int *s_fail = reinterpret_cast<int *>(emptyp + NPR);
+  int *s_fail = reinterpret_cast<int *>(emptyp + NP);
 
   const int tid = threadIdx.x;
   const int shot = a.shot_major ? blockIdx.z : blockIdx.x;
@@ -112,7 +103,7 @@ fd_step_ws(StreamArgs a) {
       mbar_init(&full[i], 1);
       mbar_init(&emptyc[i], 1);
     }
-    for (int i = 0; i < NPR; i++) mbar_init(&emptyp[i], 1);
+    for (int i = 0; i < NP; i++) mbar_init(&emptyp[i], 1);
     fence_mbar_init();
     *s_fail = 0;
   }
@@ -134,10 +125,9 @@ fd_step_ws(StreamArgs a) {
         *(volatile int *)s_fail = 1;
         break;
       }
-      const bool pv = !GPV && k >= 12;
+      const bool pv = k >= 12;
       const int ps = (k - 12) & (NP - 1);
-      if (pv && k - 12 >= NP &&
-          !mbar_wait(&emptyp[ps & (NPR > 0 ? NPR - 1 : 0)], (uint32_t)((((k - 12) / NP) + 1) & 1))) {
+      if (pv && k - 12 >= NP && !mbar_wait(&emptyp[ps], (uint32_t)((((k - 12) / NP) + 1) & 1))) {
         atomicExch(a.err, 1);
         *(volatile int *)s_fail = 1;
         break;
@@ -145,12 +135,10 @@ fd_step_ws(StreamArgs a) {
       uint64_t *fb = &full[k & (NC - 1)];
       mbar_expect_tx(fb, cbytes + (pv ? 2u * pbytes : 0u));
       bulk_g2s(&cring[k & (NC - 1)][0], curr + (long long)(xa - 6 + k) * P, cbytes, fb);
-      if constexpr (!GPV) {
-        if (pv) {
-          long long off = (long long)(xa - 12 + k) * P;
-          bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
-          bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
-        }
+      if (pv) {
+        long long off = (long long)(xa - 12 + k) * P;
+        bulk_g2s(&pring[ps][0], prevw + off, pbytes, fb);
+        bulk_g2s(&vring[ps][0], rcpw + off, pbytes, fb);
       }
     }
     return;
@@ -237,17 +225,6 @@ fd_step_ws(StreamArgs a) {
     // fused imaging: this step's receiver field and image values, loaded
     // early so their latency overlaps the update
     float4 gimg = make_float4(0.f, 0.f, 0.f, 0.f), vimg = gimg;
-    float4 p4g = gimg, r4g = gimg;
-    if constexpr (GPV) {
-      // every outgroup lane's 4 depths lie inside the pitched row (halo and
-      // pad included), 16-byte aligned
-      if (has_out && outgroup) {
-        const long long row = (long long)(xa - 12 + k) * P + zg;
-        p4g = ld4g(a.prev + (long long)shot * a.shot_stride + row);
-        r4g = __ldg(reinterpret_cast<const float4 *>(
-            a.rcp + (long long)(shot / a.shots_per_vel) * a.vel_stride + row));
-      }
-    }
     if constexpr (EPI == 2 || EPI == 3) {
       if (EPI == 2 && a.epi.image && has_out && outgroup) {
         const long long o = (long long)shot * a.shot_stride + (long long)(xa - 12 + k) * P + zg;
@@ -308,11 +285,9 @@ fd_step_ws(StreamArgs a) {
     if (t == 0) {
       if (has_u2) mbar_arrive(&emptyc[cs(-10)]);
       // (stage 11 carries no prev/vel rows: the first release is at step 13)
-      if constexpr (!GPV) {
-        if (k >= 13) {
-          if constexpr (PH >= 0) mbar_arrive(&emptyp[(PH - 13) & (NP - 1)]);
-          else mbar_arrive(&emptyp[(k - 13) & (NP - 1)]);
-        }
+      if (k >= 13) {
+        if constexpr (PH >= 0) mbar_arrive(&emptyp[(PH - 13) & (NP - 1)]);
+        else mbar_arrive(&emptyp[(k - 13) & (NP - 1)]);
       }
     }
     if (has_out && outgroup) {
@@ -321,14 +296,8 @@ fd_step_ws(StreamArgs a) {
       const float *uc = &u2r[us(-1)][4 * t];
       const float *up = &u2r[us(0)][4 * t];
       float4 c4 = ld4(&cring[cs(-6)][8 + 4 * t]);
-      float4 p4, r4;
-      if constexpr (GPV) {
-        p4 = p4g;
-        r4 = r4g;
-      } else {
-        p4 = ld4(&pring[ps][4 * t]);
-        r4 = ld4(&vring[ps][4 * t]);
-      }
+      const float4 p4 = ld4(&pring[ps][4 * t]);
+      const float4 r4 = ld4(&vring[ps][4 * t]);
       float4 um4 = ld4(um), uc4 = ld4(uc), up4 = ld4(up);
       float ucl = uc[-1], ucr = uc[4];
       float o[4];

@@ -67,9 +67,8 @@ def test_fast_forward_within_tolerance(cuda, fdo):
     print(f"seismogram rel-L2 vs FP64: REF {rel_l2(g['dcal'][1], d64):.2e}  FAST {rel_l2(d.cpu().numpy(), d64):.2e}")
 
 
-@pytest.mark.parametrize("kern,bz,rows,depth", [(0, 248, 7, 5), (1, 376, 64, 3), (2, 360, 64, 3),
-                                                (2, 240, 9, 7), (3, 376, 64, 7), (3, 376, 31, 3),
-                                                (4, 376, 64, 3), (4, 248, 9, 7)])
+@pytest.mark.parametrize("kern,bz,rows,depth", [(1, 376, 64, 3), (1, 248, 9, 7), (5, 120, 48, 3),
+                                                (5, 120, 31, 7)])
 def test_fast_forward_every_kernel_within_tolerance(cuda, kern, bz, rows, depth):
     # FAST arithmetic in every stencil kernel: seismogram within 1e-5
     # relative L2 of the reference's
@@ -190,12 +189,8 @@ def test_errors_reported(cuda):
 
 
 @pytest.mark.parametrize("kern,bz,rows,depth,order", [
-    (0, 120, 1, 3, 1), (0, 248, 7, 5, 0), (0, 120, 64, 5, 0),
     (1, 120, 1, 3, 1), (1, 248, 9, 7, 0), (1, 376, 64, 7, 0), (1, 376, 3, 3, 1), (1, 120, 200, 7, 0),
     (1, 376, 16, 3, 0), (1, 248, 33, 3, 1),
-    (2, 240, 1, 3, 1), (2, 360, 64, 7, 0), (2, 480, 9, 3, 0), (2, 240, 33, 7, 0), (2, 360, 16, 3, 1),
-    (3, 376, 64, 7, 0), (3, 376, 33, 3, 0), (3, 248, 1, 7, 1), (3, 120, 2, 3, 0), (3, 376, 17, 7, 1),
-    (4, 376, 64, 3, 0), (4, 376, 33, 7, 0), (4, 248, 1, 3, 1), (4, 120, 2, 7, 0), (4, 376, 17, 3, 1),
     (5, 120, 1, 3, 0), (5, 120, 9, 7, 0), (5, 120, 64, 3, 0), (5, 120, 33, 7, 0), (5, 120, 200, 3, 0),
     (5, 120, 11, 3, 0), (5, 120, 12, 7, 0), (5, 120, 8, 3, 0), (5, 120, 16, 7, 0)])
 def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
@@ -209,9 +204,7 @@ def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     np.testing.assert_array_equal(d.cpu().numpy(), g["dcal"][2])
 
 
-@pytest.mark.parametrize("kern,bz,depth", [(0, 120, 5), (0, 248, 3), (1, 120, 7), (1, 248, 3), (1, 376, 3),
-                                           (1, 376, 7), (2, 240, 3), (2, 360, 7), (2, 480, 3), (3, 376, 7),
-                                           (3, 248, 3), (4, 376, 3), (4, 376, 7), (4, 248, 3),
+@pytest.mark.parametrize("kern,bz,depth", [(1, 120, 7), (1, 248, 3), (1, 376, 3), (1, 376, 7),
                                            (5, 120, 3), (5, 120, 7)])
 def test_stream_matches_reference_large_grid(cuda, ref, kern, bz, depth):
     # 921 x 301 (993 x 343 padded, pitch 344): several bands, a short last
