@@ -119,19 +119,25 @@ fd_step_rq(StreamArgs a, int nslots) {
 
   // lane 0 issues stage s into slot s % NC (current row) and s % NP
   // (previous field and 1/vt, from stage 12 on)
+  // Lanes 0..2 each issue one copy of a stage (called by the whole warp):
+  // lane 0 the current row and the barrier's arrival with the stage's byte
+  // count, lanes 1 and 2 the previous-field and 1/vt rows (from stage 12
+  // on).  A lane's source row pointer and ring base are fixed.
+  const float *my_src = lane == 0 ? src_c : (lane == 1 ? src_p : src_v);
+  const uint32_t my_ring = lane == 0 ? smem_u32(&S.c[0][0]) : (lane == 1 ? smem_u32(&S.p[0][0]) : smem_u32(&S.v[0][0]));
+  const uint32_t my_slot_bytes = lane == 0 ? 4u * WC : 4u * WP;
+  const uint32_t my_bytes = lane == 0 ? cbytes : pbytes;
   auto issue = [&](int s, int cs, int ps) {
-    uint64_t *fb = &S.full[cs];
-    const bool pv = s >= 12;
-    mbar_expect_tx(fb, cbytes + (pv ? 2u * pbytes : 0u));
-    const long long off = (long long)s * P;
-    bulk_g2s(&S.c[cs][0], src_c + off, cbytes, fb);
-    if (pv) {
-      bulk_g2s(&S.p[ps][0], src_p + off, pbytes, fb);
-      bulk_g2s(&S.v[ps][0], src_v + off, pbytes, fb);
+    if (lane < 3) {
+      const bool pv = s >= 12;
+      const uint32_t bar = smem_u32(&S.full[cs]);
+      if (lane == 0) mbar_expect_tx(&S.full[cs], cbytes + (pv ? 2u * pbytes : 0u));
+      if (lane == 0 || pv)
+        bulk_g2s_u32(my_ring + (uint32_t)(lane == 0 ? cs : ps) * my_slot_bytes, my_src + (long long)s * P, my_bytes,
+                     bar);
     }
   };
-  if (lane == 0)
-    for (int s = 0; s < D && s < K; s++) issue(s, s & (NC - 1), s & (NP - 1));
+  for (int s = 0; s < D && s < K; s++) issue(s, s & (NC - 1), s & (NP - 1));
 
   // ---- this lane's depths
   const int zg = zo - 4 + 4 * lane;
@@ -295,7 +301,7 @@ fd_step_rq(StreamArgs a, int nslots) {
     // before the refill is issued, as in a release through an "empty"
     // barrier.
     __syncwarp();
-    if (lane == 0 && k + D < K) issue(k + D, (U + D) % NC, (U + D) % NP);
+    if (k + D < K) issue(k + D, (U + D) % NC, (U + D) % NP);
     return true;
   };
 
