@@ -122,11 +122,11 @@ int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, i
  * in place of the separate source, residual and image launches.  Results
  * are bit-identical either way. */
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on);
-/* CUDA graphs for the forward and backward time loops (default on): from a
- * loop's second use, while a step covers at most 8e6 points (fields x
- * nxpad x nzpad) and stencil timing is off, the loop is captured on a
- * private stream and replayed on the propagator's stream.  Same kernels,
- * same results. */
+/* CUDA graphs for the forward and backward time loops: on = 0 never, 1
+ * (default) while a step covers at most 8e6 points (fields x nxpad x
+ * nzpad), 2 for every step size.  From a loop's second use, and while
+ * stencil timing is off, the loop is captured on a private stream and
+ * replayed on the propagator's stream.  Same kernels, same results. */
 int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on);
 /* Per-shot receiver lists (uneven spreads; not in the reference, whose
  * ShotPosition is one common line): shot s has receivers
@@ -325,12 +325,15 @@ int swfwi_fwi_last_trials(const swfwi_fwi *h, int *trials);
 /* ------------------------------------------------------------------------
  * Measurement (no counterpart in the reference, which prints wall-clock
  * timers only, src/common/timer.h:14-29).  Process-wide counters of kernel
- * launches and, when enabled, CUDA-event timing of every stencil launch on
- * its own stream with its algorithmic work (interior point-updates; bytes =
- * 12 per point-update plus 4 per point per velocity model read).
+ * launches and, when enabled, every stencil launch's algorithmic work
+ * (interior point-updates; bytes = 12 per point-update plus 4 per point per
+ * velocity model read) with CUDA-event timing, on the launch's own stream,
+ * of every on-th stencil launch (on = 1: all of them).
  * kernel_launches counts launches issued from the host: a time loop replayed
  * as a CUDA graph (swfwi_damp4t10d_set_graphs) is counted when captured, not
  * again per replay; stencil timing turns the replay off.
+ * step_ms is the timed launches' total: their mean is step_ms /
+ * step_timed_launches.
  * ---------------------------------------------------------------------- */
 typedef struct {
   long long kernel_launches;
@@ -338,8 +341,10 @@ typedef struct {
   double step_ms;
   double step_point_updates;
   double step_bytes;
+  long long step_timed_launches;
 } swfwi_stats;
 int swfwi_stats_reset(void);
+/* on = 0: off; on >= 1: count every stencil launch, time every on-th. */
 int swfwi_stats_enable_step_timing(int on);
 /* waits for the timed launches to finish */
 int swfwi_stats_read(swfwi_stats *out);

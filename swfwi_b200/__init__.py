@@ -37,7 +37,8 @@ class SwfwiError(RuntimeError):
 
 class Stats(C.Structure):
     _fields_ = [("kernel_launches", C.c_longlong), ("step_launches", C.c_longlong),
-                ("step_ms", C.c_double), ("step_point_updates", C.c_double), ("step_bytes", C.c_double)]
+                ("step_ms", C.c_double), ("step_point_updates", C.c_double), ("step_bytes", C.c_double),
+                ("step_timed_launches", C.c_longlong)]
 
 
 class _ShotPos(C.Structure):
@@ -247,7 +248,9 @@ def stats_reset() -> None:
     _check(lib().swfwi_stats_reset())
 
 
-def stats_enable_step_timing(on: bool = True) -> None:
+def stats_enable_step_timing(on=True) -> None:
+    """False/0: off; True/1: count every stencil launch and time each;
+    n >= 2: count every launch, time every n-th."""
     _check(lib().swfwi_stats_enable_step_timing(int(on)))
 
 
@@ -503,9 +506,10 @@ class Damp4t10d:
         source back-step, residual injection in the receiver step)."""
         _check(lib().swfwi_damp4t10d_set_fusion(self.h, int(bool(on))))
 
-    def set_graphs(self, on: bool):
-        """CUDA graphs for the forward/backward time loops of small steps."""
-        _check(lib().swfwi_damp4t10d_set_graphs(self.h, int(bool(on))))
+    def set_graphs(self, on):
+        """CUDA graphs for the forward/backward time loops: False/0 never,
+        True/1 for small (launch-bound) steps, 2 for every step size."""
+        _check(lib().swfwi_damp4t10d_set_graphs(self.h, int(on)))
 
     def set_strip_format(self, fmt: int):
         """Boundary strips of the gradients: STRIP_F32 (exact), STRIP_F16 or

@@ -2,10 +2,9 @@
 
 The streaming step (``stream.cuh``) has knobs that do not change its
 results: which kernel (register-queue warps, each a self-contained TMA
-pipeline; warp-specialised with a copy warp, with two rows per step, or
-with the previous field read from global memory; independent consumer
-warps), output depths per CTA, rows per task, rows in flight ahead of the
-compute and the launch order (shots slowest or fastest).  ``tune`` times short batched forward runs of a survey for each
+pipeline; or warp-specialised CTAs with a copy warp), output depths per
+CTA, rows per task, rows in flight ahead of the compute and the launch
+order (shots slowest or fastest).  ``tune`` times short batched forward runs of a survey for each
 candidate with the library's CUDA-event step timing and returns the fastest;
 ``apply`` sets it on a propagator.
 """
@@ -21,26 +20,25 @@ DEFAULT = {"kernel": 5, "band_depth": 120, "rows_per_cta": 48, "rows_in_flight":
 
 def candidates(nz: int):
     """The register-queue kernel's task lengths and prefetch depths, the
-    warp-specialised kernel's band depths, chunk lengths and prefetch
-    depths."""
+    warp-specialised kernel's band depths, chunk lengths, prefetch depths
+    and launch orders."""
     for rows, depth in itertools.product((24, 32, 48, 64), (3, 7)):
         yield {"kernel": 5, "band_depth": 120, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": False}
-    for bz, rows, depth, order in itertools.product((120, 248, 376), (48, 64, 128), (3, 7), (False, True)):
+    for bz, rows, depth, order in itertools.product((248, 376), (48, 64), (3, 7), (False, True)):
         yield {"kernel": 1, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": order}
-    for bz, rows, depth in itertools.product((248, 376), (48, 64, 128), (3, 7)):
-        yield {"kernel": 4, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
-               "shots_slowest": False}
-    for bz, rows, depth in itertools.product((248, 376), (48, 64, 128), (3, 7)):
-        yield {"kernel": 3, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
-               "shots_slowest": False}
-    for bz, rows, depth in itertools.product((240, 360, 480), (48, 64, 128), (3, 7)):
-        yield {"kernel": 2, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": depth,
-               "shots_slowest": False}
-    for bz, rows in itertools.product((120, 248), (64, 128)):
-        yield {"kernel": 0, "band_depth": bz, "rows_per_cta": rows, "rows_in_flight": 3,
-               "shots_slowest": False}
+
+
+def valid(cfg: dict) -> bool:
+    """The launch shapes swfwi_damp4t10d_set_tuning accepts."""
+    if cfg["kernel"] == 5:
+        ok_bz = cfg["band_depth"] == 120
+    elif cfg["kernel"] == 1:
+        ok_bz = cfg["band_depth"] in (120, 248, 376)
+    else:
+        return False
+    return ok_bz and cfg["rows_in_flight"] in (3, 7) and cfg["rows_per_cta"] >= 1
 
 
 def time_config(method, wlt, dcal, ids, cfg, repeats=2) -> float:

@@ -14,8 +14,17 @@ std::string last_error() { return g_last_error; }
 
 using namespace swfwi;
 
+// The handle: the propagator, and the device buffers and copy stream of the
+// host-buffer gradient (kept between calls, grown on demand).
 struct swfwi_damp4t10d {
   std::unique_ptr<Propagator> p;
+  DevBuf<float> hv, hw, hd, hg;
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copied = nullptr;
+  ~swfwi_damp4t10d() {
+    if (copied) cudaEventDestroy(copied);
+    if (copy) cudaStreamDestroy(copy);
+  }
 };
 
 struct swfwi_fwi {
@@ -199,7 +208,10 @@ int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on) {
 }
 
 int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on) {
-  return guarded([&] { P(h).graphs = on != 0; });
+  return guarded([&] {
+    SWFWI_REQUIRE(on >= 0 && on <= 2, "graph mode must be 0, 1 or 2");
+    P(h).graphs = on;
+  });
 }
 
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
@@ -422,24 +434,39 @@ int swfwi_gradient_host(swfwi_damp4t10d *h, const float *exvel, const float *wlt
     SWFWI_REQUIRE(p.nxpad > 0, "model size unknown");
     cudaStream_t st = p.stream();
     long long np = (long long)p.nxpad * p.nzpad, dn = (long long)p.nt * p.ngmax;
-    DevBuf<float> v, w, d, g;
-    v.upload(exvel, np, st);
-    w.upload(wlt, p.nt, st);
-    d.upload(dobs, (size_t)nshots * dn, st);
-    g.resize(np);
     // the host data hold only the listed shots: address them as 0..n-1
     std::vector<int> local(nshots);
     for (int i = 0; i < nshots; i++) {
       SWFWI_REQUIRE(shot_ids[i] >= 0 && shot_ids[i] < p.ns, "shot id out of range");
       local[i] = i;
     }
+    if (!h->copy) {
+      SWFWI_CUDA(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking));
+      SWFWI_CUDA(cudaEventCreateWithFlags(&h->copied, cudaEventDisableTiming));
+    }
+    h->hv.upload(exvel, np, st);
+    h->hw.upload(wlt, p.nt, st);
+    h->hd.resize((size_t)nshots * dn);
+    h->hg.resize(np);
+    // the observed data are first read by the residual, after the forward
+    // sweep: upload them on the copy stream meanwhile
+    const size_t dbytes = sizeof(float) * (size_t)nshots * dn;
+    std::function<void()> upload = [&] {
+      SWFWI_CUDA(cudaStreamWaitEvent(h->copy, h->copied, 0));   // the previous call's reads are done
+      SWFWI_CUDA(cudaMemcpyAsync(h->hd.get(), dobs, dbytes, cudaMemcpyHostToDevice, h->copy));
+      SWFWI_CUDA(cudaEventRecord(h->copied, h->copy));
+      SWFWI_CUDA(cudaStreamWaitEvent(st, h->copied, 0));
+    };
     const float *old = p.velocity();
-    p.bind_velocity(v.get());
+    p.bind_velocity(h->hv.get());
     // slot i models shot_ids[i]; its observed data sit at row i
-    p.gradient_batch(w.get(), d.get(), shot_ids, nshots, g.get(), obj, false, local.data());
-    SWFWI_CUDA(cudaMemcpyAsync(grad, g.get(), sizeof(float) * np, cudaMemcpyDeviceToHost, st));
+    p.gradient_batch(h->hw.get(), h->hd.get(), shot_ids, nshots, h->hg.get(), obj, false, local.data(),
+                     &upload);
+    SWFWI_CUDA(cudaEventRecord(h->copied, st));
+    SWFWI_CUDA(cudaMemcpyAsync(grad, h->hg.get(), sizeof(float) * np, cudaMemcpyDeviceToHost, st));
     SWFWI_CUDA(cudaStreamSynchronize(st));
     if (old) p.bind_velocity(old);
+    else p.unbind_velocity(h->hv.get());
   });
 }
 
@@ -633,20 +660,25 @@ int swfwi_stats_reset(void) {
 }
 
 int swfwi_stats_enable_step_timing(int on) {
-  return guarded([&] { step_timer().enabled.store(on != 0); });
+  return guarded([&] {
+    SWFWI_REQUIRE(on >= 0, "timing period must be >= 0");
+    step_timer().period.store(on > 0 ? on : 1);
+    step_timer().enabled.store(on != 0);
+  });
 }
 
 int swfwi_stats_read(swfwi_stats *out) {
   return guarded([&] {
     SWFWI_REQUIRE(out, "null output");
     double ms = 0, pts = 0, b = 0;
-    long long n = 0;
-    step_timer().read(ms, n, pts, b);
+    long long n = 0, timed = 0;
+    step_timer().read(ms, n, pts, b, timed);
     out->kernel_launches = g_kernel_launches.load();
     out->step_launches = n;
     out->step_ms = ms;
     out->step_point_updates = pts;
     out->step_bytes = b;
+    out->step_timed_launches = timed;
   });
 }
 

@@ -28,7 +28,7 @@ void StepTimer::reset() {
   g_kernel_launches.store(0);
 }
 
-void StepTimer::read(double &ms, long long &n, double &pts, double &b) {
+void StepTimer::read(double &ms, long long &n, double &pts, double &b, long long &timed) {
   std::lock_guard<std::mutex> g(mu);
   ms = 0;
   for (size_t i = 0; i < used; i++) {
@@ -40,6 +40,7 @@ void StepTimer::read(double &ms, long long &n, double &pts, double &b) {
   n = launches;
   pts = points;
   b = bytes;
+  timed = (long long)used;
 }
 
 // Algorithmic work of one step launch: every interior point of every field
@@ -48,6 +49,11 @@ void StepTimer::read(double &ms, long long &n, double &pts, double &b) {
 cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el) {
   if (!enabled.load(std::memory_order_relaxed)) return nullptr;
   std::lock_guard<std::mutex> g(mu);
+  const long long k = launches++;
+  points += pts * n;
+  bytes += pts * n * 3 * el + pts * el * nvel;
+  const int per = std::max(period.load(std::memory_order_relaxed), 1);
+  if (k % per != 0) return nullptr;
   if (used == pool.size()) {
     cudaEvent_t x, y;
     SWFWI_CUDA(cudaEventCreate(&x));
@@ -55,9 +61,6 @@ cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el
     pool.emplace_back(x, y);
   }
   auto ev = pool[used++];
-  launches++;
-  points += pts * n;
-  bytes += pts * n * 3 * el + pts * el * nvel;
   SWFWI_CUDA(cudaEventRecord(ev.first, st));
   return ev.second;
 }
@@ -118,7 +121,7 @@ void Propagator::loop_key_common(std::vector<long long> &k) const {
 
 template <typename F>
 void Propagator::run_loop(int which, double points_per_step, const std::vector<long long> &key, F &&body) {
-  const bool use = graphs && loop_warm_[which] && points_per_step <= kGraphMaxPoints &&
+  const bool use = graphs > 0 && loop_warm_[which] && (graphs == 2 || points_per_step <= kGraphMaxPoints) &&
                    !step_timer().enabled.load(std::memory_order_relaxed);
   loop_warm_[which] = true;
   if (!use) {
@@ -810,7 +813,8 @@ void Propagator::forward_batch(const float *wlt, float *dcal, const int *ids, in
 }
 
 void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *ids, int n,
-                                float *grad, double *obj, bool accumulate, const int *rows) {
+                                float *grad, double *obj, bool accumulate, const int *rows,
+                                const std::function<void()> *before_residual) {
   SWFWI_REQUIRE(wlt && dobs && ids && grad && n > 0, "bad batch arguments");
   for (int i = 0; i < n; i++) SWFWI_REQUIRE(ids[i] >= 0 && ids[i] < ns, "shot id out of range");
   const float *rcp = rcp_of(vel_);
@@ -840,6 +844,7 @@ void Propagator::gradient_batch(const float *wlt, const float *dobs, const int *
     run_forward<float>(w_, k, src, wlt, 1, 0, 0, rec, ngmax, w_.dcal.get(), true, rcp);
     launch_mute_windows(w_.win.get(), vel_, nxpad, nzpad, d_src_x_.get(), d_src_z_.get(),
                         d_rec_x_.get(), d_rec_z_.get(), ngmax, ngmax, ss, half_len, nt, k, st_);
+    if (before_residual && c0 == 0) (*before_residual)();
     launch_muted_residual(w_.res.get(), dobs, dn, rr, w_.dcal.get(), w_.win.get(), w_.win.get(), nt,
                           ngmax, k, st_);
     launch_sumsq_f64(w_.obj.get(), w_.res.get(), dn, k, w_.partials.get(), kPartials, st_);

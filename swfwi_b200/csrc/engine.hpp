@@ -10,6 +10,7 @@
 // [nxpad][nzpad] layout.
 #pragma once
 #include <atomic>
+#include <functional>
 #include <mutex>
 #include <vector>
 #include "common.hpp"
@@ -18,16 +19,19 @@
 namespace swfwi {
 
 // Process-wide timing of stencil launches (CUDA events on the launching
-// stream) and their algorithmic work, read by benchmarks.
+// stream) and their algorithmic work, read by benchmarks.  While enabled,
+// every launch's work is counted and every period-th launch is timed.
 struct StepTimer {
   std::atomic<bool> enabled{false};
+  std::atomic<int> period{1};
   std::mutex mu;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
   size_t used = 0;
   long long launches = 0;
   double points = 0, bytes = 0;
   void reset();
-  void read(double &ms, long long &n, double &pts, double &b);
+  // ms: the timed launches' total; n: launches counted; timed: launches timed
+  void read(double &ms, long long &n, double &pts, double &b, long long &timed);
   // Opens the timing of one launch over n fields of pts interior points
   // reading nvel velocity models, el bytes an element; returns the event to
   // record after the launch (null when timing is off).
@@ -84,10 +88,11 @@ class Propagator {
   // steps (the caller zeroes it).
   float *illum = nullptr;
   int illum_every = 4;
-  // CUDA graphs for the time loops of the forward and backward sweeps when
-  // a step is small enough to be launch-bound (n fields x nxpad x nzpad at
-  // most kGraphMaxPoints); never while stencil launches are being timed.
-  bool graphs = true;
+  // CUDA graphs for the time loops of the forward and backward sweeps:
+  // 0 never, 1 when a step is small enough to be launch-bound (n fields x
+  // nxpad x nzpad at most kGraphMaxPoints), 2 for every step size; never
+  // while stencil launches are being timed.
+  int graphs = 1;
   static constexpr double kGraphMaxPoints = 8e6;
 
   void set_receivers_per_shot(const int *offsets, const int *gx, const int *gz);
@@ -131,8 +136,12 @@ class Propagator {
   // Gradient loop of FwiFramework::epoch for the listed shots; grad
   // overwritten (or accumulated); obj[n] host.  rows (host, optional): the
   // dobs row of each listed shot (default: the shot id).
+  // before_residual (optional) runs on the host after each batch's forward
+  // sweep is enqueued and before its residual is (a caller's upload of the
+  // observed data can overlap the sweep).
   void gradient_batch(const float *wlt, const float *dobs, const int *ids, int n, float *grad,
-                      double *obj, bool accumulate = false, const int *rows = nullptr);
+                      double *obj, bool accumulate = false, const int *rows = nullptr,
+                      const std::function<void()> *before_residual = nullptr);
   // Trial objective: sum over listed shots of |mute(obs) - mute(cal(vel))|^2,
   // the observed data muted with the bound velocity (host result).
   double trial_objective_fwi(const float *wlt, const float *dobs, const int *ids, int n,

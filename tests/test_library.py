@@ -128,3 +128,12 @@ def test_header_is_c99_and_links(tmp_path):
     run = subprocess.run([str(exe)], capture_output=True, text=True)
     assert run.returncode == 0, (run.stdout, run.stderr)
     assert "bad argument" in run.stdout
+
+
+def test_autotune_candidates_are_accepted_shapes():
+    # every launch shape the tuner tries is one the C ABI accepts, and the
+    # default is among them
+    from swfwi_b200 import autotune
+    cands = list(autotune.candidates(343))
+    assert cands and all(autotune.valid(c) for c in cands)
+    assert autotune.DEFAULT in cands
