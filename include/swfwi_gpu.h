@@ -309,6 +309,38 @@ int swfwi_fwi_set_regularization(swfwi_fwi *h, float lx, float lz);
 int swfwi_regu_term(const float *vel, int nx, int nz, float lx, float lz, double *term, void *stream);
 int swfwi_regu_gradient(const float *vel, int nx, int nz, float lx, float lz, float *grad, int accumulate,
                         void *stream);
+
+/* ------------------------------------------------------------------------
+ * The prestack LSRTM linear operator (src/unused/prtm2d.cpp; the reference
+ * never built it: its prtm2d.h is missing).  One handle is one prtm2d_init
+ * (:241-338): second-order-time, fourth-order-space propagator with a
+ * Gaussian sponge of nb cells on every side, Ricker source of peak
+ * frequency fm and amplitude amp, shots at (sxbeg + is jsx, szbeg + is jsz),
+ * receivers at (gxbeg + ig jgx, gzbeg + ig jgz), moved with each shot when
+ * csdgather = 1 (common-shot gathers).  vel: DEVICE [nx][nz] in m/s.  Every
+ * shot and receiver must lie in the model (the reference checks the first
+ * and last and exits; here SWFWI_ERR_BAD_ARG).
+ * arith SWFWI_ARITH_REF: bit-identical to the compiled prtm2d.cpp, shots
+ * in order, the receiver-side fields carried between shots and calls as
+ * the reference's Born branch leaves them (it never clears them, :408-434).
+ * SWFWI_ARITH_FAST: FP32 with FMA, shots batched, every shot from zero.
+ * ---------------------------------------------------------------------- */
+typedef struct swfwi_prtm swfwi_prtm;
+/* migration: the reference's (:371-407; not the adjoint of its Born
+ * branch: <Lm, d> != <m, L'd>), or the exact transpose of the Born branch */
+enum { SWFWI_PRTM_ADJ_REFERENCE = 0, SWFWI_PRTM_ADJ_EXACT = 1 };
+int swfwi_prtm2d_create(swfwi_prtm **out, int arith, float dz, float dx, float dt, float amp, float fm, int nz,
+                        int nx, int nb, int nt, int ns, int ng, int sxbeg, int szbeg, int jsx, int jsz, int gxbeg,
+                        int gzbeg, int jgx, int jgz, int csdgather, const float *vel, void *stream);
+int swfwi_prtm2d_set_adjoint(swfwi_prtm *h, int mode);
+/* shots one launch sequence carries (1 for REF) */
+int swfwi_prtm2d_batch(swfwi_prtm *h, int *shots);
+/* prtm2d_lop (:354-437): adj = 0: dat += L mod (Born); adj = 1: mod += L'
+ * dat; add = 0 zeroes the output first (sf_adjnull).  nm = nx nz, nd = nt
+ * ng ns; mod DEVICE [nx][nz], dat DEVICE [ns][ng][nt].  Asynchronous on
+ * stream. */
+int swfwi_prtm2d_lop(swfwi_prtm *h, int adj, int add, int nm, int nd, float *mod, float *dat, void *stream);
+int swfwi_prtm2d_destroy(swfwi_prtm *h);
 /* Failure-detection self-test: one thread waits, with the stencil kernels'
  * bounded mbarrier wait (about 2^31 cycles, a second), on a barrier nothing
  * arrives at; the wait gives up, raises the error flag, and the call returns

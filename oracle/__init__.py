@@ -1,6 +1,6 @@
 """The oracle: test infrastructure only.
 
-Two CPU checkers for swfwi's acoustic FWI path, loaded with ctypes:
+CPU checkers for swfwi's acoustic FWI path, loaded with ctypes:
 
 * ``RefLib`` wraps ``oracle/_ref/libswfwi_ref.so``: the reference's own C/C++
   sources (src/modeling, src/common, src/essfwi, src/fwi) compiled in place
@@ -8,6 +8,8 @@ Two CPU checkers for swfwi's acoustic FWI path, loaded with ctypes:
 * ``FdOracle`` wraps ``oracle/_ref/libfd_oracle.so``: a plain-C restatement of
   the stencil (reference arithmetic and FP64) and an FP64 restatement of the
   per-shot forward modelling and gradient (``oracle/fd_oracle.c``).
+* ``PrtmRef`` wraps ``oracle/_ref/libprtm_ref.so``: the reference's LSRTM
+  operator (src/unused/prtm2d.cpp) compiled in place by ``harness_prtm.cpp``.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg may import this package, and only as the checker or the timed CPU
@@ -346,3 +348,41 @@ class FdOracle:
                                   dptr(np.ascontiguousarray(wlt, np.float64)), int(src_pos), iptr(rec), rec.size,
                                   dptr(np.ascontiguousarray(vsrc, np.float64)), dptr(g))
         return g
+
+
+class PrtmRef:
+    """The reference's LSRTM operator (src/unused/prtm2d.cpp, compiled in
+    place into ``oracle/_ref/libprtm_ref.so`` by ``harness_prtm.cpp``).  The
+    operator lives in file-scope variables, so one object at a time: the
+    constructor is prtm2d_init (receiver-side fields cleared, which the
+    reference leaves to malloc), ``close`` is prtm2d_close."""
+
+    _open = False
+
+    def __init__(self, vel, dz, dx, dt, amp, fm, nb, nt, ns, ng, sxbeg, szbeg, jsx, jsz, gxbeg, gzbeg, jgx, jgz,
+                 csdgather=False):
+        if PrtmRef._open:
+            raise RuntimeError("the reference operator is a single instance: close the open one first")
+        self.lib = C.CDLL(os.path.join(REF_DIR, "libprtm_ref.so"))
+        L = self.lib
+        L.ref_prtm_init.argtypes = [C.c_int] + [C.c_float] * 5 + [C.c_int] * 14 + [_fp]
+        L.ref_prtm_lop.argtypes = [C.c_int] * 4 + [_fp, _fp]
+        vel = np.ascontiguousarray(vel, np.float32)
+        self.nx, self.nz = vel.shape
+        self.nt, self.ns, self.ng = nt, ns, ng
+        L.ref_prtm_init(int(csdgather), dz, dx, dt, amp, fm, self.nz, self.nx, nb, nt, ns, ng, sxbeg, szbeg, jsx, jsz,
+                        gxbeg, gzbeg, jgx, jgz, fptr(vel))
+        PrtmRef._open = True
+
+    def lop(self, adj, add, mod, dat):
+        """prtm2d_lop in place on float32 arrays mod [nx][nz], dat [ns][ng][nt]"""
+        self.lib.ref_prtm_lop(int(bool(adj)), int(bool(add)), mod.size, dat.size, fptr(mod), fptr(dat))
+
+    def clear(self):
+        """zero the receiver-side fields (a per-shot operator's start)"""
+        self.lib.ref_prtm_clear()
+
+    def close(self):
+        if PrtmRef._open:
+            self.lib.ref_prtm_close()
+            PrtmRef._open = False

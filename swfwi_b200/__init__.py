@@ -147,6 +147,11 @@ _SIGS = {
     "swfwi_fwi_set_regularization": [_vp, C.c_float, C.c_float],
     "swfwi_regu_term": [_vp, C.c_int, C.c_int, C.c_float, C.c_float, _dp, _vp],
     "swfwi_regu_gradient": [_vp, C.c_int, C.c_int, C.c_float, C.c_float, _vp, C.c_int, _vp],
+    "swfwi_prtm2d_create": [C.POINTER(_vp), C.c_int] + [C.c_float] * 5 + [C.c_int] * 15 + [_vp, _vp],
+    "swfwi_prtm2d_set_adjoint": [_vp, C.c_int],
+    "swfwi_prtm2d_batch": [_vp, _ip],
+    "swfwi_prtm2d_lop": [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp],
+    "swfwi_prtm2d_destroy": [_vp],
     "swfwi_fwi_set_learned_min_decrease": [_vp, C.c_float],
     "swfwi_fwi_set_learned_patience": [_vp, C.c_int],
     "swfwi_fwi_get_gradient": [_vp, _fp],
@@ -425,6 +430,62 @@ def regu_gradient(vel, lx: float, lz: float, grad, accumulate: bool = False, str
     """ReguFactor::getReguGradient (:67-108) into (or added to) grad."""
     nx, nz = vel.shape
     _check(lib().swfwi_regu_gradient(_ptr(vel), nx, nz, lx, lz, _ptr(grad), int(accumulate), _stream(stream)))
+
+
+PRTM_ADJ_REFERENCE, PRTM_ADJ_EXACT = 0, 1
+
+
+class Prtm2d:
+    """The prestack LSRTM linear operator of src/unused/prtm2d.cpp on the GPU:
+    the constructor is prtm2d_init (:241-338) with the velocity ``vel`` a
+    CUDA [nx][nz] tensor (m/s), ``lop`` is prtm2d_lop (:354-437), ``close``
+    prtm2d_close.  Unlike the reference's file-scope state, each object is
+    its own operator.
+
+    ``arith=ARITH_REF`` is bit-identical to the compiled reference (shots in
+    order; the Born branch continues from the receiver-side fields the
+    previous shot or call left, as the reference's does); ``ARITH_FAST``
+    batches the shots in FP32 with FMA, every shot starting from zero.
+    ``set_adjoint(PRTM_ADJ_EXACT)`` makes ``lop(adj=True)`` the exact
+    transpose of the Born branch instead of the reference's migration, which
+    is not its adjoint."""
+
+    def __init__(self, vel, dz: float, dx: float, dt: float, amp: float, fm: float, nb: int, nt: int, ns: int,
+                 ng: int, sxbeg: int, szbeg: int, jsx: int, jsz: int, gxbeg: int, gzbeg: int, jgx: int, jgz: int,
+                 csdgather: bool = False, arith: int = ARITH_REF, stream=None):
+        self.h = None
+        nx, nz = vel.shape
+        self.nx, self.nz, self.nt, self.ns, self.ng = nx, nz, nt, ns, ng
+        h = _vp()
+        _check(lib().swfwi_prtm2d_create(C.byref(h), arith, dz, dx, dt, amp, fm, nz, nx, nb, nt, ns, ng, sxbeg,
+                                         szbeg, jsx, jsz, gxbeg, gzbeg, jgx, jgz, int(csdgather), _ptr(vel),
+                                         _stream(stream)))
+        self.h = h
+
+    def set_adjoint(self, mode: int) -> None:
+        _check(lib().swfwi_prtm2d_set_adjoint(self.h, mode))
+
+    def batch(self) -> int:
+        out = C.c_int()
+        _check(lib().swfwi_prtm2d_batch(self.h, C.byref(out)))
+        return out.value
+
+    def lop(self, adj: bool, add: bool, mod, dat, stream=None) -> None:
+        """adj False: dat (+)= L mod; adj True: mod (+)= L' dat.  mod CUDA
+        float32 [nx][nz], dat CUDA float32 [ns][ng][nt]."""
+        _check(lib().swfwi_prtm2d_lop(self.h, int(bool(adj)), int(bool(add)), mod.numel(), dat.numel(),
+                                      _ptr(mod), _ptr(dat), _stream(stream)))
+
+    def close(self) -> None:
+        if self.h is not None:
+            _check(lib().swfwi_prtm2d_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def cal_objective_static(r, out, stream=None) -> None:

@@ -14,7 +14,9 @@ reproduced here:
   * src/tool/main-test.cpp:37-60 - the parabolaVertex triple.
 Plus small end-to-end cases on a seeded 50 x 40 survey: forward modelling,
 direct-arrival mute, the time derivative, per-shot and encoded gradients,
-the per-shot gradient loop, and two epochs of plain and encoded FWI.
+the per-shot gradient loop, and two epochs of plain and encoded FWI; the
+regularisation factor (``--regu``) and the LSRTM operator (``--prtm``,
+src/unused/prtm2d.cpp) on seeded inputs.
 """
 from __future__ import annotations
 
@@ -154,9 +156,51 @@ def regu_fixture(R=None):
                         grad_ragged=g2, lx_ragged=np.float32(1.5), lz_ragged=np.float32(0.25))
 
 
+PRTM_CASES = {
+    # one line of surface shots, receivers every other cell
+    "line": dict(nx=48, nz=36, dz=10.0, dx=10.0, dt=1e-3, amp=1.0, fm=20.0, nb=10, nt=160, ns=3, ng=23,
+                 sxbeg=6, szbeg=2, jsx=16, jsz=0, gxbeg=2, gzbeg=1, jgx=2, jgz=0, csdgather=0),
+    # common-shot gathers along a slanted shot line, all receivers of a shot
+    # in one cell, the thinnest sponge the scheme allows
+    "gather": dict(nx=33, nz=29, dz=8.0, dx=12.0, dt=8e-4, amp=2.0, fm=25.0, nb=2, nt=120, ns=2, ng=5,
+                   sxbeg=20, szbeg=3, jsx=4, jsz=2, gxbeg=10, gzbeg=24, jgx=0, jgz=0, csdgather=1),
+}
+
+
+def prtm_fixture():
+    """The reference's LSRTM operator (src/unused/prtm2d.cpp, compiled in
+    place) on seeded inputs: two Born calls on one operator (the second
+    continues from the receiver fields the first left), the migration of
+    seeded data, and the migration added onto a seeded model."""
+    out = {}
+    for name, c in PRTM_CASES.items():
+        rng = np.random.default_rng(sum(map(ord, name)))
+        nx, nz = c["nx"], c["nz"]
+        vel = rng.uniform(1800.0, 2600.0, (nx, nz)).astype(np.float32)
+        mod = rng.standard_normal((nx, nz)).astype(np.float32)
+        dat = rng.standard_normal((c["ns"], c["ng"], c["nt"])).astype(np.float32)
+        base = rng.standard_normal((nx, nz)).astype(np.float32)
+        kw = {k: v for k, v in c.items() if k not in ("nx", "nz")}
+        op = oracle.PrtmRef(vel, **kw)
+        b1 = np.zeros_like(dat)
+        op.lop(0, 0, mod, b1)
+        b2 = np.zeros_like(dat)
+        op.lop(0, 0, mod, b2)
+        m1 = np.zeros_like(mod)
+        op.lop(1, 0, m1, dat)
+        m2 = base.copy()
+        op.lop(1, 1, m2, dat)
+        op.close()
+        out.update({f"{name}_vel": vel, f"{name}_mod": mod, f"{name}_dat": dat, f"{name}_base": base,
+                    f"{name}_born1": b1, f"{name}_born2": b2, f"{name}_mig": m1, f"{name}_mig_add": m2})
+    np.savez_compressed(os.path.join(HERE, "prtm.npz"), **out)
+
+
 if __name__ == "__main__":
     import sys
     if "--regu" in sys.argv:
         regu_fixture()
+    elif "--prtm" in sys.argv:
+        prtm_fixture()
     else:
         main()
