@@ -506,6 +506,60 @@ def record_enkf(torch, arith, tuning, cpu, members=64):
     return rec
 
 
+def record_lsrtm(torch, cpu=True):
+    """The LSRTM operator (src/unused/prtm2d.cpp) on the plain-FWI survey
+    (151 x 461, 25 m, dt 2 ms, nt 2000, 20 shots, 461 receivers, 30-cell
+    sponge) with a layered model: Born modelling and migration (the
+    reference's, and the exact transpose of Born) in FAST arithmetic, all
+    shots in one batch.  Work unit: grid-point updates of the padded fields
+    (Born: source and scattered field, 2 per point per step; migration: the
+    source field forward, then its reconstruction and the receiver field, 3
+    per point per step).  Parity: the dot-product test of Born and its exact
+    transpose on this survey."""
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    s = sv.config("fwi")
+    vt = sv.layered_model(s.nx, s.nz, seed=2024)
+    vel = torch.from_numpy(np.ascontiguousarray(vt)).cuda()
+    kw = dict(dz=s.dx, dx=s.dx, dt=s.dt, amp=1.0, fm=s.fm, nb=s.nb, nt=s.nt, ng=s.ng, sxbeg=s.sxbeg, szbeg=1,
+              jsx=s.jsx, jsz=0, gxbeg=0, gzbeg=1, jgx=1, jgz=0)
+    op = S.Prtm2d(vel, ns=s.ns, arith=S.ARITH_FAST, **kw)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    mod = torch.randn((s.nx, s.nz), device="cuda", generator=g)
+    dat = torch.randn((s.ns, s.ng, s.nt), device="cuda", generator=g)
+    born = torch.empty_like(dat)
+    img = torch.empty_like(mod)
+    op.lop(False, False, mod, born)                        # warm-up
+    t_born, _ = _timed(torch, lambda: op.lop(False, False, mod, born))
+    t_mig, _ = _timed(torch, lambda: op.lop(True, False, img, dat))
+    op.set_adjoint(S.PRTM_ADJ_EXACT)
+    t_adj, _ = _timed(torch, lambda: op.lop(True, False, img, dat))
+    a = float(torch.dot(born.double().ravel(), dat.double().ravel()))
+    b = float(torch.dot(mod.double().ravel(), img.double().ravel()))
+    op.close()
+    pts = (s.nx + 2 * s.nb) * (s.nz + 2 * s.nb) * s.nt * s.ns
+    rec = {"workload": f"LSRTM operator, {s.ns} shots of {s.nx}x{s.nz} ({s.nx + 2 * s.nb}x{s.nz + 2 * s.nb} "
+                       f"padded), nt {s.nt}, {s.ng} receivers; FAST arithmetic, one batch",
+           "born_s": t_born, "born_gpts": 2 * pts / t_born / 1e9,
+           "migration_s": t_mig, "migration_gpts": 3 * pts / t_mig / 1e9,
+           "exact_adjoint_s": t_adj, "exact_adjoint_gpts": 3 * pts / t_adj / 1e9,
+           "unit": "Gpts/s of padded-field point updates (Born 2, migration 3 per point per step)",
+           "dot_product": {"lm_d": a, "m_ltd": b, "rel": abs(a - b) / abs(a), "ok": abs(a - b) <= 1e-5 * abs(a)}}
+    if cpu:
+        import oracle
+        if os.path.exists(os.path.join(oracle.REF_DIR, "libprtm_ref.so")):
+            r = oracle.PrtmRef(vt, ns=1, **kw)
+            m1 = mod.cpu().numpy()
+            d1 = np.zeros((1, s.ng, s.nt), np.float32)
+            tc, _ = _cpu_timed(lambda: r.lop(0, 0, m1, d1))
+            r.close()
+            rec["cpu"] = {"born_s": tc * s.ns, "kind": "reference", "cores": _cores(),
+                          "basis": f"the reference's prtm2d_lop Born branch (compiled in place, OpenMP) for one "
+                                   f"shot ({tc:.2f} s) x {s.ns} shots"}
+            rec["born_speedup_vs_cpu"] = tc * s.ns / t_born
+    return rec
+
+
 def _cores():
     return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
@@ -524,12 +578,17 @@ def network_flops(layers, N, H, W):
 
 
 def run_learned_mode(args):
+    print(json.dumps(learned_record(args, verbose=True)))
+    return 0
+
+
+def learned_record(args, verbose=False):
     """FWI wall-clock to equal model error, learned vs plain: train the
     preconditioner on plain FWI runs over seeded models, then on each
     held-out model run plain FWI for its epoch budget and learned FWI until
     it reaches the lowest model error plain reached.  value: the geometric
-    mean over the held-out models of plain seconds / learned seconds.  Also
-    times the network's kernels."""
+    mean over the held-out models of plain seconds / learned seconds, with
+    every model's own figure beside it.  Also times the network's kernels."""
     import math
     import torch
     from swfwi_b200 import precond as P
@@ -537,7 +596,8 @@ def run_learned_mode(args):
                       ns=args.learned_shots).scaled(maxdv=100.0)
     net, st = P.train_from_plain(s, range(100, 100 + args.learned_models), args.learned_iters,
                                  args.learned_epochs, batch=16)
-    print(json.dumps({"training": st}), file=sys.stderr, flush=True)
+    if verbose:
+        print(json.dumps({"training": st}), file=sys.stderr, flush=True)
     tests = []
     for seed in args.learned_test_seeds:
         r = P.compare(s, net, seed, args.learned_iters, min_decrease=args.learned_min_decrease)
@@ -552,7 +612,9 @@ def run_learned_mode(args):
                       "learned_steps": {"tried": r["learned_stats"][1], "accepted": r["learned_stats"][2]},
                       "plain_history": [[round(a, 3), b] for a, b, _, _ in r["plain_history"]],
                       "learned_history": [[round(a, 3), b, bool(d)] for a, b, _, d in r["learned_history"]]})
-        print(json.dumps({k: v for k, v in tests[-1].items() if "history" not in k}), file=sys.stderr, flush=True)
+        if verbose:
+            print(json.dumps({k: v for k, v in tests[-1].items() if "history" not in k}), file=sys.stderr,
+                  flush=True)
     sps = [t["speedup"] for t in tests]
     value = math.exp(sum(math.log(x) for x in sps) / len(sps))
     H, W = P.image_shape(P.Damp4t10d.from_survey(s))
@@ -573,8 +635,7 @@ def run_learned_mode(args):
                    "test_seeds": list(args.learned_test_seeds)},
         "training": st, "tests": tests, "network": network,
     }
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def time_network(net, N, H, W, reps=10):
@@ -642,8 +703,10 @@ def main():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the records of the other workloads (plain FWI iteration, encoded-source "
-                         "FWI, EnKF analysis)")
+                         "FWI, EnKF analysis, LSRTM operator, learned vs plain FWI)")
     ap.add_argument("--ess-iters", type=int, default=3, help="timed encoded-source FWI iterations")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="leave the learned-vs-plain record (about three minutes) out of the configs")
     ap.add_argument("--mode", default="bench", choices=["bench", "kernel", "tune", "learned", "network"],
                     help="kernel: short 96-shot batched forward (the small case for ncu); "
                          "tune: print the autotuner's table; learned: FWI wall-clock to equal model "
@@ -805,7 +868,9 @@ def main():
         for key, fn in (("fwi_iteration_151x461", lambda: record_fwi_iteration(torch, arith, tuning,
                                                                                 not args.no_cpu_baseline)),
                         ("encoded_fwi_301x921", lambda: record_encoded(torch, arith, tuning, args.ess_iters)),
-                        ("enkf_201x461", lambda: record_enkf(torch, arith, tuning, not args.no_cpu_baseline))):
+                        ("enkf_201x461", lambda: record_enkf(torch, arith, tuning, not args.no_cpu_baseline)),
+                        ("lsrtm_151x461", lambda: record_lsrtm(torch, not args.no_cpu_baseline)),
+                        ("learned_fwi_240x80", lambda: None if args.no_learned else learned_record(args))):
             try:
                 configs[key] = fn()
             except Exception as e:   # reported, never required

@@ -333,6 +333,10 @@ int swfwi_prtm2d_create(swfwi_prtm **out, int arith, float dz, float dx, float d
                         int nx, int nb, int nt, int ns, int ng, int sxbeg, int szbeg, int jsx, int jsz, int gxbeg,
                         int gzbeg, int jgx, int jgz, int csdgather, const float *vel, void *stream);
 int swfwi_prtm2d_set_adjoint(swfwi_prtm *h, int mode);
+/* on = 1 (default): a call that repeats an earlier call's arrays, direction
+ * and adjoint mode replays its time loops as one CUDA graph (captured on
+ * the second such call); 0: every call launches its kernels one by one. */
+int swfwi_prtm2d_set_graphs(swfwi_prtm *h, int on);
 /* shots one launch sequence carries (1 for REF) */
 int swfwi_prtm2d_batch(swfwi_prtm *h, int *shots);
 /* prtm2d_lop (:354-437): adj = 0: dat += L mod (Born); adj = 1: mod += L'

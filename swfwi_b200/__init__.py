@@ -149,6 +149,7 @@ _SIGS = {
     "swfwi_regu_gradient": [_vp, C.c_int, C.c_int, C.c_float, C.c_float, _vp, C.c_int, _vp],
     "swfwi_prtm2d_create": [C.POINTER(_vp), C.c_int] + [C.c_float] * 5 + [C.c_int] * 15 + [_vp, _vp],
     "swfwi_prtm2d_set_adjoint": [_vp, C.c_int],
+    "swfwi_prtm2d_set_graphs": [_vp, C.c_int],
     "swfwi_prtm2d_batch": [_vp, _ip],
     "swfwi_prtm2d_lop": [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp],
     "swfwi_prtm2d_destroy": [_vp],
@@ -464,6 +465,10 @@ class Prtm2d:
 
     def set_adjoint(self, mode: int) -> None:
         _check(lib().swfwi_prtm2d_set_adjoint(self.h, mode))
+
+    def set_graphs(self, on: bool) -> None:
+        """Replay repeated calls (same arrays, direction, mode) as CUDA graphs."""
+        _check(lib().swfwi_prtm2d_set_graphs(self.h, int(bool(on))))
 
     def batch(self) -> int:
         out = C.c_int()

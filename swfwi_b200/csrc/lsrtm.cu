@@ -34,6 +34,7 @@
 // passes the dot-product test and is what a least-squares (CG) solver needs.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <memory>
 #include <vector>
 #include "common.hpp"
@@ -48,17 +49,31 @@ struct PrtmCoef {
   float c0, c11, c12, c21, c22;
 };
 
-// One time step of every slot's field: u0 <- 2 u1 - u0 + (stencil) on
-// [2, nxpad-2) x [2, nzpad-2), in place (a point reads only its own u0).
-// Grid (z blocks, nxpad - 4 columns, slots).
+// The cells of column ix that the sponge touches: all of an edge column,
+// else the nb cells at each end.  Thread t of the column -> iz, or -1.
+__device__ __forceinline__ int sponge_iz(int t, int ix, int nxpad, int nzpad, int nb) {
+  const bool edge = ix < nb || ix >= nxpad - nb;
+  if (edge) return t < nzpad ? t : -1;
+  if (t >= 2 * nb) return -1;
+  return t < nb ? t : nzpad - 2 * nb + t;
+}
+
+// Field geometry shared by the kernels.  Per-slot positions: the source
+// spos[slot] and the receivers rpos[slot*ng + ig] (padded linear indices).
+struct PrtmGeo {
+  int nx, nz, nb, nxpad, nzpad, nt, ng;
+  long long fsz;             // floats per field slot
+  const int *spos, *rpos;
+  const float *w;            // sponge taper [nb]
+  int serial;                // receivers share a cell: inject in ig order
+};
+
+// One time step u0 <- 2 u1 - u0 + (stencil) at the padded point (ix, iz)
+// of one slot (ix, iz in [2, n-2)); in place (a point reads only its own
+// u0).
 template <int ARITH, bool ADJ>
-__global__ void k_prtm_step(float *u0, const float *u1, const float *vv, int nzpad, long long fsz, PrtmCoef c) {
-  const int iz = 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (iz >= nzpad - 2) return;
-  const long long off = (long long)blockIdx.z * fsz;
-  const long long p = (long long)(2 + blockIdx.y) * nzpad + iz;
-  const float *w = u1 + off;
-  float *o = u0 + off;
+__device__ __forceinline__ void prtm_update(float *o, const float *w, const float *vv, long long p, int nzpad,
+                                            const PrtmCoef &c) {
   const float uc = w[p];
   if constexpr (ARITH == ARITH_REF) {
     if constexpr (!ADJ) {
@@ -101,108 +116,150 @@ __global__ void k_prtm_step(float *u0, const float *u1, const float *vv, int nzp
   }
 }
 
-// The cells of column ix that the sponge touches: all of an edge column,
-// else the nb cells at each end.  Thread t of the column -> iz, or -1.
-__device__ __forceinline__ int sponge_iz(int t, int ix, int nxpad, int nzpad, int nb) {
-  const bool edge = ix < nb || ix >= nxpad - nb;
-  if (edge) return t < nzpad ? t : -1;
-  if (t >= 2 * nb) return -1;
-  return t < nb ? t : nzpad - 2 * nb + t;
+// Receivers of one time step for one slot, receiver ig: dat += field
+// (mode 2, record) or field += dat (mode 1, inject); dat[slot*nt*ng + ig*nt
+// + it].  With g.serial one thread injects every receiver in ig order.
+__device__ __forceinline__ void prtm_receiver(const PrtmGeo &g, int slot, int ig, float *f, float *dat, int it,
+                                              int mode) {
+  if (ig >= g.ng || (g.serial && mode == 1 && ig > 0)) return;
+  const int last = (g.serial && mode == 1) ? g.ng : ig + 1;
+  for (int r = ig; r < last; r++) {
+    float *q = f + (long long)slot * g.fsz + g.rpos[(long long)slot * g.ng + r];
+    float *d = dat + (long long)slot * g.nt * g.ng + (long long)r * g.nt + it;
+    if (mode == 2) *d = __fadd_rn(*d, *q);
+    else *q = __fadd_rn(*q, *d);
+  }
 }
 
-// apply_sponge on two sets of fields.  A point ibz cells from the top or
-// bottom and ibx cells from the left or right edge is multiplied by w[ibz]
-// and w[ibx] (each only when < nb) in the reference's loop order: ib
-// ascending, the z edges before the x edges of the same ib.  Grid (z
-// blocks of nzpad, nxpad columns, slots).
-__global__ void k_prtm_sponge(float *a, float *b, const float *w, int nxpad, int nzpad, int nb, long long fsz) {
-  const int ix = blockIdx.y;
-  const int iz = sponge_iz(blockIdx.x * blockDim.x + threadIdx.x, ix, nxpad, nzpad, nb);
-  if (iz < 0) return;
-  const int ibz = min(iz, nzpad - 1 - iz), ibx = min(ix, nxpad - 1 - ix);
-  const long long p = (long long)blockIdx.z * fsz + (long long)ix * nzpad + iz;
-  float *fs[2] = {a + p, b + p};
+// The stencil steps of one time step, in one launch: the receiver-side
+// pair (G, kg slots, Born's form when gadj) and the source-side pair (S,
+// ks slots), blockIdx.z over kg + ks; blocks with blockIdx.y >= nxpad - 4
+// record the receivers of G1 (rec_mode 2), which the G step only reads.
+// Grid (z blocks of nzpad - 4, nxpad - 4 + receiver columns, kg + ks).
+template <int ARITH, bool GADJ>
+__global__ void k_prtm_steps(PrtmGeo g, const float *vv, PrtmCoef c, float *g0, const float *g1, int kg, float *s0,
+                             const float *s1, float *dat, int it, int rec_mode) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int z = blockIdx.z;
+  if ((int)blockIdx.y >= g.nxpad - 4) {
+    if (z < kg && rec_mode)
+      prtm_receiver(g, z, (blockIdx.y - (g.nxpad - 4)) * gridDim.x * blockDim.x + t, const_cast<float *>(g1), dat,
+                    it, rec_mode);
+    return;
+  }
+  const int iz = 2 + t;
+  if (iz >= g.nzpad - 2) return;
+  const long long p = (long long)(2 + blockIdx.y) * g.nzpad + iz;
+  if (z < kg) {
+    const long long off = (long long)z * g.fsz;
+    prtm_update<ARITH, GADJ>(g0 + off, g1 + off, vv, p, g.nzpad, c);
+  } else {
+    const long long off = (long long)(z - kg) * g.fsz;
+    prtm_update<ARITH, false>(s0 + off, s1 + off, vv, p, g.nzpad, c);
+  }
+}
+
+// Index in the boundary_rw store of the padded cell (ix, iz), or -1: the 4
+// cells above and below each model column, then the two columns on each
+// side of the model (:37-80).
+__device__ __forceinline__ int prtm_ring_index(const PrtmGeo &g, int ix, int iz) {
+  const int mx = ix - g.nb, mz = iz - g.nb;
+  if (mx >= 0 && mx < g.nx) {
+    if (mz == -2 || mz == -1) return 4 * mx + mz + 2;
+    if (mz == g.nz || mz == g.nz + 1) return 4 * mx + 2 + mz - g.nz;
+    return -1;
+  }
+  if (mz >= 0 && mz < g.nz) {
+    if (mx == -2 || mx == -1) return 4 * g.nx + mz + g.nz * (mx + 2);
+    if (mx == g.nx || mx == g.nx + 1) return 4 * g.nx + mz + g.nz * (2 + mx - g.nx);
+  }
+  return -1;
+}
+
+// The work of one time step on cells that no stencil step of the same
+// launch touches, in one launch.  Three roles by blockIdx.y:
+//  * y < nxpad, edge cells of column y (the sponge bands, nb cells from
+//    every side; the 2-cell ring lies inside them): apply_sponge (:123-145)
+//    to up to four fields, in the reference's order for a point ibz cells
+//    from the top or bottom and ibx from the left or right (ib ascending,
+//    the z edges before the x edges); then save the ring of ring_f (after
+//    its sponge) or overwrite it from the store;
+//  * nxpad <= y < nxpad + nx, model column y - nxpad: Born injection g +=
+//    S mod (cross 1) or imaging img += S g (cross 2), and the source
+//    add_source (:161-189) at the slot's source cell;
+//  * y >= nxpad + nx: receivers (rec_mode 1 inject, 2 record).
+// The model interior (W = 1) and the sponge bands are disjoint, so the
+// roles never touch the same cell.  Grid (z blocks of nzpad, nxpad + nx +
+// receiver columns, slots).
+struct PrtmAux {
+  float *sp[4];
+  float *ring_f, *ring;
+  long long ring_stride;
+  int ring_mode;             // 0 none, 1 save, 2 read
+  int cross;                 // 0 none, 1 Born injection, 2 imaging
+  float *cg;
+  const float *cs, *mod;
+  float *img;
+  long long img_stride;
+  float *src_f;              // null: no source operation
+  const float *src_val;
+  int src_sign;
+  float *rec_f, *dat;
+  int rec_it, rec_mode;
+};
+
+__global__ void k_prtm_aux(PrtmGeo g, PrtmAux a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, slot = blockIdx.z;
+  if (y < g.nxpad) {
+    const int ix = y;
+    const int iz = sponge_iz(t, ix, g.nxpad, g.nzpad, g.nb);
+    if (iz < 0) return;
+    const long long p = (long long)slot * g.fsz + (long long)ix * g.nzpad + iz;
+    const int ibz = min(iz, g.nzpad - 1 - iz), ibx = min(ix, g.nxpad - 1 - ix);
 #pragma unroll
-  for (int f = 0; f < 2; f++) {
-    float v = *fs[f];
-    if (ibz <= ibx) {
-      if (ibz < nb) v = __fmul_rn(v, w[ibz]);
-      if (ibx < nb) v = __fmul_rn(v, w[ibx]);
-    } else {
-      if (ibx < nb) v = __fmul_rn(v, w[ibx]);
-      if (ibz < nb) v = __fmul_rn(v, w[ibz]);
+    for (int f = 0; f < 4; f++) {
+      if (!a.sp[f]) continue;
+      float v = a.sp[f][p];
+      if (ibz <= ibx) {
+        if (ibz < g.nb) v = __fmul_rn(v, g.w[ibz]);
+        if (ibx < g.nb) v = __fmul_rn(v, g.w[ibx]);
+      } else {
+        if (ibx < g.nb) v = __fmul_rn(v, g.w[ibx]);
+        if (ibz < g.nb) v = __fmul_rn(v, g.w[ibz]);
+      }
+      a.sp[f][p] = v;
     }
-    *fs[f] = v;
+    if (a.ring_mode) {
+      const int i = prtm_ring_index(g, ix, iz);
+      if (i >= 0) {
+        float *b = a.ring + (long long)slot * a.ring_stride + i;
+        if (a.ring_mode == 1) *b = a.ring_f[p];
+        else a.ring_f[p] = *b;
+      }
+    }
+    return;
   }
-}
-
-// boundary_rw: the 2-cell ring of one step, 4 (nx + nz) values a slot at
-// bnd + slot * bnd_stride, in the reference's order (the 4 cells above and
-// below each column, then the two columns left and right of the model).
-// Grid (ring blocks, slots).
-__global__ void k_prtm_ring(float *p, float *bnd, long long bnd_stride, int nx, int nz, int nb, int nzpad,
-                            long long fsz, int read) {
-  const int m = 4 * (nx + nz);
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
-  int gx, gz;
-  if (i < 4 * nx) {
-    const int r = i % 4;
-    gx = i / 4 + nb;
-    gz = r < 2 ? r - 2 + nb : r - 2 + nz + nb;
-  } else {
-    const int j = i - 4 * nx, col = j / nz;
-    gz = j % nz + nb;
-    gx = col < 2 ? col - 2 + nb : col - 2 + nx + nb;
+  if (y < g.nxpad + g.nx) {
+    const int mx = y - g.nxpad, mz = t;
+    if (mz >= g.nz) return;
+    const long long q = (long long)(mx + g.nb) * g.nzpad + mz + g.nb;
+    const long long p = (long long)slot * g.fsz + q;
+    if (a.cross == 1) {
+      a.cg[p] = __fadd_rn(a.cg[p], __fmul_rn(a.cs[p], a.mod[(long long)mx * g.nz + mz]));
+    } else if (a.cross == 2) {
+      float *o = a.img + (long long)slot * a.img_stride + (long long)mx * g.nz + mz;
+      *o = __fadd_rn(*o, __fmul_rn(a.cs[p], a.cg[p]));
+    }
+    if (a.src_f && q == g.spos[slot]) {
+      float *f = a.src_f + p;
+      *f = a.src_sign > 0 ? __fadd_rn(*f, *a.src_val) : __fsub_rn(*f, *a.src_val);
+    }
+    return;
   }
-  float *f = p + (long long)blockIdx.y * fsz + (long long)gx * nzpad + gz;
-  float *b = bnd + (long long)blockIdx.y * bnd_stride + i;
-  if (read) *f = *b;
-  else *b = *f;
-}
-
-// add_source (:161-189) of the wavelet sample *val at slot s's position
-__global__ void k_prtm_source(float *p, const int *pos, const float *val, long long fsz, int nslots, int sign) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nslots) return;
-  float *f = p + (long long)s * fsz + pos[s];
-  *f = sign > 0 ? __fadd_rn(*f, *val) : __fsub_rn(*f, *val);
-}
-
-// Receivers of one time step: dat += field (record) or field += dat
-// (inject).  rec[s*ng + ig] padded linear index; dat[s*dat_stride + ig*nt
-// + it].  serial: receivers that share a cell, injected in ig order by one
-// thread.  Grid (receiver blocks, slots).
-__global__ void k_prtm_receivers(float *p, float *dat, const int *rec, long long dat_stride, int ng, int nt, int it,
-                                 long long fsz, int record, int serial) {
-  const int s = blockIdx.y;
-  const int first = blockIdx.x * blockDim.x + threadIdx.x;
-  if (first >= ng || (serial && first > 0)) return;
-  const int last = serial ? ng : first + 1;
-  for (int ig = first; ig < last; ig++) {
-    float *f = p + (long long)s * fsz + rec[(long long)s * ng + ig];
-    float *d = dat + (long long)s * dat_stride + (long long)ig * nt + it;
-    if (record) *d = __fadd_rn(*d, *f);
-    else *f = __fadd_rn(*f, *d);
-  }
-}
-
-// Over the model interior: imaging img[s*img_stride + ix*nz + iz] += S g
-// (born = 0), or Born injection g += S mod (born = 1).  Grid (z blocks,
-// nx, slots).
-__global__ void k_prtm_cross(float *img, long long img_stride, float *g, const float *sf, const float *mod, int nz,
-                             int nb, int nzpad, long long fsz, int born) {
-  const int iz = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iz >= nz) return;
-  const int ix = blockIdx.y, slot = blockIdx.z;
-  const long long m = (long long)ix * nz + iz;
-  const long long p = (long long)slot * fsz + (long long)(ix + nb) * nzpad + iz + nb;
-  if (born) {
-    g[p] = __fadd_rn(g[p], __fmul_rn(sf[p], mod[m]));
-  } else {
-    float *o = img + (long long)slot * img_stride + m;
-    *o = __fadd_rn(*o, __fmul_rn(sf[p], g[p]));
-  }
+  if (a.rec_mode)
+    prtm_receiver(g, slot, (y - g.nxpad - g.nx) * gridDim.x * blockDim.x + t, a.rec_f, a.dat, a.rec_it,
+                  a.rec_mode);
 }
 
 // mod += the per-slot images, in slot order
@@ -286,26 +343,24 @@ class Prtm {
     SWFWI_REQUIRE(vel, "null velocity");
     nzpad_ = nz + 2 * nb;
     nxpad_ = nx + 2 * nb;
-    SWFWI_REQUIRE((long long)nzpad_ * nxpad_ < (1LL << 31) && nxpad_ <= 65535, "grid too large");
+    SWFWI_REQUIRE((long long)nzpad_ * nxpad_ < (1LL << 31) && nxpad_ + nx_ + ng <= 65535, "grid too large");
     SWFWI_REQUIRE((long long)nt * ng * ns < (1LL << 31) && (long long)nx * nz < (1LL << 31),
                   "data or model too large for the operator's int sizes");
     // prtm2d_init's geometry checks (:326-336), applied to every shot and
     // receiver: the reference checks the first and last only
     const int distx = sxbeg - gxbeg;
-    spos_h_.resize(ns);
-    rpos_h_.resize((size_t)ns * ng);
+    std::vector<int> spos(ns), rpos((size_t)ns * ng);
     for (int is = 0; is < ns; is++) {
       const int sx = sxbeg + is * jsx, sz = szbeg + is * jsz;
       SWFWI_REQUIRE(sx >= 0 && sx < nx && sz >= 0 && sz < nz, "sources exceed the computing zone");
-      spos_h_[is] = pidx(sx, sz);
+      spos[is] = pidx(sx, sz);
       const int gx0 = csd ? sx - distx : gxbeg;
       for (int ig = 0; ig < ng; ig++) {
         const int gx = gx0 + ig * jgx, gz = gzbeg + ig * jgz;
         SWFWI_REQUIRE(gx >= 0 && gx < nx && gz >= 0 && gz < nz, "geophones exceed the computing zone");
-        rpos_h_[(size_t)is * ng + ig] = pidx(gx, gz);
+        rpos[(size_t)is * ng + ig] = pidx(gx, gz);
       }
     }
-    serial_rec_ = ng > 1 && jgx == 0 && jgz == 0;
     // coefficients, as prtm2d_init computes them (:254-261)
     float t = (float)(1.0 / (dz * dz));
     c_.c11 = (float)(4.0 * t / 3.0);
@@ -327,21 +382,32 @@ class Prtm {
     }
     sponge_.upload(w, st);
     wlt_.upload(wlt, st);
+    spos_.upload(spos, st);
+    rpos_.upload(rpos, st);
     vv_.resize((size_t)nxpad_ * nzpad_);
     k_prtm_vv<<<dim3((nzpad_ + kLsZ - 1) / kLsZ, nxpad_), kLsZ, 0, st>>>(vv_.get(), vel, nx, nz, nb, dt);
     note_launch();
     SWFWI_CUDA(cudaGetLastError());
     // the shot batch: one shot for REF (the reference's order), else as
-    // many as the budget holds
+    // many as the budget holds; every buffer a call needs, allocated here
     const size_t fsz = (size_t)nxpad_ * nzpad_;
-    const size_t per_shot =
-        sizeof(float) * (5 * fsz + (size_t)nt * 4 * (nx + nz) + (size_t)nx * nz) + sizeof(int) * (1 + ng);
+    const size_t per_shot = sizeof(float) * (5 * fsz + (size_t)nt * 4 * (nx + nz) + (size_t)nx * nz);
     kmax_ = arith == ARITH_REF ? 1 : (int)std::max<size_t>(1, std::min<size_t>(ns, kBatchBudget / per_shot));
     kmax_ = std::min(kmax_, 65535);
-    for (DevBuf<float> *f : {&sp0_, &sp1_, &gp0_, &gp1_}) {
+    for (DevBuf<float> *f : {&sp0_, &sp1_, &gp0_, &gp1_, &gp2_}) {
       f->resize((size_t)kmax_ * fsz);
       f->zero(st);
     }
+    ring_.resize((size_t)kmax_ * nt * 4 * (nx + nz));
+    if (kmax_ > 1) img_.resize((size_t)kmax_ * nx * nz);
+    geo_ = PrtmGeo{nx, nz, nb, nxpad_, nzpad_, nt, ng, (long long)fsz, spos_.get(), rpos_.get(), sponge_.get(),
+                   ng > 1 && jgx == 0 && jgz == 0 ? 1 : 0};
+  }
+
+  ~Prtm() {
+    for (Graph &g : graphs_)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (cap_) cudaStreamDestroy(cap_);
   }
 
   int nx() const { return nx_; }
@@ -354,66 +420,121 @@ class Prtm {
     SWFWI_REQUIRE(m == SWFWI_PRTM_ADJ_REFERENCE || m == SWFWI_PRTM_ADJ_EXACT, "unknown adjoint mode");
     adj_mode_ = m;
   }
+  void set_graphs(bool on) { use_graphs_ = on; }
 
-  // prtm2d_lop (:354-437) on device arrays
+  // prtm2d_lop (:354-437) on device arrays.  A call that repeats an earlier
+  // one's arrays, direction and mode replays the time loops as one CUDA
+  // graph (captured on the second such call).
   void lop(bool adj, bool add, float *mod, float *dat, cudaStream_t st) {
-    const long long nm = (long long)nx_ * nz_, nd = (long long)nt_ * ng_ * ns_;
-    // sf_adjnull: without add, the output starts at zero
-    if (!add) {
-      if (adj) SWFWI_CUDA(cudaMemsetAsync(mod, 0, sizeof(float) * nm, st));
-      else SWFWI_CUDA(cudaMemsetAsync(dat, 0, sizeof(float) * nd, st));
+    const std::vector<long long> key = {adj, add, adj_mode_, reinterpret_cast<long long>(mod),
+                                        reinterpret_cast<long long>(dat), g_swapped_};
+    auto body = [&](cudaStream_t s) {
+      const long long nm = (long long)nx_ * nz_, nd = (long long)nt_ * ng_ * ns_;
+      // sf_adjnull: without add, the output starts at zero
+      if (!add) {
+        if (adj) SWFWI_CUDA(cudaMemsetAsync(mod, 0, sizeof(float) * nm, s));
+        else SWFWI_CUDA(cudaMemsetAsync(dat, 0, sizeof(float) * nd, s));
+      }
+      for (int s0 = 0; s0 < ns_; s0 += kmax_) run(adj, mod, dat, s0, std::min(kmax_, ns_ - s0), s);
+    };
+    if (!use_graphs_) {
+      body(st);
+      SWFWI_CUDA(cudaGetLastError());
+      return;
     }
-    for (int s0 = 0; s0 < ns_; s0 += kmax_) run(adj, mod, dat, s0, std::min(kmax_, ns_ - s0), st);
+    for (size_t i = 0; i < graphs_.size(); i++)
+      if (graphs_[i].key == key) {
+        if (graphs_[i].exec) {
+          SWFWI_CUDA(cudaGraphLaunch(graphs_[i].exec, st));
+          g_swapped_ = graphs_[i].swapped_after;
+          return;
+        }
+        // second call with these arrays: capture the calls from now on
+        if (!cap_) SWFWI_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        SWFWI_CUDA(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal));
+        try {
+          body(cap_);
+        } catch (...) {
+          cudaStreamEndCapture(cap_, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        SWFWI_CUDA(cudaStreamEndCapture(cap_, &g));
+        const cudaError_t err = cudaGraphInstantiate(&graphs_[i].exec, g, 0);
+        cudaGraphDestroy(g);
+        SWFWI_CUDA(err);
+        graphs_[i].swapped_after = g_swapped_;
+        SWFWI_CUDA(cudaGraphLaunch(graphs_[i].exec, st));
+        return;
+      }
+    body(st);
     SWFWI_CUDA(cudaGetLastError());
+    if (graphs_.size() >= kGraphs) {
+      if (graphs_.front().exec) cudaGraphExecDestroy(graphs_.front().exec);
+      graphs_.erase(graphs_.begin());
+    }
+    graphs_.push_back(Graph{key, nullptr, g_swapped_});
   }
 
  private:
+  struct Graph {
+    std::vector<long long> key;
+    cudaGraphExec_t exec;
+    bool swapped_after;
+  };
+  static constexpr size_t kGraphs = 4;
+
   int pidx(int x, int z) const { return (x + nb_) * nzpad_ + z + nb_; }
   long long fsz() const { return (long long)nxpad_ * nzpad_; }
+  int rec_cols(int zthreads) const { return (ng_ + zthreads - 1) / zthreads; }
 
-  void step(float *u0, const float *u1, bool adj_form, int k, cudaStream_t st) {
-    const dim3 g((nzpad_ - 4 + kLsZ - 1) / kLsZ, nxpad_ - 4, k);
+  // the stencil steps of one time step (k_prtm_steps); kg, ks slots of the
+  // receiver and source pairs, G's in Born's form when gadj
+  void steps(bool gadj, float *g0, const float *g1, int kg, float *s0, const float *s1, int ks, float *dat, int it,
+             int rec_mode, cudaStream_t st) {
+    const int zb = (nzpad_ - 4 + kLsZ - 1) / kLsZ;
+    const dim3 grid(zb, nxpad_ - 4 + (rec_mode ? rec_cols(zb * kLsZ) : 0), kg + ks);
     if (arith_ == ARITH_REF) {
-      if (adj_form) k_prtm_step<ARITH_REF, true><<<g, kLsZ, 0, st>>>(u0, u1, vv_.get(), nzpad_, fsz(), c_);
-      else k_prtm_step<ARITH_REF, false><<<g, kLsZ, 0, st>>>(u0, u1, vv_.get(), nzpad_, fsz(), c_);
+      if (gadj) k_prtm_steps<ARITH_REF, true><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
+                                                                     rec_mode);
+      else k_prtm_steps<ARITH_REF, false><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
+                                                                 rec_mode);
     } else {
-      if (adj_form) k_prtm_step<ARITH_FAST, true><<<g, kLsZ, 0, st>>>(u0, u1, vv_.get(), nzpad_, fsz(), c_);
-      else k_prtm_step<ARITH_FAST, false><<<g, kLsZ, 0, st>>>(u0, u1, vv_.get(), nzpad_, fsz(), c_);
+      if (gadj) k_prtm_steps<ARITH_FAST, true><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat,
+                                                                      it, rec_mode);
+      else k_prtm_steps<ARITH_FAST, false><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
+                                                                  rec_mode);
     }
     note_launch();
   }
 
-  void sponge(float *a, float *b, int k, cudaStream_t st) {
-    const dim3 g((nzpad_ + kLsZ - 1) / kLsZ, nxpad_, k);
-    k_prtm_sponge<<<g, kLsZ, 0, st>>>(a, b, sponge_.get(), nxpad_, nzpad_, nb_, fsz());
+  void aux(const PrtmAux &a, int k, cudaStream_t st) {
+    const int zb = (nzpad_ + kLsZ - 1) / kLsZ;
+    const dim3 grid(zb, nxpad_ + nx_ + (a.rec_mode ? rec_cols(zb * kLsZ) : 0), k);
+    k_prtm_aux<<<grid, kLsZ, 0, st>>>(geo_, a);
     note_launch();
   }
 
-  void source(float *p, int it, int sign, int k, cudaStream_t st) {
-    k_prtm_source<<<(k + 127) / 128, 128, 0, st>>>(p, spos_.get(), wlt_.get() + it, fsz(), k, sign);
-    note_launch();
+  static PrtmAux none() {
+    PrtmAux a;
+    memset(&a, 0, sizeof(a));
+    return a;
   }
 
-  void receivers(float *p, float *d, int it, bool record, int k, cudaStream_t st) {
-    const bool serial = serial_rec_ && !record;
-    const dim3 g(serial ? 1 : (ng_ + 127) / 128, k);
-    k_prtm_receivers<<<g, 128, 0, st>>>(p, d, rpos_.get(), (long long)nt_ * ng_, ng_, nt_, it, fsz(), record,
-                                        serial);
-    note_launch();
-  }
-
-  void ring(float *p, int it, bool read, int k, cudaStream_t st) {
-    const int m = 4 * (nx_ + nz_);
-    k_prtm_ring<<<dim3((m + 255) / 256, k), 256, 0, st>>>(p, ring_.get() + (long long)it * m, (long long)nt_ * m,
-                                                          nx_, nz_, nb_, nzpad_, fsz(), read);
-    note_launch();
-  }
-
+  // One batch of k shots from shot s0.  Each time step is two or three
+  // launches: the stencil steps of both field pairs in one (k_prtm_steps),
+  // and the sponge, ring, imaging or Born injection, source and receivers
+  // in one or two (k_prtm_aux), the reference's operations regrouped where
+  // they touch disjoint cells and so commute.
   void run(bool adj, float *mod, float *dat, int s0, int k, cudaStream_t st) {
     const long long nm = (long long)nx_ * nz_;
     const size_t fbytes = sizeof(float) * (size_t)k * fsz();
-    spos_.upload(spos_h_.data() + s0, k, st);
-    rpos_.upload(rpos_h_.data() + (size_t)s0 * ng_, (size_t)k * ng_, st);
+    PrtmGeo g = geo_;
+    g.spos = spos_.get() + s0;
+    g.rpos = rpos_.get() + (size_t)s0 * ng_;
+    const PrtmGeo saved = geo_;
+    geo_ = g;
     // the shot's source fields start at zero (:364-365); the receiver
     // fields do in the migration (:381-382) and, outside REF, in Born
     SWFWI_CUDA(cudaMemsetAsync(sp0_.get(), 0, fbytes, st));
@@ -426,52 +547,84 @@ class Prtm {
       SWFWI_CUDA(cudaMemsetAsync(G1, 0, fbytes, st));
     }
     float *d = dat + (long long)s0 * nt_ * ng_;
-    const dim3 gmod((nz_ + kLsZ - 1) / kLsZ, nx_, k);
+    const float *wl = wlt_.get();
     if (adj) {
-      // the source field forward, its ring saved every step (:372-379)
-      ring_.resize((size_t)k * nt_ * 4 * (nx_ + nz_));
+      const int m = 4 * (nx_ + nz_);
+      const long long rstride = (long long)nt_ * m;
+      // the source field forward, its ring saved every step (:372-379):
+      // source at it, step, sponge, swap, save; the next step's source
+      // rides with this step's sponge
+      PrtmAux a = none();
+      a.src_f = S1;
+      a.src_val = wl;
+      a.src_sign = 1;
+      aux(a, k, st);
       for (int it = 0; it < nt_; it++) {
-        source(S1, it, +1, k, st);
-        step(S0, S1, false, k, st);
-        sponge(S0, S1, k, st);
+        steps(false, nullptr, nullptr, 0, S0, S1, k, nullptr, 0, 0, st);
+        a = none();
+        a.sp[0] = S0;
+        a.sp[1] = S1;
         std::swap(S0, S1);
-        ring(S0, it, false, k, st);
+        a.ring_mode = 1;
+        a.ring_f = S0;
+        a.ring = ring_.get() + (long long)it * m;
+        a.ring_stride = rstride;
+        if (it + 1 < nt_) {
+          a.src_f = S1;
+          a.src_val = wl + it + 1;
+          a.src_sign = 1;
+        }
+        aux(a, k, st);
       }
       float *img = mod;
       long long img_stride = 0;
       if (k > 1) {
-        img_.resize((size_t)k * nm);
-        img_.zero(st);
+        SWFWI_CUDA(cudaMemsetAsync(img_.get(), 0, sizeof(float) * (size_t)k * nm, st));
         img = img_.get();
         img_stride = nm;
       }
       const bool exact = adj_mode_ == SWFWI_PRTM_ADJ_EXACT;
-      float *G2 = nullptr;
-      if (exact) {
-        gp2_.resize((size_t)k * fsz());
-        G2 = gp2_.get();
-      }
+      float *G2 = gp2_.get();
       const dim3 gfull((nzpad_ + kLsZ - 1) / kLsZ, nxpad_, k);
       for (int it = nt_ - 1; it >= 0; it--) {
-        // reconstruct the source field (:388-391)
-        ring(S0, it, true, k, st);
+        // ring of the source field (:388), the previous step's source
+        // subtraction (:391), the data into the receiver field (:394-398)
+        a = none();
+        a.ring_mode = 2;
+        a.ring_f = S0;
+        a.ring = ring_.get() + (long long)it * m;
+        a.ring_stride = rstride;
+        if (it + 1 < nt_) {
+          a.src_f = S1;
+          a.src_val = wl + it + 1;
+          a.src_sign = -1;
+        }
+        a.rec_f = G1;
+        a.dat = d;
+        a.rec_it = it;
+        a.rec_mode = 1;
+        aux(a, k, st);
         std::swap(S0, S1);
-        step(S0, S1, false, k, st);
-        source(S1, it, -1, k, st);
-        receivers(G1, d, it, false, k, st);
         if (exact) {
-          // G0 = a^, G1 = b^ (the data just injected), G2 scratch
+          // G0 = a^, G1 = b^ (data injected), G2 scratch
+          steps(false, nullptr, nullptr, 0, S0, S1, k, nullptr, 0, 0, st);
           k_prtm_born_transpose<<<gfull, kLsZ, 0, st>>>(G2, G1, G0, vv_.get(), sponge_.get(), S0, img, img_stride,
                                                         nx_, nz_, nb_, nxpad_, nzpad_, fsz(), c_);
           note_launch();
           std::swap(G0, G2);
         } else {
-          // back-propagate the receiver field and image (:394-406)
-          step(G0, G1, false, k, st);
-          sponge(G0, G1, k, st);
+          // reconstruct (:390), back-propagate (:399-402) and image (:404-406)
+          steps(false, G0, G1, k, S0, S1, k, nullptr, 0, 0, st);
+          a = none();
+          a.sp[0] = G0;
+          a.sp[1] = G1;
           std::swap(G0, G1);
-          k_prtm_cross<<<gmod, kLsZ, 0, st>>>(img, img_stride, G1, S0, nullptr, nz_, nb_, nzpad_, fsz(), 0);
-          note_launch();
+          a.cross = 2;
+          a.cs = S0;
+          a.cg = G1;
+          a.img = img;
+          a.img_stride = img_stride;
+          aux(a, k, st);
         }
       }
       if (k > 1) {
@@ -488,30 +641,42 @@ class Prtm {
         G1 = gp1_.get();
       }
     } else {
-      // Born modelling (:410-434)
+      // Born modelling (:410-434).  Per step: the injection G1 += S0 mod,
+      // the swap, the receiver pair's sponge, the source into S1 and the
+      // source pair's sponge of the previous step; then both stencil steps
+      // with the receivers recorded from G1
       for (int it = 0; it < nt_; it++) {
-        k_prtm_cross<<<gmod, kLsZ, 0, st>>>(nullptr, 0, G1, S0, mod, nz_, nb_, nzpad_, fsz(), 1);
-        note_launch();
+        PrtmAux a = none();
+        a.cross = 1;
+        a.cg = G1;
+        a.cs = S0;
+        a.mod = mod;
         std::swap(G0, G1);
-        sponge(G0, G1, k, st);
-        step(G0, G1, true, k, st);
-        receivers(G1, d, it, true, k, st);
-        source(S1, it, +1, k, st);
-        step(S0, S1, false, k, st);
-        sponge(S0, S1, k, st);
+        a.sp[0] = G0;
+        a.sp[1] = G1;
+        a.sp[2] = S0;
+        a.sp[3] = S1;
+        a.src_f = S1;
+        a.src_val = wl + it;
+        a.src_sign = 1;
+        aux(a, k, st);
+        steps(true, G0, G1, k, S0, S1, k, d, it, 2, st);
         std::swap(S0, S1);
       }
     }
     g_swapped_ = G0 != gp0_.get();
+    geo_ = saved;
   }
 
   int arith_, nz_, nx_, nb_, nt_, ns_, ng_, nzpad_ = 0, nxpad_ = 0;
   int kmax_ = 1, adj_mode_ = SWFWI_PRTM_ADJ_REFERENCE;
-  bool serial_rec_ = false, g_swapped_ = false;
+  bool g_swapped_ = false, use_graphs_ = true;
   PrtmCoef c_{};
-  std::vector<int> spos_h_, rpos_h_;
+  PrtmGeo geo_{};
   DevBuf<float> vv_, wlt_, sponge_, sp0_, sp1_, gp0_, gp1_, gp2_, ring_, img_;
   DevBuf<int> spos_, rpos_;
+  std::vector<Graph> graphs_;
+  cudaStream_t cap_ = nullptr;
 };
 
 }  // namespace swfwi
@@ -540,6 +705,13 @@ extern "C" int swfwi_prtm2d_set_adjoint(swfwi_prtm *h, int mode) {
   return guarded([&] {
     SWFWI_REQUIRE(h && h->p, "null handle");
     h->p->set_adjoint_mode(mode);
+  });
+}
+
+extern "C" int swfwi_prtm2d_set_graphs(swfwi_prtm *h, int on) {
+  return guarded([&] {
+    SWFWI_REQUIRE(h && h->p, "null handle");
+    h->p->set_graphs(on != 0);
   });
 }
 
