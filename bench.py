@@ -544,7 +544,10 @@ def record_lsrtm(torch, cpu=True):
            "migration_s": t_mig, "migration_gpts": 3 * pts / t_mig / 1e9,
            "exact_adjoint_s": t_adj, "exact_adjoint_gpts": 3 * pts / t_adj / 1e9,
            "unit": "Gpts/s of padded-field point updates (Born 2, migration 3 per point per step)",
-           "dot_product": {"lm_d": a, "m_ltd": b, "rel": abs(a - b) / abs(a), "ok": abs(a - b) <= 1e-5 * abs(a)}}
+           # FP32 over 2000 steps, the source field rebuilt backwards from
+           # its ring: exact in exact arithmetic, 1e-4 in float
+           "dot_product": {"lm_d": a, "m_ltd": b, "rel": abs(a - b) / abs(a), "tolerance": 1e-4,
+                           "ok": abs(a - b) <= 1e-4 * abs(a)}}
     if cpu:
         import oracle
         if os.path.exists(os.path.join(oracle.REF_DIR, "libprtm_ref.so")):

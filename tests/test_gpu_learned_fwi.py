@@ -1,13 +1,17 @@
-"""What the trained preconditioner gains over plain FWI, on a held-out
-seeded model (the measurement itself, at full size and over several
-models, is `bench.py --mode learned`)."""
+"""The trained preconditioner on a held-out seeded model: training lowers
+its loss, learned steps are accepted, and the learned run keeps lowering the
+model error to the plain run's level.  No wall-clock gain is asserted: at
+this size the measured per-model ratios (plain / learned seconds to the
+plain run's best error) are 0.89x, 2.70x and 0.71x on held-out seeds
+200-202, so a gain is not expected on every model; ``bench.py`` records the
+per-model figures and their geometric mean."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def test_learned_fwi_against_plain(cuda):
+def test_learned_fwi_trains_and_reaches_plain_error_level(cuda):
     from swfwi_b200 import precond as P
     s = P.demo_survey(nt=1000).scaled(maxdv=100.0)
     iters = 15
@@ -23,7 +27,7 @@ def test_learned_fwi_against_plain(cuda):
           f"{'%.2f s' % r['learned_s'] if r['learned_s'] else 'not reached'}; "
           f"learned steps {accepted}/{tried}; wall-clock ratio {ratio}")
     assert accepted >= 1
-    # every epoch keeps the objective falling, so the learned run reaches
-    # the plain run's error level within the same epoch budget
+    # every epoch keeps the objective falling, so the learned run gets to
+    # within 10 % of the plain run's best error in the same epoch budget
     assert min(learned_errs) <= 1.10 * plain_best
     assert learned_errs[-1] < r["initial_error"]
