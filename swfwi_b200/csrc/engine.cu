@@ -577,28 +577,26 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
       reinterpret_cast<long long>(w.strips.get()), reinterpret_cast<long long>(w.qstrips.get()),
       reinterpret_cast<long long>(w.qscale.get())};
   loop_key_common(key);
+  const bool qstrips = save_strips && sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32;
   run_loop(0, (double)n * nxpad * nzpad, key, [&] {
+  // addSource -> stepForward -> swap -> recordSeis / writeBndry
+  // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144); the record, the FP32
+  // strips and the next step's addSource share one launch
+  launch_inject<T>(p1, fstride, n, src, vals, slot_stride, i_stride, +1, st_);
   for (int it = 0; it < nt; it++) {
-    // addSource -> stepForward -> swap -> recordSeis / writeBndry
-    // (damp4t10d.cpp:283-288, fwiframework.cpp:137-144)
-    launch_inject<T>(p1, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
-                     +1, st_);
     step_fields(ar, true, p0, p1, velrcp, n);
     std::swap(p0, p1);
-    if (dcal)
-      launch_record<T>(dcal + (long long)it * ngrec, (long long)nt * ngrec, p0, fstride, n, rec, st_);
-    if (save_strips) {
-      if (sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32)
-        launch_strip_write_q(strip_format, w.qstrips.get() + (long long)it * bsize, bstride,
-                             w.qscale.get() + it, nt, reinterpret_cast<const float *>(p0), fstride, n,
-                             nxpad, nzpad, bx0, pitch, st_);
-      else
-        launch_strip_write<T>(w.strips.get() + (long long)it * bsize, bstride, p0, fstride, n, nxpad,
-                              nzpad, bx0, pitch, st_);
-      if (sizeof(T) == 4 && illum && it % std::max(illum_every, 1) == 0)
-        launch_illum_accum(illum, reinterpret_cast<const float *>(p0), fstride, n, nxpad, nzpad, pitch,
-                           st_);
-    }
+    const bool more = it + 1 < nt;
+    launch_after_forward<T>(dcal ? dcal + (long long)it * ngrec : nullptr, (long long)nt * ngrec, p0, rec,
+                            save_strips && !qstrips ? w.strips.get() + (long long)it * bsize : nullptr, bstride,
+                            nxpad, nzpad, bx0, pitch, more ? p1 : nullptr, src,
+                            more ? vals + (long long)(it + 1) * it_stride : nullptr, slot_stride, i_stride,
+                            fstride, n, st_);
+    if (qstrips)
+      launch_strip_write_q(strip_format, w.qstrips.get() + (long long)it * bsize, bstride, w.qscale.get() + it,
+                           nt, reinterpret_cast<const float *>(p0), fstride, n, nxpad, nzpad, bx0, pitch, st_);
+    if (save_strips && sizeof(T) == 4 && illum && it % std::max(illum_every, 1) == 0)
+      launch_illum_accum(illum, reinterpret_cast<const float *>(p0), fstride, n, nxpad, nzpad, pitch, st_);
   }
   });
   // leave the final (current, next) pair for a backward sweep: every step
@@ -702,10 +700,8 @@ bool Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
                            nzpad, bx0, pitch, st_);
     std::swap(sp0, sp1);
     step_fields(ar, false, sp0, sp1, velrcp, n);
-    launch_inject<T>(sp0, fstride, n, src, vals + (long long)it * it_stride, slot_stride, i_stride,
-                     -1, st_);
-    launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1,
-                     +1, st_);
+    launch_inject2<T>(sp0, src, vals + (long long)it * it_stride, slot_stride, i_stride, -1, gp1, rec,
+                      vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1, +1, fstride, n, st_);
     step_fields(ar, true, gp0, gp1, velrcp, n);
     std::swap(gp0, gp1);
     float t = dt * (float)it;

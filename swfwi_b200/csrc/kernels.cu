@@ -144,6 +144,97 @@ void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long
   note_launch();
 }
 
+// ---------------------------------------------------------------- fused small steps
+// The point work around one stencil step, in one launch instead of up to
+// three.  After a forward step: record the current field, save its FP32
+// strips, and add the next step's source into the other field
+// (FwiForwardModeling and calgradient's forward, damp4t10d.cpp:283-288,
+// fwiframework.cpp:137-144).  The first two read `cur`, the third writes
+// `next`, so the three commute; each element is the same single operation
+// as in k_record, k_strip and k_inject.  Grid (blocks over the longest of
+// the three lists, slots).
+template <typename T>
+__global__ void k_after_forward(T *seis, long long seis_slot_stride, const T *cur, PointSet rec, T *bndr,
+                                long long bndr_slot_stride, int bs, int nx, int nz, int bx0, int pitch, T *next,
+                                PointSet src, const T *vals, long long val_slot_stride, int val_stride,
+                                long long shot_stride) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, slot = blockIdx.y;
+  const long long off = (long long)slot * shot_stride;
+  if (seis && i < rec.per_shot) {
+    const int shot = rec.slot_shot ? rec.slot_shot[slot] : slot;
+    const int p = rec.pos[(long long)shot * rec.per_shot + i];
+    seis[(long long)slot * seis_slot_stride + i] = p < 0 ? T(0) : cur[off + p];
+  }
+  if (bndr && i < bs) bndr[(long long)slot * bndr_slot_stride + i] = cur[off + strip_index(i, nx, nz, bx0, pitch)];
+  if (next && i < src.per_shot) {
+    const int shot = src.slot_shot ? src.slot_shot[slot] : slot;
+    const int p = src.pos[(long long)shot * src.per_shot + i];
+    if (p >= 0) {
+      T *f = next + off + p;
+      *f = exact_add<T>(*f, vals[(long long)slot * val_slot_stride + (long long)i * val_stride]);
+    }
+  }
+}
+
+template <typename T>
+void launch_after_forward(T *seis, long long seis_slot_stride, const T *cur, PointSet rec, T *bndr,
+                          long long bndr_slot_stride, int nx, int nz, int bx0, int pitch, T *next, PointSet src,
+                          const T *vals, long long val_slot_stride, int val_stride, long long shot_stride,
+                          int nslots, cudaStream_t st) {
+  if (nslots <= 0) return;
+  const int bs = bndr ? strip_size(nx, nz, bx0) : 0;
+  const int nr = seis ? rec.per_shot : 0, ni = next ? src.per_shot : 0;
+  const int most = nr > bs ? (nr > ni ? nr : ni) : (bs > ni ? bs : ni);
+  if (most <= 0) return;
+  const dim3 g(grid_for(most, 128), nslots);
+  k_after_forward<T><<<g, 128, 0, st>>>(seis, seis_slot_stride, cur, rec, bndr, bndr_slot_stride, bs, nx, nz, bx0,
+                                        pitch, next, src, vals, val_slot_stride, val_stride, shot_stride);
+  note_launch();
+}
+
+// Two injections into two different fields in one launch (calgradient's
+// backward step, fwiframework.cpp:152-160: subSource on the back-stepped
+// source field, addSource of the residual on the receiver field).  The same
+// single float operation per point as k_inject.
+template <typename T>
+__global__ void k_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a,
+                          T *fb, PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
+                          long long shot_stride) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, slot = blockIdx.y;
+  const long long off = (long long)slot * shot_stride;
+  if (i < pa.per_shot) {
+    const int shot = pa.slot_shot ? pa.slot_shot[slot] : slot;
+    const int p = pa.pos[(long long)shot * pa.per_shot + i];
+    if (p >= 0) {
+      const T v = va[(long long)slot * va_slot_stride + (long long)i * va_stride];
+      T *f = fa + off + p;
+      *f = sign_a > 0 ? exact_add<T>(*f, v) : exact_sub<T>(*f, v);
+    }
+  }
+  if (i < pb.per_shot) {
+    const int shot = pb.slot_shot ? pb.slot_shot[slot] : slot;
+    const int p = pb.pos[(long long)shot * pb.per_shot + i];
+    if (p >= 0) {
+      const T v = vb[(long long)slot * vb_slot_stride + (long long)i * vb_stride];
+      T *f = fb + off + p;
+      *f = sign_b > 0 ? exact_add<T>(*f, v) : exact_sub<T>(*f, v);
+    }
+  }
+}
+
+template <typename T>
+void launch_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a, T *fb,
+                    PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
+                    long long shot_stride, int nslots, cudaStream_t st) {
+  if (nslots <= 0) return;
+  const int most = pa.per_shot > pb.per_shot ? pa.per_shot : pb.per_shot;
+  if (most <= 0) return;
+  const dim3 g(grid_for(most, 128), nslots);
+  k_inject2<T><<<g, 128, 0, st>>>(fa, pa, va, va_slot_stride, va_stride, sign_a, fb, pb, vb, vb_slot_stride,
+                                  vb_stride, sign_b, shot_stride);
+  note_launch();
+}
+
 // ---------------------------------------------------------------- image
 template <typename T>
 __global__ void k_image(T *image, long long image_stride, const T *s, const T *r,
@@ -911,6 +1002,16 @@ void launch_strip_read_q(int format, const uint16_t *q, long long q_slot_stride,
   note_launch();
 }
 
+template void launch_after_forward<float>(float *, long long, const float *, PointSet, float *, long long, int,
+                                          int, int, int, float *, PointSet, const float *, long long, int,
+                                          long long, int, cudaStream_t);
+template void launch_after_forward<double>(double *, long long, const double *, PointSet, double *, long long,
+                                           int, int, int, int, double *, PointSet, const double *, long long,
+                                           int, long long, int, cudaStream_t);
+template void launch_inject2<float>(float *, PointSet, const float *, long long, int, int, float *, PointSet,
+                                    const float *, long long, int, int, long long, int, cudaStream_t);
+template void launch_inject2<double>(double *, PointSet, const double *, long long, int, int, double *, PointSet,
+                                     const double *, long long, int, int, long long, int, cudaStream_t);
 template void launch_strip_write<float>(float *, long long, const float *, long long, int, int, int,
                                         int, int, cudaStream_t);
 template void launch_strip_write<double>(double *, long long, const double *, long long, int, int,

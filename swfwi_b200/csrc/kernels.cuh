@@ -37,6 +37,22 @@ template <typename T>
 void launch_record(T *seis, long long seis_slot_stride, const T *field, long long shot_stride,
                    int nslots, PointSet ps, cudaStream_t st);
 
+// After a forward step, in one launch: seis[slot*seis_slot_stride + i] =
+// cur[slot][rec pos] (record; seis NULL: none), the FP32 strips of cur into
+// bndr (NULL: none), and next[slot][src pos] += vals (next NULL: none).  The
+// same per-element operations as launch_record, launch_strip_write and
+// launch_inject, which they replace when cur and next are different fields.
+template <typename T>
+void launch_after_forward(T *seis, long long seis_slot_stride, const T *cur, PointSet rec, T *bndr,
+                          long long bndr_slot_stride, int nx, int nz, int bx0, int pitch, T *next, PointSet src,
+                          const T *vals, long long val_slot_stride, int val_stride, long long shot_stride,
+                          int nslots, cudaStream_t st);
+// Two launch_inject calls on two different fields in one launch.
+template <typename T>
+void launch_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a, T *fb,
+                    PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
+                    long long shot_stride, int nslots, cudaStream_t st);
+
 // Boundary strips (writeBndry/readBndry, damp4t10d.cpp:478-536) for all
 // slots at one time step.  bndr layout [slot][bndr_slot_stride], one step's
 // strip of strip_size(nx,nz,bx0) values at offset it*strip_size.
