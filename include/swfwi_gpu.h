@@ -111,8 +111,10 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
  * (band depth 120, rows ahead 3 or 7); kernel 1 = warp-specialised
  * streaming step (band depth 120, 248 or 376 = 1-3 consumer warps plus a
  * copy warp, rows ahead 3 or 7; the fused time loop always uses it);
- * rows per CTA >= 1; shots_slowest = 1 runs the CTAs of one shot together
- * (kernel 1). */
+ * rows per CTA >= 1, or 0 (default): kernel 5 takes the longest task (at
+ * least 8 rows) with which every (shot, depth slice) column's tasks fit in
+ * one wave of resident warps, kernel 1 takes 64; shots_slowest = 1 runs the CTAs of one
+ * shot together (kernel 1). */
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest);
 /* Fused backward time loop (default off): where sources and receivers form

@@ -3,7 +3,8 @@
 The streaming step (``stream.cuh``) has knobs that do not change its
 results: which kernel (register-queue warps, each a self-contained TMA
 pipeline; or warp-specialised CTAs with a copy warp), output depths per
-CTA, rows per task, rows in flight ahead of the compute and the launch
+CTA, rows per task (0: the register-queue kernel's automatic length, one
+wave of tasks), rows in flight ahead of the compute and the launch
 order (shots slowest or fastest).  ``tune`` times short batched forward runs of a survey for each
 candidate with the library's CUDA-event step timing and returns the fastest;
 ``apply`` sets it on a propagator.
@@ -14,7 +15,7 @@ import itertools
 
 import numpy as np
 
-DEFAULT = {"kernel": 5, "band_depth": 120, "rows_per_cta": 48, "rows_in_flight": 3,
+DEFAULT = {"kernel": 5, "band_depth": 120, "rows_per_cta": 0, "rows_in_flight": 3,
            "shots_slowest": False}
 
 
@@ -22,7 +23,7 @@ def candidates(nz: int):
     """The register-queue kernel's task lengths and prefetch depths, the
     warp-specialised kernel's band depths, chunk lengths, prefetch depths
     and launch orders."""
-    for rows, depth in itertools.product((24, 32, 48, 64), (3, 7)):
+    for rows, depth in itertools.product((0, 32, 48, 64), (3, 7)):
         yield {"kernel": 5, "band_depth": 120, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": False}
     for bz, rows, depth, order in itertools.product((248, 376), (48, 64), (3, 7), (False, True)):
@@ -38,7 +39,7 @@ def valid(cfg: dict) -> bool:
         ok_bz = cfg["band_depth"] in (120, 248, 376)
     else:
         return False
-    return ok_bz and cfg["rows_in_flight"] in (3, 7) and cfg["rows_per_cta"] >= 1
+    return ok_bz and cfg["rows_in_flight"] in (3, 7) and cfg["rows_per_cta"] >= 0
 
 
 def time_config(method, wlt, dcal, ids, cfg, repeats=2) -> float:

@@ -225,7 +225,7 @@ int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, i
                     "band depth must be 120, 248 or 376");
     }
     SWFWI_REQUIRE(rows_in_flight == 3 || rows_in_flight == 7, "rows in flight must be 3 or 7");
-    SWFWI_REQUIRE(rows_per_cta >= 1, "rows per CTA must be positive");
+    SWFWI_REQUIRE(rows_per_cta >= 0, "rows per CTA must be 0 (automatic) or positive");
     P(h).stream_kernel = kernel;
     P(h).stream_bz = band_depth;
     P(h).stream_xchunk = rows_per_cta;

@@ -376,11 +376,12 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   a.err = d_err_.get();
   if (epi) {
     // the fused step is the warp-specialised kernel with 376-deep bands
-    if (stream_kernel != 1) a.xchunk = 64;
+    if (stream_kernel != 1 || a.xchunk <= 0) a.xchunk = 64;
     launch_ws_step(ar, damped, 376, stream_kernel == 1 ? stream_depth : 3, a, n, st_);
   } else if (stream_kernel == 5) {
-    launch_rq_step(ar, damped, stream_depth, a, n, st_);
+    launch_rq_step(ar, damped, stream_depth, a, n, st_);   // xchunk 0: automatic
   } else {
+    if (a.xchunk <= 0) a.xchunk = 64;
     launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   }
   if (done) SWFWI_CUDA(cudaEventRecord(done, st_));

@@ -79,7 +79,7 @@ class Propagator {
   int strip_format = SWFWI_STRIP_F32;
   int stream_kernel = 5;      // 1: warp-specialised, 5: register-queue warps
   int stream_bz = 120;        // output depths per CTA (120 for kernel 5; 120, 248 or 376 for kernel 1)
-  int stream_xchunk = 48;     // rows per CTA (per warp task for kernel 5)
+  int stream_xchunk = 0;      // rows per CTA (per warp task for kernel 5); 0: automatic
   int stream_depth = 3;       // rows ahead (3 or 7)
   int stream_shot_major = 0;  // launch order: 0 = shots fastest
   bool fuse = false;          // fused time loops where they apply

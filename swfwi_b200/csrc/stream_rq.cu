@@ -1,5 +1,6 @@
 // Launcher of the register-queue streaming step (stream_rq.cuh); its own
 // translation unit so it compiles beside kernels.cu.
+#include <algorithm>
 #include "common.hpp"
 #include "kernels.cuh"
 #include "stream_rq.cuh"
@@ -17,11 +18,33 @@ void rq_t(const StreamArgs &a, int nslots, cudaStream_t st) {
                          (int)smem);
     attr_set = true;
   }
-  const long long nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
-  const long long tasks = (long long)nslots * rq_detail::slices(a.nz) * nchunks;
+  StreamArgs b = a;
+  const long long pairs = (long long)nslots * rq_detail::slices(a.nz);   // (shot, depth slice) columns
+  if (b.xchunk <= 0) {
+    // automatic task length: the longest chunk of rows with which every
+    // column's tasks fit in one wave of resident warps (a partial last wave
+    // costs a whole task duration; shorter tasks spend more of their steps
+    // filling the register queue)
+    static int per_sm = 0, sms = 0;
+    if (!per_sm) {
+      int dev = 0;
+      SWFWI_CUDA(cudaGetDevice(&dev));
+      SWFWI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      SWFWI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fd_step_rq<ARITH, DAMPED, NW, D>, NW * 32,
+                                                               smem));
+      per_sm = std::max(per_sm, 1);
+    }
+    const long long resident = (long long)per_sm * NW * sms;
+    const long long per_column = std::max<long long>(1, resident / pairs);
+    // at least 8 rows: a task fills its queue with 12 stages before its
+    // first output
+    b.xchunk = std::max(8, (int)((a.nx - 12 + per_column - 1) / per_column));
+  }
+  const long long nchunks = (b.nx - 12 + b.xchunk - 1) / b.xchunk;
+  const long long tasks = pairs * nchunks;
   const long long blocks = (tasks + NW - 1) / NW;
   if (blocks > 0x7fffffffLL) throw Error(SWFWI_ERR_BAD_ARG, "too many stencil tasks for one launch");
-  fd_step_rq<ARITH, DAMPED, NW, D><<<(unsigned)blocks, NW * 32, smem, st>>>(a, nslots);
+  fd_step_rq<ARITH, DAMPED, NW, D><<<(unsigned)blocks, NW * 32, smem, st>>>(b, nslots);
 }
 
 // One warp per CTA: the warps' tasks are independent, and a one-warp CTA
@@ -38,7 +61,6 @@ void rq_d(int depth, const StreamArgs &a, int nslots, cudaStream_t st) {
 
 void launch_rq_step(int arith, bool damped, int depth, const StreamArgs &a, int nslots, cudaStream_t st) {
   if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
-  if (a.xchunk <= 0) throw Error(SWFWI_ERR_BAD_ARG, "rows per task must be positive");
   if (arith == ARITH_REF) {
     if (damped) rq_d<ARITH_REF, true>(depth, a, nslots, st);
     else rq_d<ARITH_REF, false>(depth, a, nslots, st);

@@ -192,7 +192,8 @@ def test_errors_reported(cuda):
     (1, 120, 1, 3, 1), (1, 248, 9, 7, 0), (1, 376, 64, 7, 0), (1, 376, 3, 3, 1), (1, 120, 200, 7, 0),
     (1, 376, 16, 3, 0), (1, 248, 33, 3, 1),
     (5, 120, 1, 3, 0), (5, 120, 9, 7, 0), (5, 120, 64, 3, 0), (5, 120, 33, 7, 0), (5, 120, 200, 3, 0),
-    (5, 120, 11, 3, 0), (5, 120, 12, 7, 0), (5, 120, 8, 3, 0), (5, 120, 16, 7, 0)])
+    (5, 120, 11, 3, 0), (5, 120, 12, 7, 0), (5, 120, 8, 3, 0), (5, 120, 16, 7, 0),
+    (5, 120, 0, 3, 0), (5, 120, 0, 7, 0), (1, 376, 0, 3, 0)])
 def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     # every band depth / chunk length of the streaming stencil gives the
     # reference's seismogram bit for bit
