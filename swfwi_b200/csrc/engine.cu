@@ -710,9 +710,10 @@ bool Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
     if ((double)t > 0.4) scale = 1.0f;
     else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
     else break;
-    if (summed)
+    if (summed)   // only the gradient's unmasked region (maskGradient, damp4t10d.cpp:216-226) is used
       launch_image_sum(reinterpret_cast<float *>(w.image.get()) + kStreamCoff, reinterpret_cast<const float *>(sp0),
-                       reinterpret_cast<const float *>(gp0), fstride, n, npts, scale, st_);
+                       reinterpret_cast<const float *>(gp0), fstride, n, bx0, nxpad - bxn, bz0, nzpad - bzn, pitch,
+                       scale, st_);
     else
       launch_image<T>(w.image.get() + kStreamCoff, fstride, sp0, gp0, fstride, n, npts, scale, st_);
   }

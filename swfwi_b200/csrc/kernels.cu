@@ -257,14 +257,16 @@ __global__ void k_image(T *image, long long image_stride, const T *s, const T *r
 // a thread; one image read-modify-write for all slots.  n % 4 == 0 and
 // every array 16-byte aligned.
 __global__ void __launch_bounds__(kThreads)
-k_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, long long n4,
-            float scale) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n4;
-       q += (long long)gridDim.x * blockDim.x) {
+k_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int x0, int nrows,
+            int g0, int ngroups, int pitch4, float scale) {
+  const int n = nrows * ngroups;
+  const long long st4 = shot_stride / 4;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int row = q / ngroups;
+    const long long e = (long long)(x0 + row) * pitch4 + g0 + (q - row * ngroups);   // float4 index
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 *a = reinterpret_cast<const float4 *>(s) + q;
-    const float4 *b = reinterpret_cast<const float4 *>(r) + q;
-    const long long st4 = shot_stride / 4;
+    const float4 *a = reinterpret_cast<const float4 *>(s) + e;
+    const float4 *b = reinterpret_cast<const float4 *>(r) + e;
 #pragma unroll 8
     for (int slot = 0; slot < nslots; slot++) {
       const float4 x = __ldcs(a + slot * st4), y = __ldcs(b + slot * st4);
@@ -273,7 +275,7 @@ k_image_sum(float *image, const float *s, const float *r, long long shot_stride,
       acc.z = fmaf(x.z, y.z, acc.z);
       acc.w = fmaf(x.w, y.w, acc.w);
     }
-    float4 *g = reinterpret_cast<float4 *>(image) + q;
+    float4 *g = reinterpret_cast<float4 *>(image) + e;
     float4 v = *g;
     v.x = __fsub_rn(v.x, __fmul_rn(acc.x, scale));
     v.y = __fsub_rn(v.y, __fmul_rn(acc.y, scale));
@@ -283,13 +285,16 @@ k_image_sum(float *image, const float *s, const float *r, long long shot_stride,
   }
 }
 
-void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int n,
-                      float scale, cudaStream_t st) {
-  if (n % 4 != 0 || shot_stride % 4 != 0 || (reinterpret_cast<uintptr_t>(image) | reinterpret_cast<uintptr_t>(s) |
-                                              reinterpret_cast<uintptr_t>(r)) % 16 != 0)
+void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int x0,
+                      int x1, int z0, int z1, int pitch, float scale, cudaStream_t st) {
+  if (pitch % 4 != 0 || shot_stride % 4 != 0 || (reinterpret_cast<uintptr_t>(image) |
+                                                  reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(r)) %
+                                                     16 != 0)
     throw Error(SWFWI_ERR_BAD_ARG, "summed image: sizes and arrays must be 16-byte aligned");
-  const long long n4 = n / 4;
-  k_image_sum<<<grid_for(n4), kThreads, 0, st>>>(image, s, r, shot_stride, nslots, n4, scale);
+  if (x1 <= x0 || z1 <= z0) return;
+  const int g0 = z0 / 4, ngroups = (z1 + 3) / 4 - g0, nrows = x1 - x0;
+  k_image_sum<<<grid_for((long long)nrows * ngroups), kThreads, 0, st>>>(image, s, r, shot_stride, nslots, x0,
+                                                                         nrows, g0, ngroups, pitch / 4, scale);
   note_launch();
 }
 

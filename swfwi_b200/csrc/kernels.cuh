@@ -83,10 +83,12 @@ void launch_image(T *image, long long image_stride, const T *s, const T *r, long
 // image -= (sum over slots of s[slot] * r[slot]) * scale: all slots'
 // cross-correlations into ONE image (FAST arithmetic; the slot terms are
 // added in slot order before the scale, so the bits differ from per-slot
-// images summed later).  n points from each array start, n % 4 == 0,
-// 16-byte aligned arrays and shot_stride.
-void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int n,
-                      float scale, cudaStream_t st);
+// images summed later), over rows [x0, x1) and depths [z0, z1) of the
+// pitched fields (depths widened to whole groups of 4; a caller that masks
+// the gradient passes the unmasked region).  16-byte aligned arrays, pitch
+// and shot_stride.
+void launch_image_sum(float *image, const float *s, const float *r, long long shot_stride, int nslots, int x0,
+                      int x1, int z0, int z1, int pitch, float scale, cudaStream_t st);
 
 // One FD step for all slots: the shared-memory tile form (any pitch, any
 // arithmetic; stencil.cuh).

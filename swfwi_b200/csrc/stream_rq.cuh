@@ -179,6 +179,9 @@ fd_step_rq(StreamArgs a, int nslots) {
   const float *damp_row = a.damp_x + xa - 12;   // damp_x of output row xa-12+k
   const float2 *coef_row = a.coef_x + xa - 12;  // its FAST coefficients
   const int k_ramp_lo = a.ramp - xa + 12, k_ramp_hi = nx - a.ramp - xa + 12;
+  // rows k_ramp_lo <= k < k_ramp_lo + ramp_span are off the ramps (none when
+  // the ramps overlap)
+  const unsigned ramp_span = (unsigned)max(k_ramp_hi - k_ramp_lo, 0);
 
   float4 q[11];   // own values of current rows (stages k-10 .. k after the push)
   float4 um = make_float4(0.f, 0.f, 0.f, 0.f), uc = um;   // u2 of the two previous rows
@@ -243,7 +246,10 @@ fd_step_rq(StreamArgs a, int nslots) {
         const float4 c4 = q[4];
         const float4 p4 = ld4(&S.p[SP][po]);
         const float4 r4 = ld4(&S.v[SP][po]);
-        const bool ramp_row = DAMPED && (k < k_ramp_lo || k >= k_ramp_hi);
+        // a left/right ramp row: one unsigned compare, marked unlikely (7 %
+        // of the rows on the benchmark grid), so the test stays a branch
+        const bool ramp_row =
+            __builtin_expect(DAMPED && (unsigned)(k - k_ramp_lo) >= ramp_span, 0);
         float4 o;
         if constexpr (ARITH == ARITH_FAST) {
           float2 cf0 = coefz[0], cf1 = coefz[1], pc0 = pcz[0], pc1 = pcz[1];
