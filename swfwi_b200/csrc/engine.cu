@@ -688,7 +688,14 @@ bool Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
   const bool summed = sum_images && sizeof(T) == 4 && ar == ARITH_FAST;
   key.push_back(summed ? 2 : 0);   // separate launches (2: one summed image)
   loop_key_common(key);
+  // With the summed image (interior cells only), step it-1's FP32 strip
+  // restore, which writes boundary cells of the field the source
+  // subtraction of step it writes, rides in that launch.
+  const bool fold_strips = summed && strip_format == SWFWI_STRIP_F32;
   run_loop(1, (double)n * nxpad * nzpad, key, [&] {
+  if (fold_strips)
+    launch_strip_read<T>(w.strips.get() + (long long)(nt - 1) * bsize, bstride, sp0, fstride, n, nxpad, nzpad, bx0,
+                         pitch, st_);
   for (int it = nt - 1; it >= 0; it--) {
     // fwiframework.cpp:146-176: readBndry -> swap -> stepBackward ->
     // subSource; receiver addSource -> stepForward -> swap; image.
@@ -696,13 +703,16 @@ bool Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
       launch_strip_read_q(strip_format, w.qstrips.get() + (long long)it * bsize, bstride,
                           w.qscale.get() + it, nt, reinterpret_cast<float *>(sp0), fstride, n, nxpad,
                           nzpad, bx0, pitch, st_);
-    else
+    else if (!fold_strips)
       launch_strip_read<T>(w.strips.get() + (long long)it * bsize, bstride, sp0, fstride, n, nxpad,
                            nzpad, bx0, pitch, st_);
     std::swap(sp0, sp1);
     step_fields(ar, false, sp0, sp1, velrcp, n);
+    const bool next_strip = fold_strips && it > 0;
     launch_inject2<T>(sp0, src, vals + (long long)it * it_stride, slot_stride, i_stride, -1, gp1, rec,
-                      vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1, +1, fstride, n, st_);
+                      vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1, +1, fstride, n, st_,
+                      next_strip ? w.strips.get() + (long long)(it - 1) * bsize : nullptr, bstride, nxpad, nzpad,
+                      bx0, pitch);
     step_fields(ar, true, gp0, gp1, velrcp, n);
     std::swap(gp0, gp1);
     float t = dt * (float)it;

@@ -158,20 +158,24 @@ __global__ void k_after_forward(T *seis, long long seis_slot_stride, const T *cu
                                 long long bndr_slot_stride, int bs, int nx, int nz, int bx0, int pitch, T *next,
                                 PointSet src, const T *vals, long long val_slot_stride, int val_stride,
                                 long long shot_stride) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, slot = blockIdx.y;
+  const int slot = blockIdx.y;
   const long long off = (long long)slot * shot_stride;
-  if (seis && i < rec.per_shot) {
-    const int shot = rec.slot_shot ? rec.slot_shot[slot] : slot;
-    const int p = rec.pos[(long long)shot * rec.per_shot + i];
-    seis[(long long)slot * seis_slot_stride + i] = p < 0 ? T(0) : cur[off + p];
-  }
-  if (bndr && i < bs) bndr[(long long)slot * bndr_slot_stride + i] = cur[off + strip_index(i, nx, nz, bx0, pitch)];
-  if (next && i < src.per_shot) {
-    const int shot = src.slot_shot ? src.slot_shot[slot] : slot;
-    const int p = src.pos[(long long)shot * src.per_shot + i];
-    if (p >= 0) {
-      T *f = next + off + p;
-      *f = exact_add<T>(*f, vals[(long long)slot * val_slot_stride + (long long)i * val_stride]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x;; i += gridDim.x * blockDim.x) {
+    const bool r = seis && i < rec.per_shot, b = bndr && i < bs, n = next && i < src.per_shot;
+    if (!(r || b || n)) return;
+    if (r) {
+      const int shot = rec.slot_shot ? rec.slot_shot[slot] : slot;
+      const int p = rec.pos[(long long)shot * rec.per_shot + i];
+      seis[(long long)slot * seis_slot_stride + i] = p < 0 ? T(0) : cur[off + p];
+    }
+    if (b) bndr[(long long)slot * bndr_slot_stride + i] = cur[off + strip_index(i, nx, nz, bx0, pitch)];
+    if (n) {
+      const int shot = src.slot_shot ? src.slot_shot[slot] : slot;
+      const int p = src.pos[(long long)shot * src.per_shot + i];
+      if (p >= 0) {
+        T *f = next + off + p;
+        *f = exact_add<T>(*f, vals[(long long)slot * val_slot_stride + (long long)i * val_stride]);
+      }
     }
   }
 }
@@ -186,7 +190,9 @@ void launch_after_forward(T *seis, long long seis_slot_stride, const T *cur, Poi
   const int nr = seis ? rec.per_shot : 0, ni = next ? src.per_shot : 0;
   const int most = nr > bs ? (nr > ni ? nr : ni) : (bs > ni ? bs : ni);
   if (most <= 0) return;
-  const dim3 g(grid_for(most, 128), nslots);
+  // four elements a thread: these launches are latency-bound, fewer and
+  // fuller blocks finish sooner
+  const dim3 g(grid_for(most, 512), nslots);
   k_after_forward<T><<<g, 128, 0, st>>>(seis, seis_slot_stride, cur, rec, bndr, bndr_slot_stride, bs, nx, nz, bx0,
                                         pitch, next, src, vals, val_slot_stride, val_stride, shot_stride);
   note_launch();
@@ -199,9 +205,13 @@ void launch_after_forward(T *seis, long long seis_slot_stride, const T *cur, Poi
 template <typename T>
 __global__ void k_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a,
                           T *fb, PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
-                          long long shot_stride) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, slot = blockIdx.y;
+                          long long shot_stride, const T *bndr, long long bndr_slot_stride, int bs, int nx, int nz,
+                          int bx0, int pitch) {
+  const int slot = blockIdx.y;
   const long long off = (long long)slot * shot_stride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bs || i < pa.per_shot || i < pb.per_shot;
+       i += gridDim.x * blockDim.x) {
+  if (bndr && i < bs) fa[off + strip_index(i, nx, nz, bx0, pitch)] = bndr[(long long)slot * bndr_slot_stride + i];
   if (i < pa.per_shot) {
     const int shot = pa.slot_shot ? pa.slot_shot[slot] : slot;
     const int p = pa.pos[(long long)shot * pa.per_shot + i];
@@ -220,18 +230,22 @@ __global__ void k_inject2(T *fa, PointSet pa, const T *va, long long va_slot_str
       *f = sign_b > 0 ? exact_add<T>(*f, v) : exact_sub<T>(*f, v);
     }
   }
+  }
 }
 
 template <typename T>
 void launch_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a, T *fb,
                     PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
-                    long long shot_stride, int nslots, cudaStream_t st) {
+                    long long shot_stride, int nslots, cudaStream_t st, const T *bndr, long long bndr_slot_stride,
+                    int nx, int nz, int bx0, int pitch) {
   if (nslots <= 0) return;
-  const int most = pa.per_shot > pb.per_shot ? pa.per_shot : pb.per_shot;
+  const int bs = bndr ? strip_size(nx, nz, bx0) : 0;
+  int most = pa.per_shot > pb.per_shot ? pa.per_shot : pb.per_shot;
+  most = most > bs ? most : bs;
   if (most <= 0) return;
-  const dim3 g(grid_for(most, 128), nslots);
+  const dim3 g(grid_for(most, 512), nslots);
   k_inject2<T><<<g, 128, 0, st>>>(fa, pa, va, va_slot_stride, va_stride, sign_a, fb, pb, vb, vb_slot_stride,
-                                  vb_stride, sign_b, shot_stride);
+                                  vb_stride, sign_b, shot_stride, bndr, bndr_slot_stride, bs, nx, nz, bx0, pitch);
   note_launch();
 }
 
@@ -1014,9 +1028,11 @@ template void launch_after_forward<double>(double *, long long, const double *, 
                                            int, int, int, int, double *, PointSet, const double *, long long,
                                            int, long long, int, cudaStream_t);
 template void launch_inject2<float>(float *, PointSet, const float *, long long, int, int, float *, PointSet,
-                                    const float *, long long, int, int, long long, int, cudaStream_t);
+                                    const float *, long long, int, int, long long, int, cudaStream_t,
+                                    const float *, long long, int, int, int, int);
 template void launch_inject2<double>(double *, PointSet, const double *, long long, int, int, double *, PointSet,
-                                     const double *, long long, int, int, long long, int, cudaStream_t);
+                                     const double *, long long, int, int, long long, int, cudaStream_t,
+                                     const double *, long long, int, int, int, int);
 template void launch_strip_write<float>(float *, long long, const float *, long long, int, int, int,
                                         int, int, cudaStream_t);
 template void launch_strip_write<double>(double *, long long, const double *, long long, int, int,

@@ -47,11 +47,14 @@ void launch_after_forward(T *seis, long long seis_slot_stride, const T *cur, Poi
                           long long bndr_slot_stride, int nx, int nz, int bx0, int pitch, T *next, PointSet src,
                           const T *vals, long long val_slot_stride, int val_stride, long long shot_stride,
                           int nslots, cudaStream_t st);
-// Two launch_inject calls on two different fields in one launch.
+// Two launch_inject calls on two different fields in one launch; with
+// bndr, also the FP32 strip restore (launch_strip_read) of bndr into fa,
+// whose strip cells are disjoint from its source cells.
 template <typename T>
 void launch_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a, T *fb,
                     PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
-                    long long shot_stride, int nslots, cudaStream_t st);
+                    long long shot_stride, int nslots, cudaStream_t st, const T *bndr = nullptr,
+                    long long bndr_slot_stride = 0, int nx = 0, int nz = 0, int bx0 = 0, int pitch = 0);
 
 // Boundary strips (writeBndry/readBndry, damp4t10d.cpp:478-536) for all
 // slots at one time step.  bndr layout [slot][bndr_slot_stride], one step's
