@@ -126,9 +126,10 @@ int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, i
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on);
 /* CUDA graphs for the forward and backward time loops: on = 0 never, 1
  * (default) while a step covers at most 8e6 points (fields x nxpad x
- * nzpad), 2 for every step size.  From a loop's second use, and while
- * stencil timing is off, the loop is captured on a private stream and
- * replayed on the propagator's stream.  Same kernels, same results. */
+ * nzpad), 2 for every step size.  From a loop's second use the loop is
+ * captured on a private stream and replayed on the propagator's stream
+ * (one graph per loop and setting, stencil timing included).  Same
+ * kernels, same results. */
 int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on);
 /* Per-shot receiver lists (uneven spreads; not in the reference, whose
  * ShotPosition is one common line): shot s has receivers
@@ -367,9 +368,10 @@ int swfwi_fwi_last_trials(const swfwi_fwi *h, int *trials);
  * (interior point-updates; bytes = 12 per point-update plus 4 per point per
  * velocity model read) with CUDA-event timing, on the launch's own stream,
  * of every on-th stencil launch (on = 1: all of them).
- * kernel_launches counts launches issued from the host: a time loop replayed
- * as a CUDA graph (swfwi_damp4t10d_set_graphs) is counted when captured, not
- * again per replay; stencil timing turns the replay off.
+ * kernel_launches counts kernel launches: a time loop replayed as a CUDA
+ * graph (swfwi_damp4t10d_set_graphs) counts the kernels it holds at every
+ * replay; its timed stencil launches are bracketed by event nodes in the
+ * graph, their times added after each replay completes.
  * step_ms is the timed launches' total: their mean is step_ms /
  * step_timed_launches.
  * ---------------------------------------------------------------------- */

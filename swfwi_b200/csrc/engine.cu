@@ -20,17 +20,42 @@ StepTimer &step_timer() {
   return t;
 }
 
+StepTimer::Capture::~Capture() {
+  for (auto &e : pairs) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+}
+
 void StepTimer::reset() {
   std::lock_guard<std::mutex> g(mu);
   used = 0;
   launches = 0;
   points = bytes = 0;
+  graph_ms = 0;
+  graph_timed = 0;
+  for (Capture *c : replayed) c->pending = false;   // launched before the reset: not counted
+  replayed.clear();
   g_kernel_launches.store(0);
+}
+
+void StepTimer::harvest(Capture *c) {
+  if (!c->pending) return;
+  for (auto &e : c->pairs) {
+    SWFWI_CUDA(cudaEventSynchronize(e.second));
+    float t = 0;
+    SWFWI_CUDA(cudaEventElapsedTime(&t, e.first, e.second));
+    graph_ms += t;
+  }
+  graph_timed += (long long)c->pairs.size();
+  c->pending = false;
 }
 
 void StepTimer::read(double &ms, long long &n, double &pts, double &b, long long &timed) {
   std::lock_guard<std::mutex> g(mu);
-  ms = 0;
+  for (Capture *c : replayed) harvest(c);
+  replayed.clear();
+  ms = graph_ms;
   for (size_t i = 0; i < used; i++) {
     SWFWI_CUDA(cudaEventSynchronize(pool[i].second));
     float t = 0;
@@ -40,20 +65,31 @@ void StepTimer::read(double &ms, long long &n, double &pts, double &b, long long
   n = launches;
   pts = points;
   b = bytes;
-  timed = (long long)used;
+  timed = (long long)used + graph_timed;
 }
 
 // Algorithmic work of one step launch: every interior point of every field
 // is updated (read current and previous, write next: 3 elements), and each
-// velocity model the launch uses is read once.
+// velocity model the launch uses is read once.  Inside a capture the work
+// goes to the capture (added per replay) and a timed launch gets its own
+// event pair, recorded as graph nodes.
 cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el) {
   if (!enabled.load(std::memory_order_relaxed)) return nullptr;
   std::lock_guard<std::mutex> g(mu);
-  const long long k = launches++;
-  points += pts * n;
-  bytes += pts * n * 3 * el + pts * el * nvel;
+  Capture *c = capturing;
+  const long long k = c ? c->launches++ : launches++;
+  (c ? c->points : points) += pts * n;
+  (c ? c->bytes : bytes) += pts * n * 3 * el + pts * el * nvel;
   const int per = std::max(period.load(std::memory_order_relaxed), 1);
   if (k % per != 0) return nullptr;
+  if (c) {
+    cudaEvent_t x, y;
+    SWFWI_CUDA(cudaEventCreate(&x));
+    SWFWI_CUDA(cudaEventCreate(&y));
+    c->pairs.emplace_back(x, y);
+    SWFWI_CUDA(cudaEventRecordWithFlags(x, st, cudaEventRecordExternal));
+    return y;
+  }
   if (used == pool.size()) {
     cudaEvent_t x, y;
     SWFWI_CUDA(cudaEventCreate(&x));
@@ -63,6 +99,47 @@ cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el
   auto ev = pool[used++];
   SWFWI_CUDA(cudaEventRecord(ev.first, st));
   return ev.second;
+}
+
+void StepTimer::close(cudaEvent_t done, cudaStream_t st) {
+  if (!done) return;
+  if (capturing) SWFWI_CUDA(cudaEventRecordWithFlags(done, st, cudaEventRecordExternal));
+  else SWFWI_CUDA(cudaEventRecord(done, st));
+}
+
+void StepTimer::begin_capture(Capture *c) {
+  std::lock_guard<std::mutex> g(mu);
+  capturing = c;
+  capture_notes0_ = g_kernel_launches.load();
+}
+
+void StepTimer::end_capture() {
+  std::lock_guard<std::mutex> g(mu);
+  if (capturing) {
+    capturing->kernels = g_kernel_launches.load() - capture_notes0_;
+    g_kernel_launches.fetch_sub(capturing->kernels);
+  }
+  capturing = nullptr;
+}
+
+void StepTimer::replay(Capture *c) {
+  std::lock_guard<std::mutex> g(mu);
+  harvest(c);   // the previous replay's times, before this one overwrites them
+  launches += c->launches;
+  points += c->points;
+  bytes += c->bytes;
+  g_kernel_launches.fetch_add(c->kernels);
+  if (!c->pairs.empty()) {
+    c->pending = true;
+    if (std::find(replayed.begin(), replayed.end(), c) == replayed.end()) replayed.push_back(c);
+  }
+}
+
+void StepTimer::forget(Capture *c) {
+  std::lock_guard<std::mutex> g(mu);
+  harvest(c);
+  replayed.erase(std::remove(replayed.begin(), replayed.end(), c), replayed.end());
+  if (capturing == c) capturing = nullptr;
 }
 
 Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, float fm_, int nb_,
@@ -105,8 +182,10 @@ Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, f
 // the handle owns no stream: work goes to the caller's (default: legacy stream 0)
 Propagator::~Propagator() {
   for (auto &c : gcache_)
-    for (LoopGraph &g : c)
+    for (LoopGraph &g : c) {
+      if (g.timing) step_timer().forget(g.timing.get());
       if (g.exec) cudaGraphExecDestroy(g.exec);
+    }
   if (cap_) cudaStreamDestroy(cap_);
 }
 
@@ -120,47 +199,58 @@ void Propagator::loop_key_common(std::vector<long long> &k) const {
 }
 
 template <typename F>
-void Propagator::run_loop(int which, double points_per_step, const std::vector<long long> &key, F &&body) {
-  const bool use = graphs > 0 && loop_warm_[which] && (graphs == 2 || points_per_step <= kGraphMaxPoints) &&
-                   !step_timer().enabled.load(std::memory_order_relaxed);
+void Propagator::run_loop(int which, double points_per_step, const std::vector<long long> &key_in, F &&body) {
+  const bool use = graphs > 0 && loop_warm_[which] && (graphs == 2 || points_per_step <= kGraphMaxPoints);
   loop_warm_[which] = true;
   if (!use) {
     body();
     return;
   }
+  // a graph captured with stencil timing off has no event nodes: the key
+  // carries the timing setting
+  std::vector<long long> key = key_in;
+  const StepTimer &tm = step_timer();
+  key.push_back(tm.enabled.load(std::memory_order_relaxed) ? tm.period.load(std::memory_order_relaxed) : 0);
   std::vector<LoopGraph> &cache = gcache_[which];
   for (size_t i = 0; i < cache.size(); i++)
     if (cache[i].key == key) {
       if (i) std::swap(cache[i], cache[0]);   // most recent first
       SWFWI_CUDA(cudaGraphLaunch(cache[0].exec, st_));
+      step_timer().replay(cache[0].timing.get());
       return;
     }
   if (!cap_) SWFWI_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
   cudaStream_t user = st_;
   cudaGraph_t g = nullptr;
+  LoopGraph e;
+  e.key = key;
+  e.timing.reset(new StepTimer::Capture);
   SWFWI_CUDA(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal));
   st_ = cap_;
+  step_timer().begin_capture(e.timing.get());
   try {
     body();
   } catch (...) {
+    step_timer().end_capture();
     st_ = user;
     cudaStreamEndCapture(cap_, &g);
     if (g) cudaGraphDestroy(g);
     throw;
   }
+  step_timer().end_capture();
   st_ = user;
   SWFWI_CUDA(cudaStreamEndCapture(cap_, &g));
-  LoopGraph e;
-  e.key = key;
   cudaError_t err = cudaGraphInstantiate(&e.exec, g, 0);
   cudaGraphDestroy(g);
   SWFWI_CUDA(err);
   if (cache.size() >= kGraphCache) {
+    if (cache.back().timing) step_timer().forget(cache.back().timing.get());
     cudaGraphExecDestroy(cache.back().exec);
     cache.pop_back();
   }
   cache.insert(cache.begin(), std::move(e));
   SWFWI_CUDA(cudaGraphLaunch(cache[0].exec, st_));
+  step_timer().replay(cache[0].timing.get());
 }
 
 void Propagator::set_stream(cudaStream_t s) { st_ = s; }
@@ -352,7 +442,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
     a.vel_stride = 0;
     a.shots_per_vel = std::max(n, 1);
     launch_step(ARITH_F64, damped, true, 32, a, n, st_);
-    if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
+    step_timer().close(done, st_);
     return;
   }
   cudaEvent_t done = step_timer().open(st_, pts, n, vel_stride_ ? n : 1, 4);
@@ -384,7 +474,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
     if (a.xchunk <= 0) a.xchunk = 64;
     launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);
   }
-  if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
+  step_timer().close(done, st_);
 }
 
 // ---- single-field operations on caller arrays ([nxpad][nzpad]) ---------
@@ -409,14 +499,14 @@ void Propagator::step_forward(float *p0, float *p1) {
   SWFWI_REQUIRE(p0 && p1 && vel_, "null field or no velocity");
   cudaEvent_t done = step_timer().open(st_, (double)(nxpad - 12) * (nzpad - 12), 1, 1, 4);
   launch_step(arith, true, false, 32, caller_args(p0, p1, vel_, nxpad, nzpad, bx0), 1, st_);
-  if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
+  step_timer().close(done, st_);
 }
 
 void Propagator::step_backward(float *p0, float *p1) {
   SWFWI_REQUIRE(p0 && p1 && vel_, "null field or no velocity");
   cudaEvent_t done = step_timer().open(st_, (double)(nxpad - 12) * (nzpad - 12), 1, 1, 4);
   launch_step(arith, false, false, 32, caller_args(p0, p1, vel_, nxpad, nzpad, bx0), 1, st_);
-  if (done) SWFWI_CUDA(cudaEventRecord(done, st_));
+  step_timer().close(done, st_);
 }
 
 void Propagator::manip_source(float *p, const float *src, int shot_id, int sign) {

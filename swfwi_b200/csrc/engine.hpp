@@ -11,6 +11,7 @@
 #pragma once
 #include <atomic>
 #include <functional>
+#include <memory>
 #include <mutex>
 #include <vector>
 #include "common.hpp"
@@ -22,6 +23,17 @@ namespace swfwi {
 // stream) and their algorithmic work, read by benchmarks.  While enabled,
 // every launch's work is counted and every period-th launch is timed.
 struct StepTimer {
+  // What a captured time loop contributes each time its graph is replayed:
+  // its stencil launches' count and work, its kernel launches, and the
+  // event pairs (graph event-record nodes) of its timed stencil launches,
+  // whose times are added up after each replay.
+  struct Capture {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pairs;
+    long long launches = 0, kernels = 0;
+    double points = 0, bytes = 0;
+    bool pending = false;   // replayed, times not yet added
+    ~Capture();
+  };
   std::atomic<bool> enabled{false};
   std::atomic<int> period{1};
   std::mutex mu;
@@ -29,13 +41,29 @@ struct StepTimer {
   size_t used = 0;
   long long launches = 0;
   double points = 0, bytes = 0;
+  double graph_ms = 0;          // times of replayed graphs' timed launches
+  long long graph_timed = 0;
+  std::vector<Capture *> replayed;
+  Capture *capturing = nullptr;   // the capture in progress (one thread)
   void reset();
   // ms: the timed launches' total; n: launches counted; timed: launches timed
   void read(double &ms, long long &n, double &pts, double &b, long long &timed);
   // Opens the timing of one launch over n fields of pts interior points
   // reading nvel velocity models, el bytes an element; returns the event to
-  // record after the launch (null when timing is off).
+  // record after the launch with close() (null when timing is off).
   cudaEvent_t open(cudaStream_t st, double pts, int n, int nvel, int el);
+  void close(cudaEvent_t done, cudaStream_t st);
+  // Stream capture of a time loop begins / ends (the kernels the capture
+  // counted are taken back; each replay adds them).
+  void begin_capture(Capture *c);
+  void end_capture();
+  // A captured loop was launched: add its counts; its times are added once
+  // its launch is complete (at its next replay or at read()).
+  void replay(Capture *c);
+  void forget(Capture *c);   // before a capture is destroyed
+ private:
+  void harvest(Capture *c);   // mu held
+  long long capture_notes0_ = 0;
 };
 StepTimer &step_timer();
 
@@ -225,6 +253,7 @@ class Propagator {
   struct LoopGraph {
     std::vector<long long> key;
     cudaGraphExec_t exec = nullptr;
+    std::unique_ptr<StepTimer::Capture> timing;   // its launches' counts and timed event pairs
   };
   static constexpr size_t kGraphCache = 4;
   cudaStream_t cap_ = nullptr;

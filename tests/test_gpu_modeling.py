@@ -289,3 +289,46 @@ def test_graph_replay_reads_current_data(cuda):
     # doubling is exact for normal floats; subnormals round on a fixed grid
     err = float((outs[0] - ref * 2).norm() / (ref * 2).norm())
     assert err < 1e-6, err
+
+
+def test_graph_replay_counts_and_times_like_direct_launches(cuda):
+    # stencil timing inside replayed loops: the same launch and work counts
+    # as direct launches, and every timed launch has a positive time
+    import swfwi_b200 as S
+    from swfwi_b200 import survey as sv
+    torch = cuda
+    s = sv.config("fwi").scaled(nt=200, ns=3, sxbeg=60, jsx=100)
+    v = sv.layered_model(s.nx, s.nz, seed=4)
+    stats = {}
+    for graphs in (0, 2):
+        m = S.Damp4t10d.from_survey(s, arith=S.ARITH_FAST)
+        m.set_graphs(graphs)
+        vel = t(torch, m.expandDomain(v))
+        m.bindVelocity(vel)
+        w = t(torch, S.ricker_wavelet(s.nt, s.fm, s.dt))
+        d = torch.zeros((s.ns, s.nt, s.ng), device="cuda")
+        grad = torch.zeros_like(vel)
+        ids = list(range(s.ns))
+        S.stats_enable_step_timing(4)
+        for _ in range(2):                  # direct, then captured
+            m.gradient_batch(w, d + 1e-3, ids, grad)
+        torch.cuda.synchronize()
+        S.stats_reset()
+        for _ in range(3):                  # replayed (graphs 2)
+            m.gradient_batch(w, d + 1e-3, ids, grad)
+        torch.cuda.synchronize()
+        stats[graphs] = S.stats_read()
+        S.stats_enable_step_timing(False)
+        del m
+    a, b = stats[0], stats[2]
+    for k in ("kernel_launches", "step_launches"):
+        assert a[k] == b[k], (k, a[k], b[k])
+    # every 4th launch: counted across loops when launched directly, from
+    # each loop's start inside a graph
+    assert abs(a["step_timed_launches"] - b["step_timed_launches"]) <= 3
+    assert a["step_point_updates"] == b["step_point_updates"]
+    assert b["step_ms"] > 0 and a["step_ms"] > 0
+    # per-launch times agree to within the two paths' launch overheads
+    ra = a["step_ms"] / a["step_timed_launches"]
+    rb = b["step_ms"] / b["step_timed_launches"]
+    assert 0.5 < rb / ra < 2.0, (ra, rb)
