@@ -91,8 +91,10 @@ def measured_peaks():
 # workload's launch (993 x 343 padded, 31,172,256 point-updates), from one
 # ncu capture: (dram__bytes_read.sum + dram__bytes_write.sum) / point-updates.
 # Kernel 1: 288.79 MB + 88.67 MB (profiles/fd_step_ws_96shots_993x343_fast.md);
-# kernel 5: 293.74 MB + 88.59 MB (profiles/fd_step_rq_96shots_993x343_fast.md).
-STENCIL_TRAFFIC_B_PER_PT = {1: 12.11, 5: 12.27}
+# kernel 5 with its automatic task length (99 rows): 282.84 MB + 87.86 MB
+# (profiles/fd_step_rq_96shots_993x343_fast.md; part of the writes is still
+# in L2 when the launch ends).
+STENCIL_TRAFFIC_B_PER_PT = {1: 12.11, 5: 11.89}
 
 
 def traffic_per_point(kernel):
