@@ -600,7 +600,7 @@ def learned_record(args, verbose=False):
     s = P.demo_survey(nz=args.learned_nz, nx=args.learned_nx, nt=args.learned_nt,
                       ns=args.learned_shots).scaled(maxdv=100.0)
     net, st = P.train_from_plain(s, range(100, 100 + args.learned_models), args.learned_iters,
-                                 args.learned_epochs, batch=16)
+                                 args.learned_epochs, batch=16, horizon=args.learned_horizon)
     if verbose:
         print(json.dumps({"training": st}), file=sys.stderr, flush=True)
     tests = []
@@ -637,6 +637,7 @@ def learned_record(args, verbose=False):
                    "train_models": args.learned_models, "plain_iters": args.learned_iters,
                    "train_epochs": args.learned_epochs, "maxdv": s.maxdv,
                    "learned_min_decrease": args.learned_min_decrease,
+                   "target_horizon": args.learned_horizon,
                    "test_seeds": list(args.learned_test_seeds)},
         "training": st, "tests": tests, "network": network,
     }
@@ -724,6 +725,8 @@ def main():
     ap.add_argument("--learned-nt", type=int, default=1000)
     ap.add_argument("--learned-shots", type=int, default=12)
     ap.add_argument("--learned-test-seeds", type=int, nargs="+", default=[200, 201, 202])
+    ap.add_argument("--learned-horizon", type=int, default=None,
+                    help="training target: the velocity this many plain epochs ahead (default: the run's end)")
     ap.add_argument("--learned-min-decrease", type=float, default=0.02,
                     help="a learned step is kept only if it lowers the objective by this fraction")
     ap.add_argument("--nt", type=int, default=24, help="steps of the kernel/tune modes")

@@ -206,20 +206,26 @@ def run_fwi(method: Damp4t10d, exvel0: np.ndarray, wlt: np.ndarray, dobs: np.nda
     return out
 
 
-def training_pairs(net: Preconditioner, method: Damp4t10d, run: dict, skip_last: int = 3):
+def training_pairs(net: Preconditioner, method: Damp4t10d, run: dict, skip_last: int = 3,
+                   horizon: int | None = None):
     """(inputs [S][H][W][3], targets [S][H][W]) on the device from one
     collected plain run: input = features of (gradient_k, velocity_k,
-    illumination_k), target = velocity_final - velocity_k at unit RMS."""
+    illumination_k), target = velocity_{k+horizon} - velocity_k (horizon
+    None: the run's final velocity) at unit RMS."""
     import torch
     final = torch.from_numpy(run["final"]).cuda()
     xs, ts = [], []
     samples = run["samples"]
-    for v, g, il in samples[: max(1, len(samples) - skip_last)]:
+    for k, (v, g, il) in enumerate(samples[: max(1, len(samples) - skip_last)]):
         vd = torch.from_numpy(v).cuda()
         gd = torch.from_numpy(g).cuda()
         ild = torch.from_numpy(il).cuda()
+        if horizon is None or k + horizon >= len(samples):
+            ahead = final
+        else:
+            ahead = torch.from_numpy(samples[k + horizon][0]).cuda()
         xs.append(net.features(method, gd, vd, ild))
-        ts.append(net.target(method, (final - vd).contiguous()))
+        ts.append(net.target(method, (ahead - vd).contiguous()))
     torch.cuda.synchronize()
     return torch.stack(xs), torch.stack(ts)
 
@@ -320,9 +326,11 @@ def synthetic_case(survey, seed: int, recipe: str = "anomaly", smooth_sigma: flo
 
 
 def train_from_plain(survey, train_seeds, iters: int, epochs: int, lr: float = 1e-3, batch: int = 16,
-                     widths=DEFAULT_WIDTHS, recipe: str = "anomaly", verbose: bool = False):
+                     widths=DEFAULT_WIDTHS, recipe: str = "anomaly", verbose: bool = False,
+                     horizon: int | None = None):
     """Collect training pairs from plain FWI runs (iters epochs each) on the
-    seeded models and train a network on them.  Returns (net, stats)."""
+    seeded models and train a network on them (targets `horizon` plain
+    epochs ahead, or the run's end).  Returns (net, stats)."""
     import torch
     net = Preconditioner(widths)
     X, T = [], []
@@ -330,7 +338,7 @@ def train_from_plain(survey, train_seeds, iters: int, epochs: int, lr: float = 1
     for sd in train_seeds:
         m, ex0, vtrue, wlt, dobs = synthetic_case(survey, sd, recipe)
         run = run_fwi(m, ex0, wlt, dobs, survey, iters, vtrue, collect=True)
-        x, t = training_pairs(net, m, run)
+        x, t = training_pairs(net, m, run, horizon=horizon)
         X.append(x)
         T.append(t)
         if verbose:
