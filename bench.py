@@ -268,8 +268,10 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_t / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "batched FWI gradient sample (reference CPU)", "grid": "301x921",
-                       "nt": CPU_SAMPLE_NT, "shots": 1},
+            "config": {"workload": "batched FWI gradient, 96 shots, 301x921 grid (993x337 padded), nt=4000, "
+                                   "uneven spreads 200-921",
+                       "sample": f"each step a bounded sample of that workload: {info['sample']}",
+                       "arith": "reference float arithmetic (the reference's own CPU code, OpenMP)"},
             "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": info["cores"], "kind": "reference",
                              "sample": info["sample"]},
             "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
