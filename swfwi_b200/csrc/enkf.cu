@@ -489,11 +489,10 @@ void gain_on_device(const float *hona, const float *dobs, const double *z, long 
   note_launch();
   k_sum_partials<<<(m + 255) / 256, 256, 0, st>>>(sc.x.get(), sc.partials.get(), nparts);
   note_launch();
-  static bool attr_set = false;
-  if (!attr_set) {
-    SWFWI_CUDA(cudaFuncSetAttribute(k_gain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gain_smem_bytes()));
-    attr_set = true;
-  }
+  // once (thread-safe static init)
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(k_gain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gain_smem_bytes());
+  SWFWI_CUDA(attr);
   k_gain<<<1, kGainThreads, gain_smem_bytes(), st>>>(sc.t4.get(), sc.status.get(), sc.x.get(), n);
   note_launch();
   SWFWI_CUDA(cudaGetLastError());

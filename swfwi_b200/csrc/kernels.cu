@@ -799,12 +799,10 @@ template <int ARITH, bool DAMPED, int NW, int D, int EPI>
 static void ws_launch(const StreamArgs &a, int nslots, cudaStream_t st) {
   constexpr int BZ = 128 * NW - 8;
   constexpr size_t smem = ws_smem_bytes<NW, D, EPI>();
-  static bool attr_set = false;   // raise the dynamic shared memory limit once
-  if (!attr_set) {
-    cudaFuncSetAttribute(fd_step_ws<ARITH, DAMPED, NW, D, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    attr_set = true;
-  }
+  // raise the dynamic shared memory limit once (thread-safe static init)
+  static const cudaError_t attr = cudaFuncSetAttribute(fd_step_ws<ARITH, DAMPED, NW, D, EPI>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  SWFWI_CUDA(attr);
   int nbands = (a.nz - 10 + BZ - 1) / BZ;
   int nchunks = (a.nx - 12 + a.xchunk - 1) / a.xchunk;
   dim3 g = a.shot_major ? dim3(nbands, nchunks, nslots) : dim3(nslots, nbands, nchunks);

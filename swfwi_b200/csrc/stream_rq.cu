@@ -12,12 +12,10 @@ namespace {
 template <int ARITH, bool DAMPED, int NW, int D>
 void rq_t(const StreamArgs &a, int nslots, cudaStream_t st) {
   constexpr size_t smem = rq_smem_bytes<NW, D>();
-  static bool attr_set = false;   // raise the dynamic shared memory limit once
-  if (!attr_set) {
-    cudaFuncSetAttribute(fd_step_rq<ARITH, DAMPED, NW, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    attr_set = true;
-  }
+  // raise the dynamic shared memory limit once (thread-safe static init)
+  static const cudaError_t attr = cudaFuncSetAttribute(fd_step_rq<ARITH, DAMPED, NW, D>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  SWFWI_CUDA(attr);
   StreamArgs b = a;
   const long long pairs = (long long)nslots * rq_detail::slices(a.nz);   // (shot, depth slice) columns
   if (b.xchunk <= 0) {
@@ -25,16 +23,15 @@ void rq_t(const StreamArgs &a, int nslots, cudaStream_t st) {
     // column's tasks fit in one wave of resident warps (a partial last wave
     // costs a whole task duration; shorter tasks spend more of their steps
     // filling the register queue)
-    static int per_sm = 0, sms = 0;
-    if (!per_sm) {
-      int dev = 0;
+    // resident warps of the device (once, thread-safe static init)
+    static const long long resident = [] {
+      int dev = 0, sms = 0, per_sm = 0;
       SWFWI_CUDA(cudaGetDevice(&dev));
       SWFWI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       SWFWI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fd_step_rq<ARITH, DAMPED, NW, D>, NW * 32,
                                                                smem));
-      per_sm = std::max(per_sm, 1);
-    }
-    const long long resident = (long long)per_sm * NW * sms;
+      return (long long)std::max(per_sm, 1) * NW * sms;
+    }();
     const long long per_column = std::max<long long>(1, resident / pairs);
     // at least 8 rows: a task fills its queue with 12 stages before its
     // first output
