@@ -775,9 +775,9 @@ def main():
     m.set_strip_format({"f32": S.STRIP_F32, "f16": S.STRIP_F16, "bf16": S.STRIP_BF16}[args.strips])
     grad = torch.zeros((nxpad, nzpad), dtype=torch.float32, device="cuda")
 
-    # the time loops replay as CUDA graphs from their second use (the first
-    # warm-up step launches directly, the second captures); the stencil
-    # timing is part of the captured graphs, so it is on from the start
+    # the time loops replay as CUDA graphs (mode 2: captured in the first
+    # warm-up step); the stencil timing is part of the captured graphs, so
+    # it is on from the start
     m.set_graphs(2)
     S.stats_enable_step_timing(TIMING_PERIOD)
     for _ in range(max(args.warmup, 0)):

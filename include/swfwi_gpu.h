@@ -126,10 +126,10 @@ int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, i
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on);
 /* CUDA graphs for the forward and backward time loops: on = 0 never, 1
  * (default) while a step covers at most 8e6 points (fields x nxpad x
- * nzpad), 2 for every step size.  From a loop's second use the loop is
- * captured on a private stream and replayed on the propagator's stream
- * (one graph per loop and setting, stencil timing included).  Same
- * kernels, same results. */
+ * nzpad), from a loop's second use; 2 for every step size, from its first
+ * use.  The loop is captured on a private stream and replayed on the
+ * propagator's stream (one graph per loop and setting, stencil timing
+ * included).  Same kernels, same results. */
 int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on);
 /* Per-shot receiver lists (uneven spreads; not in the reference, whose
  * ShotPosition is one common line): shot s has receivers

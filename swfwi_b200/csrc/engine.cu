@@ -200,7 +200,10 @@ void Propagator::loop_key_common(std::vector<long long> &k) const {
 
 template <typename F>
 void Propagator::run_loop(int which, double points_per_step, const std::vector<long long> &key_in, F &&body) {
-  const bool use = graphs > 0 && loop_warm_[which] && (graphs == 2 || points_per_step <= kGraphMaxPoints);
+  // mode 1 captures from a loop's second use (a loop run once costs no
+  // capture), mode 2 from its first
+  const bool use = graphs > 0 && (loop_warm_[which] || graphs == 2) &&
+                   (graphs == 2 || points_per_step <= kGraphMaxPoints);
   loop_warm_[which] = true;
   if (!use) {
     body();

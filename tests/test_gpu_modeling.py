@@ -310,7 +310,7 @@ def test_graph_replay_counts_and_times_like_direct_launches(cuda):
         grad = torch.zeros_like(vel)
         ids = list(range(s.ns))
         S.stats_enable_step_timing(4)
-        for _ in range(2):                  # direct, then captured
+        for _ in range(2):                  # mode 2: captured at once
             m.gradient_batch(w, d + 1e-3, ids, grad)
         torch.cuda.synchronize()
         S.stats_reset()
