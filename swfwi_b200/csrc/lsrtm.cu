@@ -446,12 +446,14 @@ class Prtm {
       if (graphs_[i].key == key) {
         if (graphs_[i].exec) {
           SWFWI_CUDA(cudaGraphLaunch(graphs_[i].exec, st));
+          g_kernel_launches.fetch_add(graphs_[i].kernels);   // the kernels the graph holds
           g_swapped_ = graphs_[i].swapped_after;
           return;
         }
         // second call with these arrays: capture the calls from now on
         if (!cap_) SWFWI_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
         cudaGraph_t g = nullptr;
+        const long long n0 = g_kernel_launches.load();
         SWFWI_CUDA(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal));
         try {
           body(cap_);
@@ -460,12 +462,16 @@ class Prtm {
           if (g) cudaGraphDestroy(g);
           throw;
         }
+        // the capture launched nothing: its kernels count at each launch
+        graphs_[i].kernels = g_kernel_launches.load() - n0;
+        g_kernel_launches.fetch_sub(graphs_[i].kernels);
         SWFWI_CUDA(cudaStreamEndCapture(cap_, &g));
         const cudaError_t err = cudaGraphInstantiate(&graphs_[i].exec, g, 0);
         cudaGraphDestroy(g);
         SWFWI_CUDA(err);
         graphs_[i].swapped_after = g_swapped_;
         SWFWI_CUDA(cudaGraphLaunch(graphs_[i].exec, st));
+        g_kernel_launches.fetch_add(graphs_[i].kernels);
         return;
       }
     body(st);
@@ -474,7 +480,7 @@ class Prtm {
       if (graphs_.front().exec) cudaGraphExecDestroy(graphs_.front().exec);
       graphs_.erase(graphs_.begin());
     }
-    graphs_.push_back(Graph{key, nullptr, g_swapped_});
+    graphs_.push_back(Graph{key, nullptr, g_swapped_, 0});
   }
 
  private:
@@ -482,6 +488,7 @@ class Prtm {
     std::vector<long long> key;
     cudaGraphExec_t exec;
     bool swapped_after;
+    long long kernels = 0;   // kernel launches the graph holds
   };
   static constexpr size_t kGraphs = 4;
 
@@ -491,28 +498,28 @@ class Prtm {
 
   // the stencil steps of one time step (k_prtm_steps); kg, ks slots of the
   // receiver and source pairs, G's in Born's form when gadj
-  void steps(bool gadj, float *g0, const float *g1, int kg, float *s0, const float *s1, int ks, float *dat, int it,
-             int rec_mode, cudaStream_t st) {
+  void steps(const PrtmGeo &geo, bool gadj, float *g0, const float *g1, int kg, float *s0, const float *s1, int ks,
+             float *dat, int it, int rec_mode, cudaStream_t st) {
     const int zb = (nzpad_ - 4 + kLsZ - 1) / kLsZ;
     const dim3 grid(zb, nxpad_ - 4 + (rec_mode ? rec_cols(zb * kLsZ) : 0), kg + ks);
     if (arith_ == ARITH_REF) {
-      if (gadj) k_prtm_steps<ARITH_REF, true><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
+      if (gadj) k_prtm_steps<ARITH_REF, true><<<grid, kLsZ, 0, st>>>(geo, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
                                                                      rec_mode);
-      else k_prtm_steps<ARITH_REF, false><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
+      else k_prtm_steps<ARITH_REF, false><<<grid, kLsZ, 0, st>>>(geo, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
                                                                  rec_mode);
     } else {
-      if (gadj) k_prtm_steps<ARITH_FAST, true><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat,
+      if (gadj) k_prtm_steps<ARITH_FAST, true><<<grid, kLsZ, 0, st>>>(geo, vv_.get(), c_, g0, g1, kg, s0, s1, dat,
                                                                       it, rec_mode);
-      else k_prtm_steps<ARITH_FAST, false><<<grid, kLsZ, 0, st>>>(geo_, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
+      else k_prtm_steps<ARITH_FAST, false><<<grid, kLsZ, 0, st>>>(geo, vv_.get(), c_, g0, g1, kg, s0, s1, dat, it,
                                                                   rec_mode);
     }
     note_launch();
   }
 
-  void aux(const PrtmAux &a, int k, cudaStream_t st) {
+  void aux(const PrtmGeo &geo, const PrtmAux &a, int k, cudaStream_t st) {
     const int zb = (nzpad_ + kLsZ - 1) / kLsZ;
     const dim3 grid(zb, nxpad_ + nx_ + (a.rec_mode ? rec_cols(zb * kLsZ) : 0), k);
-    k_prtm_aux<<<grid, kLsZ, 0, st>>>(geo_, a);
+    k_prtm_aux<<<grid, kLsZ, 0, st>>>(geo, a);
     note_launch();
   }
 
@@ -530,11 +537,10 @@ class Prtm {
   void run(bool adj, float *mod, float *dat, int s0, int k, cudaStream_t st) {
     const long long nm = (long long)nx_ * nz_;
     const size_t fbytes = sizeof(float) * (size_t)k * fsz();
+    // the batch's positions
     PrtmGeo g = geo_;
     g.spos = spos_.get() + s0;
     g.rpos = rpos_.get() + (size_t)s0 * ng_;
-    const PrtmGeo saved = geo_;
-    geo_ = g;
     // the shot's source fields start at zero (:364-365); the receiver
     // fields do in the migration (:381-382) and, outside REF, in Born
     SWFWI_CUDA(cudaMemsetAsync(sp0_.get(), 0, fbytes, st));
@@ -558,9 +564,9 @@ class Prtm {
       a.src_f = S1;
       a.src_val = wl;
       a.src_sign = 1;
-      aux(a, k, st);
+      aux(g, a, k, st);
       for (int it = 0; it < nt_; it++) {
-        steps(false, nullptr, nullptr, 0, S0, S1, k, nullptr, 0, 0, st);
+        steps(g, false, nullptr, nullptr, 0, S0, S1, k, nullptr, 0, 0, st);
         a = none();
         a.sp[0] = S0;
         a.sp[1] = S1;
@@ -574,7 +580,7 @@ class Prtm {
           a.src_val = wl + it + 1;
           a.src_sign = 1;
         }
-        aux(a, k, st);
+        aux(g, a, k, st);
       }
       float *img = mod;
       long long img_stride = 0;
@@ -603,18 +609,18 @@ class Prtm {
         a.dat = d;
         a.rec_it = it;
         a.rec_mode = 1;
-        aux(a, k, st);
+        aux(g, a, k, st);
         std::swap(S0, S1);
         if (exact) {
           // G0 = a^, G1 = b^ (data injected), G2 scratch
-          steps(false, nullptr, nullptr, 0, S0, S1, k, nullptr, 0, 0, st);
+          steps(g, false, nullptr, nullptr, 0, S0, S1, k, nullptr, 0, 0, st);
           k_prtm_born_transpose<<<gfull, kLsZ, 0, st>>>(G2, G1, G0, vv_.get(), sponge_.get(), S0, img, img_stride,
                                                         nx_, nz_, nb_, nxpad_, nzpad_, fsz(), c_);
           note_launch();
           std::swap(G0, G2);
         } else {
           // reconstruct (:390), back-propagate (:399-402) and image (:404-406)
-          steps(false, G0, G1, k, S0, S1, k, nullptr, 0, 0, st);
+          steps(g, false, G0, G1, k, S0, S1, k, nullptr, 0, 0, st);
           a = none();
           a.sp[0] = G0;
           a.sp[1] = G1;
@@ -624,7 +630,7 @@ class Prtm {
           a.cg = G1;
           a.img = img;
           a.img_stride = img_stride;
-          aux(a, k, st);
+          aux(g, a, k, st);
         }
       }
       if (k > 1) {
@@ -659,13 +665,12 @@ class Prtm {
         a.src_f = S1;
         a.src_val = wl + it;
         a.src_sign = 1;
-        aux(a, k, st);
-        steps(true, G0, G1, k, S0, S1, k, d, it, 2, st);
+        aux(g, a, k, st);
+        steps(g, true, G0, G1, k, S0, S1, k, d, it, 2, st);
         std::swap(S0, S1);
       }
     }
     g_swapped_ = G0 != gp0_.get();
-    geo_ = saved;
   }
 
   int arith_, nz_, nx_, nb_, nt_, ns_, ng_, nzpad_ = 0, nxpad_ = 0;

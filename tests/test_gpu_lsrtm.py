@@ -183,3 +183,24 @@ def test_graph_replay_is_bit_identical(cuda, arith):
     half = len(outs) // 2
     for a, b in zip(outs[:half], outs[half:]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_graph_replay_counts_its_kernels(cuda):
+    # replayed calls count the kernels their graphs hold, as direct ones do
+    import swfwi_b200 as S
+    torch = cuda
+    counts = []
+    for graphs in (False, True):
+        op, g = _op(torch, "line", S.ARITH_FAST)
+        op.set_graphs(graphs)
+        mod = t(torch, g["line_mod"])
+        b = torch.zeros(g["line_dat"].shape, dtype=torch.float32, device="cuda")
+        op.lop(False, False, mod, b)
+        torch.cuda.synchronize()
+        S.stats_reset()
+        for _ in range(3):           # with graphs: captured, then replayed
+            op.lop(False, False, mod, b)
+        torch.cuda.synchronize()
+        counts.append(S.stats_read()["kernel_launches"])
+        op.close()
+    assert counts[0] == counts[1] and counts[0] > 0, counts
