@@ -20,6 +20,13 @@ StepTimer &step_timer() {
   return t;
 }
 
+namespace {
+// the capture in progress on this thread, and its thread's launch count at
+// its start
+thread_local StepTimer::Capture *t_capturing = nullptr;
+thread_local long long t_capture_notes0 = 0;
+}  // namespace
+
 StepTimer::Capture::~Capture() {
   for (auto &e : pairs) {
     cudaEventDestroy(e.first);
@@ -76,7 +83,7 @@ void StepTimer::read(double &ms, long long &n, double &pts, double &b, long long
 cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el) {
   if (!enabled.load(std::memory_order_relaxed)) return nullptr;
   std::lock_guard<std::mutex> g(mu);
-  Capture *c = capturing;
+  Capture *c = t_capturing;
   const long long k = c ? c->launches++ : launches++;
   (c ? c->points : points) += pts * n;
   (c ? c->bytes : bytes) += pts * n * 3 * el + pts * el * nvel;
@@ -103,23 +110,21 @@ cudaEvent_t StepTimer::open(cudaStream_t st, double pts, int n, int nvel, int el
 
 void StepTimer::close(cudaEvent_t done, cudaStream_t st) {
   if (!done) return;
-  if (capturing) SWFWI_CUDA(cudaEventRecordWithFlags(done, st, cudaEventRecordExternal));
+  if (t_capturing) SWFWI_CUDA(cudaEventRecordWithFlags(done, st, cudaEventRecordExternal));
   else SWFWI_CUDA(cudaEventRecord(done, st));
 }
 
 void StepTimer::begin_capture(Capture *c) {
-  std::lock_guard<std::mutex> g(mu);
-  capturing = c;
-  capture_notes0_ = g_kernel_launches.load();
+  t_capturing = c;
+  t_capture_notes0 = thread_launches();
 }
 
 void StepTimer::end_capture() {
-  std::lock_guard<std::mutex> g(mu);
-  if (capturing) {
-    capturing->kernels = g_kernel_launches.load() - capture_notes0_;
-    g_kernel_launches.fetch_sub(capturing->kernels);
+  if (t_capturing) {
+    t_capturing->kernels = thread_launches() - t_capture_notes0;
+    g_kernel_launches.fetch_sub(t_capturing->kernels);
   }
-  capturing = nullptr;
+  t_capturing = nullptr;
 }
 
 void StepTimer::replay(Capture *c) {
@@ -139,7 +144,7 @@ void StepTimer::forget(Capture *c) {
   std::lock_guard<std::mutex> g(mu);
   harvest(c);
   replayed.erase(std::remove(replayed.begin(), replayed.end(), c), replayed.end());
-  if (capturing == c) capturing = nullptr;
+  if (t_capturing == c) t_capturing = nullptr;
 }
 
 Propagator::Propagator(const Line &src, const Line &geo, float dt_, float dx_, float fm_, int nb_,

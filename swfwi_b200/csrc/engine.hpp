@@ -44,7 +44,6 @@ struct StepTimer {
   double graph_ms = 0;          // times of replayed graphs' timed launches
   long long graph_timed = 0;
   std::vector<Capture *> replayed;
-  Capture *capturing = nullptr;   // the capture in progress (one thread)
   void reset();
   // ms: the timed launches' total; n: launches counted; timed: launches timed
   void read(double &ms, long long &n, double &pts, double &b, long long &timed);
@@ -63,7 +62,6 @@ struct StepTimer {
   void forget(Capture *c);   // before a capture is destroyed
  private:
   void harvest(Capture *c);   // mu held
-  long long capture_notes0_ = 0;
 };
 StepTimer &step_timer();
 

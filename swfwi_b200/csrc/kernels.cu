@@ -10,7 +10,14 @@
 namespace swfwi {
 
 std::atomic<long long> g_kernel_launches{0};
-void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+namespace {
+thread_local long long t_launches = 0;   // this thread's launches (captures count their own)
+}
+void note_launch() {
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+long long thread_launches() { return t_launches; }
 
 namespace {
 constexpr int kThreads = 256;

@@ -13,8 +13,11 @@ namespace swfwi {
 
 // Kernel launches issued by this library (all launchers count).
 extern std::atomic<long long> g_kernel_launches;
-// Counts one launch in g_kernel_launches.
+// Counts one launch in g_kernel_launches (and in the calling thread's count).
 void note_launch();
+// The launches the calling thread has counted (a stream capture's own
+// launches are the difference over the capture).
+long long thread_launches();
 
 // ---- wavefield point operations (batched over shot slots) --------------
 // A "slot" is one wavefield in a batch; slot_shot maps it to a shot id

@@ -453,7 +453,7 @@ class Prtm {
         // second call with these arrays: capture the calls from now on
         if (!cap_) SWFWI_CUDA(cudaStreamCreateWithFlags(&cap_, cudaStreamNonBlocking));
         cudaGraph_t g = nullptr;
-        const long long n0 = g_kernel_launches.load();
+        const long long n0 = thread_launches();
         SWFWI_CUDA(cudaStreamBeginCapture(cap_, cudaStreamCaptureModeThreadLocal));
         try {
           body(cap_);
@@ -463,7 +463,7 @@ class Prtm {
           throw;
         }
         // the capture launched nothing: its kernels count at each launch
-        graphs_[i].kernels = g_kernel_launches.load() - n0;
+        graphs_[i].kernels = thread_launches() - n0;
         g_kernel_launches.fetch_sub(graphs_[i].kernels);
         SWFWI_CUDA(cudaStreamEndCapture(cap_, &g));
         const cudaError_t err = cudaGraphInstantiate(&graphs_[i].exec, g, 0);
