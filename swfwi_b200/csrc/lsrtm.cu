@@ -49,15 +49,6 @@ struct PrtmCoef {
   float c0, c11, c12, c21, c22;
 };
 
-// The cells of column ix that the sponge touches: all of an edge column,
-// else the nb cells at each end.  Thread t of the column -> iz, or -1.
-__device__ __forceinline__ int sponge_iz(int t, int ix, int nxpad, int nzpad, int nb) {
-  const bool edge = ix < nb || ix >= nxpad - nb;
-  if (edge) return t < nzpad ? t : -1;
-  if (t >= 2 * nb) return -1;
-  return t < nb ? t : nzpad - 2 * nb + t;
-}
-
 // Field geometry shared by the kernels.  Per-slot positions: the source
 // spos[slot] and the receivers rpos[slot*ng + ig] (padded linear indices).
 struct PrtmGeo {
@@ -177,20 +168,21 @@ __device__ __forceinline__ int prtm_ring_index(const PrtmGeo &g, int ix, int iz)
 }
 
 // The work of one time step on cells that no stencil step of the same
-// launch touches, in one launch.  Three roles by blockIdx.y:
-//  * y < nxpad, edge cells of column y (the sponge bands, nb cells from
-//    every side; the 2-cell ring lies inside them): apply_sponge (:123-145)
-//    to up to four fields, in the reference's order for a point ibz cells
-//    from the top or bottom and ibx from the left or right (ib ascending,
-//    the z edges before the x edges); then save the ring of ring_f (after
-//    its sponge) or overwrite it from the store;
-//  * nxpad <= y < nxpad + nx, model column y - nxpad: Born injection g +=
-//    S mod (cross 1) or imaging img += S g (cross 2), and the source
-//    add_source (:161-189) at the slot's source cell;
-//  * y >= nxpad + nx: receivers (rec_mode 1 inject, 2 record).
+// launch touches, in one launch.  Four roles, one thread per cell, by the
+// thread's index t in its slot:
+//  * t < ne, the edge cells (the sponge bands, nb cells from every side;
+//    the 2-cell ring lies inside them): apply_sponge (:123-145) to up to
+//    four fields, in the reference's order for a point ibz cells from the
+//    top or bottom and ibx from the left or right (ib ascending, the z
+//    edges before the x edges); then save the ring of ring_f (after its
+//    sponge) or overwrite it from the store;
+//  * the next nm, the model cells: Born injection g += S mod (cross 1) or
+//    imaging img += S g (cross 2);
+//  * the next nsrc (0 or 1): add_source (:161-189) at the slot's source;
+//  * the rest: receivers (rec_mode 1 inject, 2 record).
 // The model interior (W = 1) and the sponge bands are disjoint, so the
-// roles never touch the same cell.  Grid (z blocks of nzpad, nxpad + nx +
-// receiver columns, slots).
+// roles never touch the same cell.  Grid (blocks over the roles' cells,
+// slots).
 struct PrtmAux {
   float *sp[4];
   float *ring_f, *ring;
@@ -208,13 +200,22 @@ struct PrtmAux {
   int rec_it, rec_mode;
 };
 
-__global__ void k_prtm_aux(PrtmGeo g, PrtmAux a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y, slot = blockIdx.z;
-  if (y < g.nxpad) {
-    const int ix = y;
-    const int iz = sponge_iz(t, ix, g.nxpad, g.nzpad, g.nb);
-    if (iz < 0) return;
+__global__ void k_prtm_aux(PrtmGeo g, PrtmAux a, int ne, int nm, int nsrc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x, slot = blockIdx.y;
+  if (t < ne) {
+    // edge cell t: the nb left columns, the nb right columns, then the nb
+    // cells at each end of every column between them
+    const int band = g.nb * g.nzpad;
+    int ix, iz;
+    if (t < 2 * band) {
+      const int c = t / g.nzpad;
+      ix = c < g.nb ? c : g.nxpad - 2 * g.nb + c;
+      iz = t - c * g.nzpad;
+    } else {
+      const int u = t - 2 * band, r = u % (2 * g.nb);
+      ix = g.nb + u / (2 * g.nb);
+      iz = r < g.nb ? r : g.nzpad - 2 * g.nb + r;
+    }
     const long long p = (long long)slot * g.fsz + (long long)ix * g.nzpad + iz;
     const int ibz = min(iz, g.nzpad - 1 - iz), ibx = min(ix, g.nxpad - 1 - ix);
 #pragma unroll
@@ -240,26 +241,26 @@ __global__ void k_prtm_aux(PrtmGeo g, PrtmAux a) {
     }
     return;
   }
-  if (y < g.nxpad + g.nx) {
-    const int mx = y - g.nxpad, mz = t;
-    if (mz >= g.nz) return;
-    const long long q = (long long)(mx + g.nb) * g.nzpad + mz + g.nb;
-    const long long p = (long long)slot * g.fsz + q;
+  int u = t - ne;
+  if (u < nm) {
+    const int mx = u / g.nz, mz = u - mx * g.nz;
+    const long long p = (long long)slot * g.fsz + (long long)(mx + g.nb) * g.nzpad + mz + g.nb;
     if (a.cross == 1) {
-      a.cg[p] = __fadd_rn(a.cg[p], __fmul_rn(a.cs[p], a.mod[(long long)mx * g.nz + mz]));
-    } else if (a.cross == 2) {
-      float *o = a.img + (long long)slot * a.img_stride + (long long)mx * g.nz + mz;
+      a.cg[p] = __fadd_rn(a.cg[p], __fmul_rn(a.cs[p], a.mod[u]));
+    } else {
+      float *o = a.img + (long long)slot * a.img_stride + u;
       *o = __fadd_rn(*o, __fmul_rn(a.cs[p], a.cg[p]));
-    }
-    if (a.src_f && q == g.spos[slot]) {
-      float *f = a.src_f + p;
-      *f = a.src_sign > 0 ? __fadd_rn(*f, *a.src_val) : __fsub_rn(*f, *a.src_val);
     }
     return;
   }
-  if (a.rec_mode)
-    prtm_receiver(g, slot, (y - g.nxpad - g.nx) * gridDim.x * blockDim.x + t, a.rec_f, a.dat, a.rec_it,
-                  a.rec_mode);
+  u -= nm;
+  if (u < nsrc) {
+    float *f = a.src_f + (long long)slot * g.fsz + g.spos[slot];
+    *f = a.src_sign > 0 ? __fadd_rn(*f, *a.src_val) : __fsub_rn(*f, *a.src_val);
+    return;
+  }
+  u -= nsrc;
+  if (a.rec_mode) prtm_receiver(g, slot, u, a.rec_f, a.dat, a.rec_it, a.rec_mode);
 }
 
 // mod += the per-slot images, in slot order
@@ -517,9 +518,15 @@ class Prtm {
   }
 
   void aux(const PrtmGeo &geo, const PrtmAux &a, int k, cudaStream_t st) {
-    const int zb = (nzpad_ + kLsZ - 1) / kLsZ;
-    const dim3 grid(zb, nxpad_ + nx_ + (a.rec_mode ? rec_cols(zb * kLsZ) : 0), k);
-    k_prtm_aux<<<grid, kLsZ, 0, st>>>(geo, a);
+    // the roles a launch needs, one thread per cell: edge cells, model
+    // cells, the source, the receivers
+    const bool edges = a.sp[0] || a.sp[1] || a.sp[2] || a.sp[3] || a.ring_mode;
+    const int ne = edges ? nxpad_ * nzpad_ - (nxpad_ - 2 * nb_) * (nzpad_ - 2 * nb_) : 0;
+    const int nm = a.cross ? nx_ * nz_ : 0, nsrc = a.src_f ? 1 : 0, nrec = a.rec_mode ? ng_ : 0;
+    const long long total = (long long)ne + nm + nsrc + nrec;
+    if (total <= 0) return;
+    const dim3 grid((unsigned)((total + 255) / 256), k);
+    k_prtm_aux<<<grid, 256, 0, st>>>(geo, a, ne, nm, nsrc);
     note_launch();
   }
 
