@@ -714,7 +714,7 @@ def main():
                          "FWI, EnKF analysis, LSRTM operator, learned vs plain FWI)")
     ap.add_argument("--ess-iters", type=int, default=3, help="timed encoded-source FWI iterations")
     ap.add_argument("--no-learned", action="store_true",
-                    help="leave the learned-vs-plain record (about three minutes) out of the configs")
+                    help="leave the learned-vs-plain record (about four minutes) out of the configs")
     ap.add_argument("--mode", default="bench", choices=["bench", "kernel", "tune", "learned", "network"],
                     help="kernel: short 96-shot batched forward (the small case for ncu); "
                          "tune: print the autotuner's table; learned: FWI wall-clock to equal model "
@@ -722,10 +722,10 @@ def main():
     ap.add_argument("--learned-models", type=int, default=16, help="training models of --mode learned")
     ap.add_argument("--learned-iters", type=int, default=30, help="plain epochs per training/test run")
     ap.add_argument("--learned-epochs", type=int, default=100, help="training epochs of the network")
-    ap.add_argument("--learned-nx", type=int, default=240)
-    ap.add_argument("--learned-nz", type=int, default=80)
-    ap.add_argument("--learned-nt", type=int, default=1000)
-    ap.add_argument("--learned-shots", type=int, default=12)
+    ap.add_argument("--learned-nx", type=int, default=480)
+    ap.add_argument("--learned-nz", type=int, default=160)
+    ap.add_argument("--learned-nt", type=int, default=2000)
+    ap.add_argument("--learned-shots", type=int, default=24)
     ap.add_argument("--learned-test-seeds", type=int, nargs="+", default=[200, 201, 202])
     ap.add_argument("--learned-horizon", type=int, default=None,
                     help="training target: the velocity this many plain epochs ahead (default: the run's end)")
@@ -886,7 +886,7 @@ def main():
                         ("encoded_fwi_301x921", lambda: record_encoded(torch, arith, tuning, args.ess_iters)),
                         ("enkf_201x461", lambda: record_enkf(torch, arith, tuning, not args.no_cpu_baseline)),
                         ("lsrtm_151x461", lambda: record_lsrtm(torch, not args.no_cpu_baseline)),
-                        ("learned_fwi_240x80", lambda: None if args.no_learned else learned_record(args))):
+                        ("learned_fwi", lambda: None if args.no_learned else learned_record(args))):
             try:
                 configs[key] = fn()
             except Exception as e:   # reported, never required
