@@ -93,8 +93,9 @@ def measured_peaks():
 # Kernel 1: 288.79 MB + 88.67 MB (profiles/fd_step_ws_96shots_993x343_fast.md);
 # kernel 5 with its automatic task length (99 rows): 282.84 MB + 87.86 MB
 # (profiles/fd_step_rq_96shots_993x343_fast.md; part of the writes is still
-# in L2 when the launch ends).
-STENCIL_TRAFFIC_B_PER_PT = {1: 12.11, 5: 11.89}
+# in L2 when the launch ends); kernel 6 with its automatic task length (123
+# rows): 279.60 MB + 87.87 MB (profiles/fd_step_rq2_96shots_993x343_fast.md).
+STENCIL_TRAFFIC_B_PER_PT = {1: 12.11, 5: 11.89, 6: 11.79}
 
 
 def traffic_per_point(kernel):
@@ -826,7 +827,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                 "frac": step_gbs / peak, "peak_basis": peak_kind,
                 "traffic": (tpp * per_launch_pts) if tpp else None,
-                "kernel": {1: "fd_step_ws", 5: "fd_step_rq"}.get(tuning.get("kernel", 5)),
+                "kernel": {1: "fd_step_ws", 5: "fd_step_rq", 6: "fd_step_rq2"}.get(tuning.get("kernel", 6)),
                 "launches": st["step_launches"], "timed_launches": st["step_timed_launches"],
                 "timing": f"CUDA events around every {TIMING_PERIOD}th stencil launch of the timed region (event "
                           "nodes inside the replayed time-loop graphs)",

@@ -106,14 +106,18 @@ int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith);
  * write_bndry/read_bndry calls always use FP32. */
 int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
 /* Launch shape of the propagator's stencil (results do not depend on it):
- * kernel 5 (default) = register-queue streaming step, one warp a task of
- * 120 output depths x rows_per_cta rows, each warp its own TMA pipeline
- * (band depth 120, rows ahead 3 or 7); kernel 1 = warp-specialised
+ * kernel 6 (default) = two-row register-queue streaming step, one warp a
+ * task of 120 output depths x rows_per_cta rows, each warp its own TMA
+ * pipeline two rows a stage, two stages ahead (band depth 120; rows in
+ * flight accepted but fixed at 4); FAST arithmetic, REF runs kernel 5;
+ * kernel 5 = register-queue streaming step, one row a stage (band depth
+ * 120, rows ahead 3 or 7); kernel 1 = warp-specialised
  * streaming step (band depth 120, 248 or 376 = 1-3 consumer warps plus a
  * copy warp, rows ahead 3 or 7; the fused time loop always uses it);
- * rows per CTA >= 1, or 0 (default): kernel 5 takes the longest task (at
- * least 8 rows) with which every (shot, depth slice) column's tasks fit in
- * one wave of resident warps, kernel 1 takes 64; shots_slowest = 1 runs the CTAs of one
+ * rows per CTA >= 1, or 0 (default): kernels 5 and 6 take the longest
+ * task (at least 8 rows) with which every (shot, depth slice) column's
+ * tasks fit in one wave of resident warps, kernel 1 takes 64;
+ * shots_slowest = 1 runs the CTAs of one
  * shot together (kernel 1). */
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest);

@@ -582,7 +582,7 @@ class Damp4t10d:
         STRIP_BF16 (scaled 16-bit)."""
         _check(lib().swfwi_damp4t10d_set_strip_format(self.h, fmt))
 
-    def set_tuning(self, kernel: int = 5, band_depth: int = 120, rows_per_cta: int = 0,
+    def set_tuning(self, kernel: int = 6, band_depth: int = 120, rows_per_cta: int = 0,
                    rows_in_flight: int = 3, shots_slowest: bool = False):
         """Launch shape of the stencil (results do not change)."""
         _check(lib().swfwi_damp4t10d_set_tuning(self.h, kernel, band_depth, rows_per_cta, rows_in_flight,

@@ -2,7 +2,8 @@
 
 The streaming step (``stream.cuh``) has knobs that do not change its
 results: which kernel (register-queue warps, each a self-contained TMA
-pipeline; or warp-specialised CTAs with a copy warp), output depths per
+pipeline, one or two rows a stage; or warp-specialised CTAs with a copy
+warp), output depths per
 CTA, rows per task (0: the register-queue kernel's automatic length, one
 wave of tasks), rows in flight ahead of the compute and the launch
 order (shots slowest or fastest).  ``tune`` times short batched forward runs of a survey for each
@@ -15,7 +16,7 @@ import itertools
 
 import numpy as np
 
-DEFAULT = {"kernel": 5, "band_depth": 120, "rows_per_cta": 0, "rows_in_flight": 3,
+DEFAULT = {"kernel": 6, "band_depth": 120, "rows_per_cta": 0, "rows_in_flight": 3,
            "shots_slowest": False}
 
 
@@ -23,6 +24,8 @@ def candidates(nz: int):
     """The register-queue kernel's task lengths and prefetch depths, the
     warp-specialised kernel's band depths, chunk lengths, prefetch depths
     and launch orders."""
+    for rows in (0, 64, 96, 128):
+        yield {"kernel": 6, "band_depth": 120, "rows_per_cta": rows, "rows_in_flight": 3, "shots_slowest": False}
     for rows, depth in itertools.product((0, 32, 48, 64), (3, 7)):
         yield {"kernel": 5, "band_depth": 120, "rows_per_cta": rows, "rows_in_flight": depth,
                "shots_slowest": False}
@@ -33,7 +36,7 @@ def candidates(nz: int):
 
 def valid(cfg: dict) -> bool:
     """The launch shapes swfwi_damp4t10d_set_tuning accepts."""
-    if cfg["kernel"] == 5:
+    if cfg["kernel"] in (5, 6):
         ok_bz = cfg["band_depth"] == 120
     elif cfg["kernel"] == 1:
         ok_bz = cfg["band_depth"] in (120, 248, 376)

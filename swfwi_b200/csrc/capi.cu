@@ -217,8 +217,8 @@ int swfwi_damp4t10d_set_graphs(swfwi_damp4t10d *h, int on) {
 int swfwi_damp4t10d_set_tuning(swfwi_damp4t10d *h, int kernel, int band_depth, int rows_per_cta,
                                int rows_in_flight, int shots_slowest) {
   return guarded([&] {
-    SWFWI_REQUIRE(kernel == 1 || kernel == 5, "kernel must be 1 or 5");
-    if (kernel == 5) {
+    SWFWI_REQUIRE(kernel == 1 || kernel == 5 || kernel == 6, "kernel must be 1, 5 or 6");
+    if (kernel == 5 || kernel == 6) {
       SWFWI_REQUIRE(band_depth == 120, "band depth must be 120 (one warp a task)");
     } else {
       SWFWI_REQUIRE(band_depth == 120 || band_depth == 248 || band_depth == 376,

@@ -476,8 +476,11 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
     // the fused step is the warp-specialised kernel with 376-deep bands
     if (stream_kernel != 1 || a.xchunk <= 0) a.xchunk = 64;
     launch_ws_step(ar, damped, 376, stream_kernel == 1 ? stream_depth : 3, a, n, st_);
-  } else if (stream_kernel == 5) {
-    launch_rq_step(ar, damped, stream_depth, a, n, st_);   // xchunk 0: automatic
+  } else if (stream_kernel == 6 && ar == ARITH_FAST) {
+    launch_rq2_step(damped, a, n, st_);   // xchunk 0: automatic
+  } else if (stream_kernel == 5 || stream_kernel == 6) {
+    // kernel 6 runs FAST arithmetic only: REF takes kernel 5
+    launch_rq_step(ar, damped, stream_kernel == 6 ? 3 : stream_depth, a, n, st_);   // xchunk 0: automatic
   } else {
     if (a.xchunk <= 0) a.xchunk = 64;
     launch_ws_step(ar, damped, stream_bz, stream_depth, a, n, st_);

@@ -103,7 +103,7 @@ class Propagator {
   cudaStream_t stream() const { return st_; }
   int arith = ARITH_REF;
   int strip_format = SWFWI_STRIP_F32;
-  int stream_kernel = 5;      // 1: warp-specialised, 5: register-queue warps
+  int stream_kernel = 6;      // 1: warp-specialised, 5: register-queue warps, 6: two-row register queue (FAST)
   int stream_bz = 120;        // output depths per CTA (120 for kernel 5; 120, 248 or 376 for kernel 1)
   int stream_xchunk = 0;      // rows per CTA (per warp task for kernel 5); 0: automatic
   int stream_depth = 3;       // rows ahead (3 or 7)

@@ -109,6 +109,9 @@ void launch_ws_step(int arith, bool damped, int bz, int depth, const StreamArgs 
 // pipeline (a one-warp CTA) per task of 120 output depths x a.xchunk rows
 // of one slot, depth = 3 or 7 stages ahead.
 void launch_rq_step(int arith, bool damped, int depth, const StreamArgs &a, int nslots, cudaStream_t st);
+// The two-row register-queue step (kernel 6, stream_rq2.cuh): FAST
+// arithmetic only; a.xchunk <= 0 takes the one-wave task length.
+void launch_rq2_step(bool damped, const StreamArgs &a, int nslots, cudaStream_t st);
 // out[s][ig*nt + it] = in[s][it*ng + ig] for nslots seismograms
 // (matrix_transpose of common.cpp:14-24 with n1 = ng, n2 = nt).
 void launch_transpose_traces(float *out, const float *in, int nt, int ng, int nslots, cudaStream_t st);

@@ -4,10 +4,20 @@
 #include "common.hpp"
 #include "kernels.cuh"
 #include "stream_rq.cuh"
+#include "stream_rq2.cuh"
 
 namespace swfwi {
 
 namespace {
+
+// The longest task (at least 8 rows) with which every (shot, depth slice)
+// column's tasks fit in one wave of `resident` warps: a partial last wave
+// costs a whole task duration, and shorter tasks spend more of their steps
+// filling the register queue.
+int one_wave_rows(int nx, long long columns, long long resident) {
+  const long long per_column = std::max<long long>(1, resident / columns);
+  return std::max(8, (int)((nx - 12 + per_column - 1) / per_column));
+}
 
 template <int ARITH, bool DAMPED, int NW, int D>
 void rq_t(const StreamArgs &a, int nslots, cudaStream_t st) {
@@ -32,10 +42,7 @@ void rq_t(const StreamArgs &a, int nslots, cudaStream_t st) {
                                                                smem));
       return (long long)std::max(per_sm, 1) * NW * sms;
     }();
-    const long long per_column = std::max<long long>(1, resident / pairs);
-    // at least 8 rows: a task fills its queue with 12 stages before its
-    // first output
-    b.xchunk = std::max(8, (int)((a.nx - 12 + per_column - 1) / per_column));
+    b.xchunk = one_wave_rows(a.nx, pairs, resident);
   }
   const long long nchunks = (b.nx - 12 + b.xchunk - 1) / b.xchunk;
   const long long tasks = pairs * nchunks;
@@ -54,7 +61,38 @@ void rq_d(int depth, const StreamArgs &a, int nslots, cudaStream_t st) {
   else rq_t<ARITH, DAMPED, 1, 3>(a, nslots, st);
 }
 
+template <bool DAMPED>
+void rq2_t(const StreamArgs &a, int nslots, cudaStream_t st) {
+  constexpr size_t smem = rq2_smem_bytes();
+  // raise the dynamic shared memory limit once (thread-safe static init)
+  static const cudaError_t attr = cudaFuncSetAttribute(fd_step_rq2<DAMPED>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  SWFWI_CUDA(attr);
+  StreamArgs b = a;
+  const long long columns = (long long)nslots * rq2_detail::slices(a.nz);
+  if (b.xchunk <= 0) {
+    static const long long resident = [] {
+      int dev = 0, sms = 0, per_sm = 0;
+      SWFWI_CUDA(cudaGetDevice(&dev));
+      SWFWI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      SWFWI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fd_step_rq2<DAMPED>, 32, smem));
+      return (long long)std::max(per_sm, 1) * sms;
+    }();
+    b.xchunk = one_wave_rows(a.nx, columns, resident);
+  }
+  const long long tasks = columns * ((b.nx - 12 + b.xchunk - 1) / b.xchunk);
+  if (tasks > 0x7fffffffLL) throw Error(SWFWI_ERR_BAD_ARG, "too many stencil tasks for one launch");
+  fd_step_rq2<DAMPED><<<(unsigned)tasks, 32, smem, st>>>(b, nslots);
+}
+
 }  // namespace
+
+void launch_rq2_step(bool damped, const StreamArgs &a, int nslots, cudaStream_t st) {
+  if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;
+  if (damped) rq2_t<true>(a, nslots, st);
+  else rq2_t<false>(a, nslots, st);
+  note_launch();
+}
 
 void launch_rq_step(int arith, bool damped, int depth, const StreamArgs &a, int nslots, cudaStream_t st) {
   if (nslots <= 0 || a.nx <= 12 || a.nz <= 12) return;

@@ -68,7 +68,8 @@ def test_fast_forward_within_tolerance(cuda, fdo):
 
 
 @pytest.mark.parametrize("kern,bz,rows,depth", [(1, 376, 64, 3), (1, 248, 9, 7), (5, 120, 48, 3),
-                                                (5, 120, 31, 7)])
+                                                (5, 120, 31, 7), (6, 120, 0, 3), (6, 120, 1, 3), (6, 120, 2, 3),
+                                                (6, 120, 33, 3), (6, 120, 200, 3)])
 def test_fast_forward_every_kernel_within_tolerance(cuda, kern, bz, rows, depth):
     # FAST arithmetic in every stencil kernel: seismogram within 1e-5
     # relative L2 of the reference's
@@ -193,7 +194,7 @@ def test_errors_reported(cuda):
     (1, 376, 16, 3, 0), (1, 248, 33, 3, 1),
     (5, 120, 1, 3, 0), (5, 120, 9, 7, 0), (5, 120, 64, 3, 0), (5, 120, 33, 7, 0), (5, 120, 200, 3, 0),
     (5, 120, 11, 3, 0), (5, 120, 12, 7, 0), (5, 120, 8, 3, 0), (5, 120, 16, 7, 0),
-    (5, 120, 0, 3, 0), (5, 120, 0, 7, 0), (1, 376, 0, 3, 0)])
+    (5, 120, 0, 3, 0), (5, 120, 0, 7, 0), (1, 376, 0, 3, 0), (6, 120, 0, 3, 0), (6, 120, 5, 3, 0)])
 def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
     # every band depth / chunk length of the streaming stencil gives the
     # reference's seismogram bit for bit
@@ -206,7 +207,7 @@ def test_stream_launch_shapes_bit_exact(cuda, kern, bz, rows, depth, order):
 
 
 @pytest.mark.parametrize("kern,bz,depth", [(1, 120, 7), (1, 248, 3), (1, 376, 3), (1, 376, 7),
-                                           (5, 120, 3), (5, 120, 7)])
+                                           (5, 120, 3), (5, 120, 7), (6, 120, 3)])
 def test_stream_matches_reference_large_grid(cuda, ref, kern, bz, depth):
     # 921 x 301 (993 x 343 padded, pitch 344): several bands, a short last
     # band, many chunks
@@ -332,3 +333,20 @@ def test_graph_replay_counts_and_times_like_direct_launches(cuda):
     ra = a["step_ms"] / a["step_timed_launches"]
     rb = b["step_ms"] / b["step_timed_launches"]
     assert 0.5 < rb / ra < 2.0, (ra, rb)
+
+
+
+@pytest.mark.parametrize("rows", [0, 1, 2, 7, 8, 33, 64, 200])
+def test_two_row_kernel_bit_identical_to_one_row_kernel(cuda, rows):
+    # FAST: kernel 6 (two rows a stage) and kernel 5 give the same
+    # seismogram bit for bit, for even and odd task lengths
+    import swfwi_b200 as S
+    torch = cuda
+    s, m, g, vel = small_method(torch, arith=S.ARITH_FAST)
+    out = []
+    for kern in (5, 6):
+        m.set_tuning(kern, 120, rows, 3, 0)
+        d = torch.zeros((s.nt, s.ng), device="cuda")
+        m.FwiForwardModeling(t(torch, g["wlt"]), d, 1)
+        out.append(d.cpu().numpy())
+    np.testing.assert_array_equal(out[0], out[1])

@@ -26,7 +26,7 @@ pytestmark = pytest.mark.gpu
 
 GRAD_TOL = 1e-4
 OBJ_TOL_FAST = 1e-4
-KERNELS = [(1, 376, 64, 3, 0), (5, 120, 0, 3, 0), (5, 120, 48, 7, 0)]
+KERNELS = [(1, 376, 64, 3, 0), (5, 120, 0, 3, 0), (5, 120, 48, 7, 0), (6, 120, 0, 3, 0), (6, 120, 77, 3, 0)]
 
 
 def _batched_case(ref, nt=900, picks=4):
@@ -103,11 +103,12 @@ def test_batched_workload_gradient_fast(cuda, batched_case, tuning):
 
 
 def test_fast_kernels_give_identical_bits(cuda, batched_case):
-    # kernel 5 evaluates every point in kernel 1's operation order
+    # kernels 5 and 6 evaluate every point in kernel 1's operation order
     import swfwi_b200 as S
     a, _ = _gpu_gradient(cuda, batched_case, S.ARITH_FAST, KERNELS[0])
-    b, _ = _gpu_gradient(cuda, batched_case, S.ARITH_FAST, KERNELS[1])
-    np.testing.assert_array_equal(a, b)
+    for kern in KERNELS[1:]:
+        b, _ = _gpu_gradient(cuda, batched_case, S.ARITH_FAST, kern)
+        np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.parametrize("fmt", [1, 2])
