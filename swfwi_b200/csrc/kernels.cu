@@ -1,4 +1,5 @@
 // Kernels around the stencil; see kernels.cuh for the reference citations.
+#include <climits>
 #include <atomic>
 #include <cmath>
 #include <cuda_bf16.h>
@@ -160,29 +161,48 @@ void launch_strip_read(const T *bndr, long long bndr_slot_stride, T *field, long
 // `next`, so the three commute; each element is the same single operation
 // as in k_record, k_strip and k_inject.  Grid (blocks over the longest of
 // the three lists, slots).
+// Each thread takes kSmallE elements a grid-stride apart and issues every
+// load of its elements before any store: the position gathers and the
+// field reads of the four overlap instead of running as four dependent
+// chains (these launches are latency-bound).  The loads and stores touch
+// disjoint arrays (cur vs seis, bndr and next), so the order changes no bits.
+constexpr int kSmallE = 4;
+
 template <typename T>
 __global__ void k_after_forward(T *seis, long long seis_slot_stride, const T *cur, PointSet rec, T *bndr,
                                 long long bndr_slot_stride, int bs, int nx, int nz, int bx0, int pitch, T *next,
                                 PointSet src, const T *vals, long long val_slot_stride, int val_stride,
-                                long long shot_stride) {
+                                long long shot_stride, int most) {
   const int slot = blockIdx.y;
   const long long off = (long long)slot * shot_stride;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x;; i += gridDim.x * blockDim.x) {
-    const bool r = seis && i < rec.per_shot, b = bndr && i < bs, n = next && i < src.per_shot;
-    if (!(r || b || n)) return;
-    if (r) {
-      const int shot = rec.slot_shot ? rec.slot_shot[slot] : slot;
-      const int p = rec.pos[(long long)shot * rec.per_shot + i];
-      seis[(long long)slot * seis_slot_stride + i] = p < 0 ? T(0) : cur[off + p];
+  const int stride = gridDim.x * blockDim.x;
+  const int rshot = rec.slot_shot ? rec.slot_shot[slot] : slot;
+  const int sshot = src.slot_shot ? src.slot_shot[slot] : slot;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < most; i0 += kSmallE * stride) {
+    int rp[kSmallE], sp[kSmallE];
+#pragma unroll
+    for (int e = 0; e < kSmallE; e++) {
+      const int i = i0 + e * stride;
+      rp[e] = (seis && i < rec.per_shot) ? rec.pos[(long long)rshot * rec.per_shot + i] : INT_MIN;
+      sp[e] = (next && i < src.per_shot) ? src.pos[(long long)sshot * src.per_shot + i] : -1;
     }
-    if (b) bndr[(long long)slot * bndr_slot_stride + i] = cur[off + strip_index(i, nx, nz, bx0, pitch)];
-    if (n) {
-      const int shot = src.slot_shot ? src.slot_shot[slot] : slot;
-      const int p = src.pos[(long long)shot * src.per_shot + i];
-      if (p >= 0) {
-        T *f = next + off + p;
-        *f = exact_add<T>(*f, vals[(long long)slot * val_slot_stride + (long long)i * val_stride]);
+    T rv[kSmallE], bv[kSmallE], nv[kSmallE], vv[kSmallE];
+#pragma unroll
+    for (int e = 0; e < kSmallE; e++) {
+      const int i = i0 + e * stride;
+      rv[e] = rp[e] >= 0 ? cur[off + rp[e]] : T(0);
+      bv[e] = (bndr && i < bs) ? cur[off + strip_index(i, nx, nz, bx0, pitch)] : T(0);
+      if (sp[e] >= 0) {
+        nv[e] = next[off + sp[e]];
+        vv[e] = vals[(long long)slot * val_slot_stride + (long long)i * val_stride];
       }
+    }
+#pragma unroll
+    for (int e = 0; e < kSmallE; e++) {
+      const int i = i0 + e * stride;
+      if (rp[e] != INT_MIN) seis[(long long)slot * seis_slot_stride + i] = rv[e];   // position < 0: 0
+      if (bndr && i < bs) bndr[(long long)slot * bndr_slot_stride + i] = bv[e];
+      if (sp[e] >= 0) next[off + sp[e]] = exact_add<T>(nv[e], vv[e]);
     }
   }
 }
@@ -197,11 +217,9 @@ void launch_after_forward(T *seis, long long seis_slot_stride, const T *cur, Poi
   const int nr = seis ? rec.per_shot : 0, ni = next ? src.per_shot : 0;
   const int most = nr > bs ? (nr > ni ? nr : ni) : (bs > ni ? bs : ni);
   if (most <= 0) return;
-  // four elements a thread: these launches are latency-bound, fewer and
-  // fuller blocks finish sooner
-  const dim3 g(grid_for(most, 512), nslots);
+  const dim3 g(grid_for(most, 128 * kSmallE), nslots);
   k_after_forward<T><<<g, 128, 0, st>>>(seis, seis_slot_stride, cur, rec, bndr, bndr_slot_stride, bs, nx, nz, bx0,
-                                        pitch, next, src, vals, val_slot_stride, val_stride, shot_stride);
+                                        pitch, next, src, vals, val_slot_stride, val_stride, shot_stride, most);
   note_launch();
 }
 
@@ -213,30 +231,43 @@ template <typename T>
 __global__ void k_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, int va_stride, int sign_a,
                           T *fb, PointSet pb, const T *vb, long long vb_slot_stride, int vb_stride, int sign_b,
                           long long shot_stride, const T *bndr, long long bndr_slot_stride, int bs, int nx, int nz,
-                          int bx0, int pitch) {
+                          int bx0, int pitch, int most) {
   const int slot = blockIdx.y;
   const long long off = (long long)slot * shot_stride;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bs || i < pa.per_shot || i < pb.per_shot;
-       i += gridDim.x * blockDim.x) {
-  if (bndr && i < bs) fa[off + strip_index(i, nx, nz, bx0, pitch)] = bndr[(long long)slot * bndr_slot_stride + i];
-  if (i < pa.per_shot) {
-    const int shot = pa.slot_shot ? pa.slot_shot[slot] : slot;
-    const int p = pa.pos[(long long)shot * pa.per_shot + i];
-    if (p >= 0) {
-      const T v = va[(long long)slot * va_slot_stride + (long long)i * va_stride];
-      T *f = fa + off + p;
-      *f = sign_a > 0 ? exact_add<T>(*f, v) : exact_sub<T>(*f, v);
+  const int stride = gridDim.x * blockDim.x;
+  const int ashot = pa.slot_shot ? pa.slot_shot[slot] : slot;
+  const int bshot = pb.slot_shot ? pb.slot_shot[slot] : slot;
+  // as k_after_forward: all loads of a thread's elements before its stores;
+  // the strip band and the source and receiver points are disjoint cells
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < most; i0 += kSmallE * stride) {
+    int ap[kSmallE], bp[kSmallE];
+#pragma unroll
+    for (int e = 0; e < kSmallE; e++) {
+      const int i = i0 + e * stride;
+      ap[e] = i < pa.per_shot ? pa.pos[(long long)ashot * pa.per_shot + i] : -1;
+      bp[e] = i < pb.per_shot ? pb.pos[(long long)bshot * pb.per_shot + i] : -1;
     }
-  }
-  if (i < pb.per_shot) {
-    const int shot = pb.slot_shot ? pb.slot_shot[slot] : slot;
-    const int p = pb.pos[(long long)shot * pb.per_shot + i];
-    if (p >= 0) {
-      const T v = vb[(long long)slot * vb_slot_stride + (long long)i * vb_stride];
-      T *f = fb + off + p;
-      *f = sign_b > 0 ? exact_add<T>(*f, v) : exact_sub<T>(*f, v);
+    T sv[kSmallE], af[kSmallE], av[kSmallE], bf[kSmallE], bv[kSmallE];
+#pragma unroll
+    for (int e = 0; e < kSmallE; e++) {
+      const int i = i0 + e * stride;
+      sv[e] = (bndr && i < bs) ? bndr[(long long)slot * bndr_slot_stride + i] : T(0);
+      if (ap[e] >= 0) {
+        af[e] = fa[off + ap[e]];
+        av[e] = va[(long long)slot * va_slot_stride + (long long)i * va_stride];
+      }
+      if (bp[e] >= 0) {
+        bf[e] = fb[off + bp[e]];
+        bv[e] = vb[(long long)slot * vb_slot_stride + (long long)i * vb_stride];
+      }
     }
-  }
+#pragma unroll
+    for (int e = 0; e < kSmallE; e++) {
+      const int i = i0 + e * stride;
+      if (bndr && i < bs) fa[off + strip_index(i, nx, nz, bx0, pitch)] = sv[e];
+      if (ap[e] >= 0) fa[off + ap[e]] = sign_a > 0 ? exact_add<T>(af[e], av[e]) : exact_sub<T>(af[e], av[e]);
+      if (bp[e] >= 0) fb[off + bp[e]] = sign_b > 0 ? exact_add<T>(bf[e], bv[e]) : exact_sub<T>(bf[e], bv[e]);
+    }
   }
 }
 
@@ -250,9 +281,10 @@ void launch_inject2(T *fa, PointSet pa, const T *va, long long va_slot_stride, i
   int most = pa.per_shot > pb.per_shot ? pa.per_shot : pb.per_shot;
   most = most > bs ? most : bs;
   if (most <= 0) return;
-  const dim3 g(grid_for(most, 512), nslots);
+  const dim3 g(grid_for(most, 128 * kSmallE), nslots);
   k_inject2<T><<<g, 128, 0, st>>>(fa, pa, va, va_slot_stride, va_stride, sign_a, fb, pb, vb, vb_slot_stride,
-                                  vb_stride, sign_b, shot_stride, bndr, bndr_slot_stride, bs, nx, nz, bx0, pitch);
+                                  vb_stride, sign_b, shot_stride, bndr, bndr_slot_stride, bs, nx, nz, bx0, pitch,
+                                  most);
   note_launch();
 }
 

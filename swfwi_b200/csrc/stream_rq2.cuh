@@ -109,14 +109,17 @@ __global__ void __launch_bounds__(32, kRq2MinBlocks) fd_step_rq2(StreamArgs a, i
                                 : (role < 4 ? smem_u32(&S.p[0][rowb][0]) : smem_u32(&S.v[0][rowb][0]));
   const uint32_t my_slot_bytes = is_c ? 4u * 2 * WC : 4u * 2 * WP;
   const uint32_t my_bytes = is_c ? cbytes : pbytes;
+  // stages are issued in order, so the lane's source row advances two rows
+  // a call (a running pointer: no 64-bit multiply per stage)
+  const float *run_src = my_src;
   auto issue = [&](int s, int cs, int ps) {
     if (lane < 6) {
       const bool pv = s >= 6;
       const bool b_ok = 2 * s + 2 <= R;
       if (lane == 0) mbar_expect_tx(&S.full[cs], (cbytes + (pv ? 2u * pbytes : 0u)) * (b_ok ? 2u : 1u));
       if ((is_c || pv) && (!rowb || b_ok))
-        bulk_g2s_u32(my_ring + (uint32_t)(is_c ? cs : ps) * my_slot_bytes, my_src + (long long)(2 * s) * P, my_bytes,
-                     smem_u32(&S.full[cs]));
+        bulk_g2s_u32(my_ring + (uint32_t)(is_c ? cs : ps) * my_slot_bytes, run_src, my_bytes, smem_u32(&S.full[cs]));
+      run_src += 2 * P;
     }
   };
   for (int s = 0; s < D2 && s < K2; s++) issue(s, s % NC, s % NP);
