@@ -387,7 +387,9 @@ def record_encoded(torch, arith, tuning, iters):
     every iteration (EssFwiFramework::epoch, essfwiframework.cpp:191-239).
     `iters` iterations are timed (the 50-iteration run is their mean x 50).
     The gradient's error against the FP64 GPU run of the same scheme is
-    stated for FP32, FP16 and BF16 boundary strips, on one supershot."""
+    stated for FP32, FP16 and BF16 boundary strips, on one supershot, and on
+    the gradient's unmasked interior also for FP32, FP16 and BF16 checkpoint
+    snapshots (every 64 steps), with one supershot gradient timed each way."""
     import swfwi_b200 as S
     from swfwi_b200 import survey as sv
     s = sv.config("encoded")
@@ -417,12 +419,32 @@ def record_encoded(torch, arith, tuning, iters):
     g64 = torch.zeros(exi.shape, dtype=torch.float64, device="cuda")
     t64, _ = _timed(torch, lambda: m.calgradient_ess_f64(velinit, encsrc.double(), vsrc.double(), g64))
     errs = {}
+    b = s.nb + 6   # the unmasked interior: [b, nxpad-b) x [6, nzpad-b)
+
+    def inner(a):
+        return a[b:a.shape[0] - b, 6:a.shape[1] - b]
+
+    def rel(a):
+        return float(((inner(a).double() - inner(g64)).norm() / inner(g64).norm()).item())
+
+    inner_errs, grad_s = {}, {}
     for name, fmt in (("f32", S.STRIP_F32), ("f16", S.STRIP_F16), ("bf16", S.STRIP_BF16)):
         m.set_strip_format(fmt)
         g = torch.zeros(exi.shape, device="cuda")
         m.calgradient_ess(encsrc, vsrc, g)
         errs[name] = float(((g.double() - g64).norm() / g64.norm()).item())
+        inner_errs["strips_" + name] = rel(g)
+        if name == "f32":
+            grad_s["strips_f32"], _ = _timed(torch, lambda: m.calgradient_ess(encsrc, vsrc, g.zero_()))
     m.set_strip_format(S.STRIP_F32)
+    for name, fmt in (("f32", S.STRIP_F32), ("f16", S.STRIP_F16), ("bf16", S.STRIP_BF16)):
+        m.set_reconstruction(S.RECON_SNAPSHOTS, 64, fmt)
+        g = torch.zeros(exi.shape, device="cuda")
+        m.calgradient_ess(encsrc, vsrc, g)
+        inner_errs["snapshots_" + name] = rel(g)
+        if name == "f32":
+            grad_s["snapshots_f32"], _ = _timed(torch, lambda: m.calgradient_ess(encsrc, vsrc, g.zero_()))
+    m.set_reconstruction(S.RECON_STRIPS)
     dobs_h = dobs.cpu().numpy()
     del dobs, encobs
     f = S.EssFwiFramework(m, exi, s.vmin, s.vmax, s.nita, s.maxdv, wlt_h, dobs_h)
@@ -437,7 +459,10 @@ def record_encoded(torch, arith, tuning, iters):
             "iterations_timed": len(ts), "s_per_iteration": per, "fifty_iterations_s": 50 * per,
             "gpu_first_epoch_s": t_first, "trials_last": f.lastTrials(),
             "gradient_rel_l2_vs_f64": errs, "f64_gradient_s": t64,
-            "strips": "FP32 during the timed iterations; FP16/BF16 scaled strips in the error figures"}
+            "interior_gradient_rel_l2_vs_f64": inner_errs, "supershot_gradient_s": grad_s,
+            "strips": "FP32 during the timed iterations; FP16/BF16 scaled strips in the error figures",
+            "snapshots": "checkpoint snapshots of both fields every 64 steps (FP32 or scaled FP16/BF16), each "
+                         "segment re-run forward in the backward sweep; errors on the unmasked interior"}
 
 
 def record_enkf(torch, arith, tuning, cpu, members=64):

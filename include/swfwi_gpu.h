@@ -46,6 +46,9 @@ enum { SWFWI_ARITH_REF = 0, SWFWI_ARITH_FAST = 1, SWFWI_ARITH_F64 = 2 };
  * backwards.  F32 is exact; F16/BF16 keep one scale per strip and step. */
 enum { SWFWI_STRIP_F32 = 0, SWFWI_STRIP_F16 = 1, SWFWI_STRIP_BF16 = 2 };
 
+/* How a gradient's backward sweep obtains the source wavefield. */
+enum { SWFWI_RECON_STRIPS = 0, SWFWI_RECON_SNAPSHOTS = 1 };
+
 const char *swfwi_status_string(int status);
 const char *swfwi_last_error(void);
 int swfwi_version(void);
@@ -105,6 +108,20 @@ int swfwi_damp4t10d_set_arith(swfwi_damp4t10d *h, int arith);
  * power-of-two scale per shot and step).  The single-field
  * write_bndry/read_bndry calls always use FP32. */
 int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format);
+/* Reconstruction of the source wavefield in the gradients' backward sweep.
+ * SWFWI_RECON_STRIPS (default): back-propagation with the saved boundary
+ * strips, the reference's calgradient (fwiframework.cpp:146-176).
+ * SWFWI_RECON_SNAPSHOTS (checkpointing; no counterpart in the reference):
+ * the forward sweep saves both wavefields every `every` steps (every >= 2)
+ * in `format` (SWFWI_STRIP_F32 = exact; F16/BF16 = one power-of-two scale
+ * per field, shot and snapshot); the backward sweep re-runs each segment of
+ * `every` steps forward from its snapshot into a ring of every + 1 fields
+ * and images with the forward field itself.  With F32 snapshots the imaged
+ * source field is the forward's own, bit for bit; the strips' rounding in
+ * the back-propagation is gone, so results differ from the reference's
+ * within the FP32 gradient tolerance.  Memory per shot: (every + 1) fields
+ * plus 2 fields (F32) or 1 field (16-bit) per snapshot. */
+int swfwi_damp4t10d_set_reconstruction(swfwi_damp4t10d *h, int mode, int every, int format);
 /* Launch shape of the propagator's stencil (results do not depend on it):
  * kernel 6 (default) = two-row register-queue streaming step, one warp a
  * task of 120 output depths x rows_per_cta rows, each warp its own TMA

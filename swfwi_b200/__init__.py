@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(_HERE, "libswfwi_b200.so")
 
 ARITH_REF, ARITH_FAST, ARITH_F64 = 0, 1, 2
 STRIP_F32, STRIP_F16, STRIP_BF16 = 0, 1, 2
+RECON_STRIPS, RECON_SNAPSHOTS = 0, 1
 
 
 class SwfwiError(RuntimeError):
@@ -60,6 +61,7 @@ _SIGS = {
     "swfwi_damp4t10d_set_stream": [_vp, _vp],
     "swfwi_damp4t10d_set_arith": [_vp, C.c_int],
     "swfwi_damp4t10d_set_strip_format": [_vp, C.c_int],
+    "swfwi_damp4t10d_set_reconstruction": [_vp, C.c_int, C.c_int, C.c_int],
     "swfwi_damp4t10d_set_tuning": [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int],
     "swfwi_damp4t10d_set_receivers_per_shot": [_vp, _ip, _ip, _ip],
     "swfwi_damp4t10d_dims": [_vp, _ip, _ip, _ip, _ip, _ip],
@@ -581,6 +583,14 @@ class Damp4t10d:
         """Boundary strips of the gradients: STRIP_F32 (exact), STRIP_F16 or
         STRIP_BF16 (scaled 16-bit)."""
         _check(lib().swfwi_damp4t10d_set_strip_format(self.h, fmt))
+
+    def set_reconstruction(self, mode: int, every: int = 64, fmt: int = STRIP_F32):
+        """Source-field reconstruction in the gradients' backward sweep:
+        RECON_STRIPS (back-propagation with boundary strips, the reference's
+        method) or RECON_SNAPSHOTS (checkpoint snapshots of both fields every
+        `every` steps in `fmt`, each segment re-run forward in the backward
+        sweep)."""
+        _check(lib().swfwi_damp4t10d_set_reconstruction(self.h, mode, every, fmt))
 
     def set_tuning(self, kernel: int = 6, band_depth: int = 120, rows_per_cta: int = 0,
                    rows_in_flight: int = 3, shots_slowest: bool = False):

@@ -203,6 +203,19 @@ int swfwi_damp4t10d_set_strip_format(swfwi_damp4t10d *h, int format) {
   });
 }
 
+int swfwi_damp4t10d_set_reconstruction(swfwi_damp4t10d *h, int mode, int every, int format) {
+  return guarded([&] {
+    SWFWI_REQUIRE(mode == SWFWI_RECON_STRIPS || mode == SWFWI_RECON_SNAPSHOTS,
+                  "reconstruction must be SWFWI_RECON_STRIPS or _SNAPSHOTS");
+    SWFWI_REQUIRE(every >= 2, "snapshot interval must be at least 2 steps");
+    SWFWI_REQUIRE(format == SWFWI_STRIP_F32 || format == SWFWI_STRIP_F16 || format == SWFWI_STRIP_BF16,
+                  "snapshot format must be SWFWI_STRIP_F32, _F16 or _BF16");
+    P(h).recon = mode;
+    P(h).snap_every = every;
+    P(h).snap_format = format;
+  });
+}
+
 int swfwi_damp4t10d_set_fusion(swfwi_damp4t10d *h, int on) {
   return guarded([&] { P(h).fuse = on != 0; });
 }

@@ -434,12 +434,13 @@ void Propagator::check_device_error() {
 // one velocity model): the streaming TMA kernel for float arithmetics, the
 // shared-memory tile kernel for FP64.
 void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp,
-                             int n, const Epilogue *epi) {
+                             int n, const Epilogue *epi, void *out) {
   double pts = (double)(nxpad - 12) * (nzpad - 12);
   if (ar == ARITH_F64) {
     cudaEvent_t done = step_timer().open(st_, pts, n, 1, 8);
     StepArgs a;
     a.prev = prev;
+    a.out = out;
     a.curr = curr;
     a.vel = velrcp;
     a.nx = nxpad;
@@ -456,6 +457,7 @@ void Propagator::step_fields(int ar, bool damped, void *prev, const void *curr, 
   cudaEvent_t done = step_timer().open(st_, pts, n, vel_stride_ ? n : 1, 4);
   StreamArgs a;
   a.prev = static_cast<float *>(prev);
+  a.out = static_cast<float *>(out);
   a.curr = static_cast<const float *>(curr);
   a.rcp = static_cast<const float *>(velrcp);
   a.damp_x = damp_x_.get();
@@ -605,7 +607,20 @@ void Propagator::ensure_work(Work<T> &w, int n, bool strips) {
   size_t f = (size_t)n * fstride;
   w.p0.resize(f);
   w.p1.resize(f);
-  if (strips) {
+  if (strips && recon == SWFWI_RECON_SNAPSHOTS) {
+    const size_t m = (size_t)snapshot_count();
+    if (sizeof(T) == 4 && snap_format != SWFWI_STRIP_F32) {
+      w.qsnaps.resize(m * 2 * n * (size_t)nxpad * pitch);
+      w.qsnap_scale.resize(m * 2 * n);
+      w.snap_pmax.resize((size_t)n * kSnapParts);
+    } else {
+      w.snaps.resize(m * 2 * f);
+    }
+    // the kernels never write a field's border, coordinate margin or tail:
+    // zero once, they stay zero through restores and out-of-place steps
+    w.ring.resize((size_t)(snap_every + 1) * f);
+    w.ring.zero(st_);
+  } else if (strips) {
     if (sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32) {
       w.qstrips.resize((size_t)n * nt * bsize);
       w.qscale.resize((size_t)n * nt);
@@ -660,6 +675,44 @@ bool Propagator::ess_lines(int k, std::vector<PtLine> &src, std::vector<PtLine> 
   return true;
 }
 
+// Snapshot m: the pair (a, b) = (p0, p1) after forward step
+// (m + 1) * snap_every - 1, every slot's whole field (F32 or the element
+// type: a copy of the n slots' contiguous fields; 16-bit: the values from
+// each origin over nxpad x pitch, one scale per field, slot and snapshot).
+template <typename T>
+void Propagator::save_snapshot(Work<T> &w, int n, int m, const T *a, const T *b) {
+  const long long f = (long long)n * fstride;
+  const T *src[2] = {a, b};
+  for (int k = 0; k < 2; k++) {
+    if (sizeof(T) == 4 && snap_format != SWFWI_STRIP_F32) {
+      const long long count = (long long)nxpad * pitch;
+      launch_field_write_q(snap_format, w.qsnaps.get() + ((long long)m * 2 + k) * n * count,
+                           w.qsnap_scale.get() + ((long long)m * 2 + k) * n, 1, w.snap_pmax.get(),
+                           reinterpret_cast<const float *>(src[k]), fstride, count, n, st_);
+    } else {
+      SWFWI_CUDA(cudaMemcpyAsync(w.snaps.get() + ((long long)m * 2 + k) * f, src[k] - kStreamCoff, f * sizeof(T),
+                                 cudaMemcpyDeviceToDevice, st_));
+    }
+  }
+}
+
+template <typename T>
+void Propagator::restore_snapshot(Work<T> &w, int n, int m, T *a, T *b) {
+  const long long f = (long long)n * fstride;
+  T *dst[2] = {a, b};
+  for (int k = 0; k < 2; k++) {
+    if (sizeof(T) == 4 && snap_format != SWFWI_STRIP_F32) {
+      const long long count = (long long)nxpad * pitch;
+      launch_field_read_q(snap_format, w.qsnaps.get() + ((long long)m * 2 + k) * n * count,
+                          w.qsnap_scale.get() + ((long long)m * 2 + k) * n, 1, reinterpret_cast<float *>(dst[k]),
+                          fstride, count, n, st_);
+    } else {
+      SWFWI_CUDA(cudaMemcpyAsync(dst[k] - kStreamCoff, w.snaps.get() + ((long long)m * 2 + k) * f, f * sizeof(T),
+                                 cudaMemcpyDeviceToDevice, st_));
+    }
+  }
+}
+
 template <typename T>
 void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, long long it_stride,
                              long long slot_stride, int i_stride, PointSet rec, int ngrec, T *dcal,
@@ -678,6 +731,16 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
       reinterpret_cast<long long>(p0), reinterpret_cast<long long>(p1),
       reinterpret_cast<long long>(w.strips.get()), reinterpret_cast<long long>(w.qstrips.get()),
       reinterpret_cast<long long>(w.qscale.get())};
+  // checkpoint snapshots instead of strips
+  const bool gradient_sweep = save_strips;
+  const int nsnap = save_strips ? snapshot_count() : 0;
+  if (save_strips && recon == SWFWI_RECON_SNAPSHOTS) {
+    save_strips = false;
+    for (long long v : {(long long)recon, (long long)snap_every, (long long)snap_format,
+                        reinterpret_cast<long long>(w.snaps.get()), reinterpret_cast<long long>(w.qsnaps.get()),
+                        reinterpret_cast<long long>(w.qsnap_scale.get())})
+      key.push_back(v);
+  }
   loop_key_common(key);
   const bool qstrips = save_strips && sizeof(T) == 4 && strip_format != SWFWI_STRIP_F32;
   run_loop(0, (double)n * nxpad * nzpad, key, [&] {
@@ -697,7 +760,9 @@ void Propagator::run_forward(Work<T> &w, int n, PointSet src, const T *vals, lon
     if (qstrips)
       launch_strip_write_q(strip_format, w.qstrips.get() + (long long)it * bsize, bstride, w.qscale.get() + it,
                            nt, reinterpret_cast<const float *>(p0), fstride, n, nxpad, nzpad, bx0, pitch, st_);
-    if (save_strips && sizeof(T) == 4 && illum && it % std::max(illum_every, 1) == 0)
+    if (nsnap > 0 && (it + 1) % snap_every == 0 && (it + 1) / snap_every <= nsnap)
+      save_snapshot(w, n, (it + 1) / snap_every - 1, p0, p1);
+    if (gradient_sweep && sizeof(T) == 4 && illum && it % std::max(illum_every, 1) == 0)
       launch_illum_accum(illum, reinterpret_cast<const float *>(p0), fstride, n, nxpad, nzpad, pitch, st_);
   }
   });
@@ -735,6 +800,64 @@ bool Propagator::run_backward(Work<T> &w, int n, PointSet src, const T *vals, lo
       reinterpret_cast<long long>(w.strips.get()), reinterpret_cast<long long>(w.qstrips.get()),
       reinterpret_cast<long long>(w.qscale.get()), reinterpret_cast<long long>(w.src_lines.get()),
       reinterpret_cast<long long>(w.rec_lines.get()), (long long)(dt * 1e9)};
+  if (recon == SWFWI_RECON_SNAPSHOTS) {
+    // Checkpointing: the image at backward step it uses the forward field
+    // of step it-1 (what the strips' back-propagation rebuilds in the
+    // interior, its source terms aside), taken from a re-run of its segment
+    // of snap_every steps from the segment's snapshot.  Ring slot r holds
+    // the field of forward step seg * snap_every + r - 1; each re-run step
+    // writes a fresh slot (out-of-place) and adds the next source as the
+    // forward does.
+    const int K = snap_every;
+    const bool summed = sum_images && sizeof(T) == 4 && ar == ARITH_FAST;
+    for (long long v : {(long long)(3 + (summed ? 1 : 0)), (long long)K, (long long)snap_format,
+                        reinterpret_cast<long long>(w.snaps.get()), reinterpret_cast<long long>(w.qsnaps.get()),
+                        reinterpret_cast<long long>(w.qsnap_scale.get()), reinterpret_cast<long long>(w.ring.get())})
+      key.push_back(v);
+    loop_key_common(key);
+    const long long block = (long long)n * fstride;
+    auto ring_at = [&](int r) { return w.ring.get() + (long long)r * block + kStreamCoff; };
+    run_loop(1, (double)n * nxpad * nzpad, key, [&] {
+    int seg_cur = -1;
+    for (int it = nt - 1; it >= 0; it--) {
+      // receivers, as below: addSource -> stepForward -> swap
+      launch_inject<T>(gp1, fstride, n, rec, vsrc + (long long)it * ngrec, (long long)nt * ngrec, 1, +1, st_);
+      step_fields(ar, true, gp0, gp1, velrcp, n);
+      std::swap(gp0, gp1);
+      float t = dt * (float)it;
+      float scale;
+      if ((double)t > 0.4) scale = 1.0f;
+      else if ((double)t > 0.3) scale = (float)(((double)t - 0.3) / 0.1);
+      else break;
+      const int j = it - 1;   // t > 0.3 keeps it >= 1
+      const int seg = j / K;
+      if (seg != seg_cur) {
+        const int a0 = seg * K, b0 = std::min(a0 + K, nt);
+        if (seg == 0) {   // the forward's start: zero fields, then the first source
+          SWFWI_CUDA(cudaMemsetAsync(ring_at(0) - kStreamCoff, 0, 2 * block * sizeof(T), st_));
+          launch_inject<T>(ring_at(1), fstride, n, src, vals, slot_stride, i_stride, +1, st_);
+        } else {
+          restore_snapshot(w, n, seg - 1, ring_at(0), ring_at(1));
+        }
+        for (int jj = a0; jj + 1 < b0; jj++) {
+          T *nextf = ring_at(jj - a0 + 2);
+          step_fields(ar, true, ring_at(jj - a0), ring_at(jj - a0 + 1), velrcp, n, nullptr, nextf);
+          launch_inject<T>(nextf, fstride, n, src, vals + (long long)(jj + 1) * it_stride, slot_stride, i_stride,
+                           +1, st_);
+        }
+        seg_cur = seg;
+      }
+      const T *sf = ring_at(j - seg * K + 1);
+      if (summed)
+        launch_image_sum(reinterpret_cast<float *>(w.image.get()) + kStreamCoff, reinterpret_cast<const float *>(sf),
+                         reinterpret_cast<const float *>(gp0), fstride, n, bx0, nxpad - bxn, bz0, nzpad - bzn, pitch,
+                         scale, st_);
+      else
+        launch_image<T>(w.image.get() + kStreamCoff, fstride, sf, gp0, fstride, n, npts, scale, st_);
+    }
+    });
+    return summed;
+  }
   const bool fused = fuse && sizeof(T) == 4 && src_lines && rec_lines && (int)src_lines->size() == n &&
                      (int)rec_lines->size() == n && injectable(*src_lines) && injectable(*rec_lines);
   if (fused) {
@@ -894,13 +1017,19 @@ int Propagator::max_batch() const {
   if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) return 1;
   // per slot: p0, p1, g0, g1, image fields; strips; dcal, res, vsrc data
   const double strip_bytes = strip_format == SWFWI_STRIP_F32 ? 4.0 : 2.0;
-  double per = 5.0 * fstride * 4 + (double)nt * bsize * strip_bytes + 3.0 * nt * ngmax * 4 + 4096;
+  // reconstruction storage: strips, or snapshots plus the re-forward ring
+  const double recon_bytes =
+      recon == SWFWI_RECON_SNAPSHOTS
+          ? 2.0 * snapshot_count() * (snap_format == SWFWI_STRIP_F32 ? 4.0 * fstride : 2.0 * nxpad * pitch) +
+                (snap_every + 1.0) * fstride * 4
+          : (double)nt * bsize * strip_bytes;
+  double per = 5.0 * fstride * 4 + recon_bytes + 3.0 * nt * ngmax * 4 + 4096;
   double budget = 0.85 * (double)freeb;
   // memory already held by this propagator's work space counts as free
   budget += (double)(w_.p0.capacity() + w_.p1.capacity() + w_.g0.capacity() + w_.g1.capacity() +
                      w_.image.capacity() + w_.strips.capacity() + w_.dcal.capacity() +
-                     w_.res.capacity() + w_.vsrc.capacity()) * 4 +
-            (double)w_.qstrips.capacity() * 2;
+                     w_.res.capacity() + w_.vsrc.capacity() + w_.snaps.capacity() + w_.ring.capacity()) * 4 +
+            (double)(w_.qstrips.capacity() + w_.qsnaps.capacity()) * 2;
   int m = (int)(budget / per);
   return std::max(1, std::min(m, ns));
 }

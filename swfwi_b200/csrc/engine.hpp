@@ -9,6 +9,7 @@
 // origins (slot start + 8).  Arrays the caller owns keep the reference's
 // [nxpad][nzpad] layout.
 #pragma once
+#include <algorithm>
 #include <atomic>
 #include <functional>
 #include <memory>
@@ -78,6 +79,13 @@ struct Work {
   DevBuf<T> p0, p1, g0, g1, image, strips;
   DevBuf<uint16_t> qstrips;   // 16-bit strips [slot][nt][bsize] (FP32 fields, F16/BF16 format)
   DevBuf<float> qscale;       // their scales [slot][nt]
+  // checkpoint snapshots (reconstruction by snapshots): pairs of whole
+  // fields [snapshot][2][slot][fstride] in T, or 16-bit [snapshot][2][slot]
+  // [nxpad * pitch] with scales [snapshot][2][slot]; the re-forward ring of
+  // snap_every + 1 fields [ring slot][slot][fstride]
+  DevBuf<T> snaps, ring;
+  DevBuf<uint16_t> qsnaps;
+  DevBuf<float> qsnap_scale, snap_pmax;
   DevBuf<float> dcal, res, vsrc;   // [slot][nt][ngmax]
   DevBuf<int> win, win2, slot_shot, slot_row;
   DevBuf<PtLine> src_lines, rec_lines;   // fused epilogue lines [slot]
@@ -103,6 +111,14 @@ class Propagator {
   cudaStream_t stream() const { return st_; }
   int arith = ARITH_REF;
   int strip_format = SWFWI_STRIP_F32;
+  // How the backward sweep gets the source field: SWFWI_RECON_STRIPS
+  // (back-propagation with the saved boundary strips, the reference's
+  // method) or SWFWI_RECON_SNAPSHOTS (the forward saves both fields every
+  // snap_every steps in snap_format; the backward re-runs each segment
+  // forward from its snapshot into a ring of fields).
+  int recon = SWFWI_RECON_STRIPS;
+  int snap_every = 64;
+  int snap_format = SWFWI_STRIP_F32;
   int stream_kernel = 6;      // 1: warp-specialised, 5: register-queue warps, 6: two-row register queue (FAST)
   int stream_bz = 120;        // output depths per CTA (120 for kernel 5; 120, 248 or 376 for kernel 1)
   int stream_xchunk = 0;      // rows per CTA (per warp task for kernel 5); 0: automatic
@@ -213,7 +229,15 @@ class Propagator {
   void upload_geometry();
   const float *rcp_of(const float *vel);
   void step_fields(int ar, bool damped, void *prev, const void *curr, const void *velrcp, int n,
-                   const Epilogue *epi = nullptr);
+                   const Epilogue *epi = nullptr, void *out = nullptr);
+  // Checkpoint snapshots: how many a forward sweep saves, and their save /
+  // restore (snapshot m holds the pair (p0, p1) after forward step
+  // (m + 1) * snap_every - 1).
+  int snapshot_count() const { return recon == SWFWI_RECON_SNAPSHOTS ? (nt - 1) / std::max(snap_every, 1) : 0; }
+  template <typename T>
+  void save_snapshot(Work<T> &w, int n, int m, const T *a, const T *b);
+  template <typename T>
+  void restore_snapshot(Work<T> &w, int n, int m, T *a, T *b);
   // Point lines (padded coordinates) for the fused forward epilogue; false
   // when the points do not form a regular line.
   bool line_of(const int *xs, const int *zs, int n, PtLine &out) const;

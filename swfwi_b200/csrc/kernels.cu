@@ -1058,6 +1058,109 @@ void launch_strip_read_q(int format, const uint16_t *q, long long q_slot_stride,
   note_launch();
 }
 
+// ---------------------------------------------------------------- 16-bit snapshots
+namespace {
+// Pass 1: each CTA's largest |value| of its part of one slot's field (grid
+// x = kSnapParts parts, y = slots) into part_max[slot][part]; pass 2 (the
+// encoder) reduces a slot's parts in a fixed order and encodes.
+__global__ void __launch_bounds__(1024)
+k_field_max(float *part_max, const float *field, long long shot_stride, long long count) {
+  __shared__ float wmax[32];
+  const int slot = blockIdx.y;
+  const float4 *f = reinterpret_cast<const float4 *>(field + (long long)slot * shot_stride);
+  const long long n4 = count / 4;
+  float m = 0.f;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 v = f[i];
+    m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmaxf(m, wmax[w]);
+    part_max[slot * kSnapParts + blockIdx.x] = m;
+  }
+}
+
+__device__ __forceinline__ void snap_scale_of(float m, float &s, float &inv) {
+  int e = 0;
+  if (m > 0.f && m <= 3.0e38f) frexpf(m, &e);   // m < 2^e
+  e = max(e, -100);                              // as the strips: subnormal-only fields
+  s = ldexpf(1.0f, e - 14);
+  inv = ldexpf(1.0f, 14 - e);
+}
+
+template <int FMT>
+__global__ void k_field_write_q(uint16_t *q, float *scale, long long scale_slot_stride, const float *part_max,
+                                const float *field, long long shot_stride, long long count) {
+  const int slot = blockIdx.y;
+  float m = 0.f;
+  for (int p = 0; p < kSnapParts; p++) m = fmaxf(m, part_max[slot * kSnapParts + p]);
+  float s, inv;
+  snap_scale_of(m, s, inv);
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[(long long)slot * scale_slot_stride] = s;
+  const float4 *f = reinterpret_cast<const float4 *>(field + (long long)slot * shot_stride);
+  ushort4 *qs = reinterpret_cast<ushort4 *>(q + (long long)slot * count);
+  const long long n4 = count / 4;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 v = f[i];
+    qs[i] = make_ushort4(q_encode<FMT>(v.x * inv), q_encode<FMT>(v.y * inv), q_encode<FMT>(v.z * inv),
+                         q_encode<FMT>(v.w * inv));
+  }
+}
+
+template <int FMT>
+__global__ void k_field_read_q(const uint16_t *q, const float *scale, long long scale_slot_stride, float *field,
+                               long long shot_stride, long long count) {
+  const int slot = blockIdx.y;
+  const float s = scale[(long long)slot * scale_slot_stride];
+  float4 *f = reinterpret_cast<float4 *>(field + (long long)slot * shot_stride);
+  const ushort4 *qs = reinterpret_cast<const ushort4 *>(q + (long long)slot * count);
+  const long long n4 = count / 4;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const ushort4 h = qs[i];
+    f[i] = make_float4(q_decode<FMT>(h.x) * s, q_decode<FMT>(h.y) * s, q_decode<FMT>(h.z) * s,
+                       q_decode<FMT>(h.w) * s);
+  }
+}
+
+void check_snap_args(const void *q, const float *field, long long shot_stride, long long count) {
+  if (count % 4 != 0 || shot_stride % 4 != 0 ||
+      (reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(field)) % 16 != 0)
+    throw Error(SWFWI_ERR_BAD_ARG, "snapshot: sizes and arrays must be 16-byte aligned");
+}
+}  // namespace
+
+void launch_field_write_q(int format, uint16_t *q, float *scale, long long scale_slot_stride, float *pm,
+                          const float *field, long long shot_stride, long long count, int nslots, cudaStream_t st) {
+  if (nslots <= 0 || count <= 0) return;
+  check_snap_args(q, field, shot_stride, count);
+  k_field_max<<<dim3(kSnapParts, nslots), 1024, 0, st>>>(pm, field, shot_stride, count);
+  note_launch();
+  const dim3 g(grid_for(count / 4, kThreads * 8), nslots);
+  if (format == SWFWI_STRIP_F16)
+    k_field_write_q<SWFWI_STRIP_F16><<<g, kThreads, 0, st>>>(q, scale, scale_slot_stride, pm, field, shot_stride,
+                                                             count);
+  else
+    k_field_write_q<SWFWI_STRIP_BF16><<<g, kThreads, 0, st>>>(q, scale, scale_slot_stride, pm, field,
+                                                              shot_stride, count);
+  note_launch();
+}
+
+void launch_field_read_q(int format, const uint16_t *q, const float *scale, long long scale_slot_stride,
+                         float *field, long long shot_stride, long long count, int nslots, cudaStream_t st) {
+  if (nslots <= 0 || count <= 0) return;
+  check_snap_args(q, field, shot_stride, count);
+  const dim3 g(grid_for(count / 4, kThreads * 8), nslots);
+  if (format == SWFWI_STRIP_F16)
+    k_field_read_q<SWFWI_STRIP_F16><<<g, kThreads, 0, st>>>(q, scale, scale_slot_stride, field, shot_stride, count);
+  else
+    k_field_read_q<SWFWI_STRIP_BF16><<<g, kThreads, 0, st>>>(q, scale, scale_slot_stride, field, shot_stride,
+                                                             count);
+  note_launch();
+}
+
 template void launch_after_forward<float>(float *, long long, const float *, PointSet, float *, long long, int,
                                           int, int, int, float *, PointSet, const float *, long long, int,
                                           long long, int, cudaStream_t);

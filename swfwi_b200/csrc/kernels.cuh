@@ -79,6 +79,15 @@ void launch_strip_write_q(int format, uint16_t *q, long long q_slot_stride, floa
 void launch_strip_read_q(int format, const uint16_t *q, long long q_slot_stride, const float *scale,
                          long long scale_slot_stride, float *field, long long shot_stride, int nslots,
                          int nx, int nz, int bx0, int pitch, cudaStream_t st);
+// Whole-field checkpoint snapshots in the same 16-bit formats: the first
+// `count` values from each slot's field origin, one power-of-two scale per
+// slot (the strips' rule); q is [slot][count], scale[slot * scale_slot_stride];
+// part_max is scratch of nslots * kSnapParts floats.
+constexpr int kSnapParts = 16;
+void launch_field_write_q(int format, uint16_t *q, float *scale, long long scale_slot_stride, float *part_max,
+                          const float *field, long long shot_stride, long long count, int nslots, cudaStream_t st);
+void launch_field_read_q(int format, const uint16_t *q, const float *scale, long long scale_slot_stride,
+                         float *field, long long shot_stride, long long count, int nslots, cudaStream_t st);
 
 // image[slot] -= s[slot] * r[slot] * scale  (cross_correlation,
 // fwiframework.cpp:107-112)

@@ -6,7 +6,8 @@
 //   pass 2  next = (2 - 2d + d^2) c - (1 - 2d) prev + u2/vt
 //                  + (1/12)(1/vt)^2 (u2[z-1] + u2[z+1] + u2[x-1] + u2[x+1] - 4 u2)
 // with d = 0.05 dist^2 on the left/right/bottom sponge.  Layout p[x*nz + z]
-// (z contiguous); outputs on [6, nx-6) x [6, nz-6), in place over prev.
+// (z contiguous); outputs on [6, nx-6) x [6, nz-6), in place over prev (or
+// into a separate output field, StepArgs::out).
 //
 // One CTA owns a TX x 32 output tile.  It stages the (TX+12) x 44 halo of
 // the current field in shared memory, forms u2 on the (TX+2) x 34 ring in
@@ -42,6 +43,7 @@ enum Arith { ARITH_REF = 0, ARITH_FAST = 1, ARITH_F64 = 2 };
 
 struct StepArgs {
   void *prev;           // [shot][nx][nz] (element type per ARITH)
+  void *out = nullptr;  // where the next field goes (same layout); nullptr: in place over prev
   const void *curr;     // same
   const void *vel;      // vt, or 1/vt when VEL_IS_RCP
   int nx, nz;           // padded grid
@@ -240,8 +242,8 @@ fd_step_tile(StepArgs a) {
       float delta = 0.0f;
       if constexpr (DAMPED) delta = damp_delta(gx, gz, nx, nz, a.bx0);
       T c = sc[(lx + H) * CZ + (tz + H)];
-      prev[(long long)gx * pitch + gz] =
-          update_point<ARITH, UZ, T>(c, pv[k], r, &su[(lx + 1) * UZ + (tz + 1)], delta);
+      T *dst = a.out ? (T *)a.out + (long long)shot * a.shot_stride : prev;
+      dst[(long long)gx * pitch + gz] = update_point<ARITH, UZ, T>(c, pv[k], r, &su[(lx + 1) * UZ + (tz + 1)], delta);
     }
   }
 }

@@ -48,6 +48,7 @@ struct Epilogue {
 
 struct StreamArgs {
   float *prev;            // field origins (see layout above)
+  float *out = nullptr;   // where the next field goes (same layout); nullptr: in place over prev
   const float2 *coef_x;   // FAST update coefficients of each row's left/right ramp, [nx]
   const float *curr;
   const float *rcp;       // 1/vt, same layout

@@ -150,7 +150,7 @@ fd_step_rq(StreamArgs a, int nslots) {
   const int qo = 4 * lane + 8;                  // own depths in the current window
   const int po = 4 * min(max(lane - 1, 0), kOutLanes - 1);   // own depths in the previous / 1/vt
                                                              // window (lanes 0, 31: a neighbour's)
-  float *outp = prevb + (long long)xa * P + zg; // output row xa, advanced a row per output
+  float *outp = (a.out ? a.out + (long long)shot * a.shot_stride : prevb) + (long long)xa * P + zg;   // output row xa, a row per output
 
   // sponge: the bottom ramp (per depth) overrides the left/right one (per
   // row).  REF keeps the depth ramp dz (-1 above the bottom sponge); FAST

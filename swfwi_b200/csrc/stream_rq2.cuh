@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(32, kRq2MinBlocks) fd_step_rq2(StreamArgs a, i
   const int zw = 4 * lane;       // z window (depths zg-8 .. zg+11) in the current window
   const int qo = 4 * lane + 8;   // own depths in the current window
   const int po = 4 * min(max(lane - 1, 0), kOutLanes - 1);   // own depths in the previous / 1/vt window
-  float *outp = prevb + (long long)xa * P + zg;               // output row xa, two rows a stage
+  float *outp = (a.out ? a.out + (long long)shot * a.shot_stride : prevb) + (long long)xa * P + zg;   // output row xa, two rows a stage
 
   // sponge as in fd_step_rq: this lane's depth coefficients, the row's on
   // left/right ramp rows where no bottom ramp acts

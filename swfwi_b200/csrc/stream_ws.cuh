@@ -147,7 +147,7 @@ fd_step_ws(StreamArgs a) {
   // ---------------------------------------------------------------- consumers
   const int t = tid;
   const int zg = z0 - 4 + 4 * t;
-  float *prevg = a.prev + (long long)shot * a.shot_stride + (long long)xa * P + zg;   // output row xa
+  float *prevg = (a.out ? a.out : a.prev) + (long long)shot * a.shot_stride + (long long)xa * P + zg;   // output row xa
   float dz[4] = {-1.f, -1.f, -1.f, -1.f};
   bool zok[4];
   bool coldamp = false;
