@@ -907,10 +907,14 @@ def main():
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
         configs = {}
-        for key, fn in (("fwi_iteration_151x461", lambda: record_fwi_iteration(torch, arith, tuning,
+        # the records run other grids and batch sizes: the tuned kernel with
+        # the automatic task length, which sizes the tasks for each grid (a
+        # row count tuned on this grid leaves small grids with few tasks)
+        rec_tuning = dict(tuning, rows_per_cta=0)
+        for key, fn in (("fwi_iteration_151x461", lambda: record_fwi_iteration(torch, arith, rec_tuning,
                                                                                 not args.no_cpu_baseline)),
-                        ("encoded_fwi_301x921", lambda: record_encoded(torch, arith, tuning, args.ess_iters)),
-                        ("enkf_201x461", lambda: record_enkf(torch, arith, tuning, not args.no_cpu_baseline)),
+                        ("encoded_fwi_301x921", lambda: record_encoded(torch, arith, rec_tuning, args.ess_iters)),
+                        ("enkf_201x461", lambda: record_enkf(torch, arith, rec_tuning, not args.no_cpu_baseline)),
                         ("lsrtm_151x461", lambda: record_lsrtm(torch, not args.no_cpu_baseline)),
                         ("learned_fwi", lambda: None if args.no_learned else learned_record(args))):
             try:
