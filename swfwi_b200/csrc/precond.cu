@@ -1,7 +1,7 @@
-// Learned preconditioner: BF16 tensor-core convolutions (forward, data
-// gradient, weight gradient), the encoder-decoder around them, its training
-// step and the features/scatter between the padded model grid and the
-// network's image.
+// Learned preconditioner: BF16 tensor-core convolutions (forward and data
+// gradient on tcgen05 with tensor-memory accumulators; weight gradient on
+// mma.sync), the encoder-decoder around them, its training step and the
+// features/scatter between the padded model grid and the network's image.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -9,6 +9,7 @@
 #include <random>
 #include "kernels.cuh"
 #include "precond.hpp"
+#include "stream.cuh"
 
 namespace swfwi {
 namespace {
@@ -45,74 +46,205 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<uint32_t *>(&v);
 }
 
-// ---------------------------------------------------------------- 3x3 conv
-// Implicit GEMM: M = pixels (16 consecutive columns of one image row per
-// warp), N = output channels (8*NJ per CTA), K = 9 taps x cin (16 channels
-// of one tap per mma).  Zero padding at the image edges.  F32: FP32 output
-// without bias (the data gradient), else BF16 output with bias and ReLU.
-template <int NJ, bool F32>
-__global__ void __launch_bounds__(128) k_conv3x3(const bf16 *__restrict__ in, int cin,
-                                                 const bf16 *__restrict__ w,
-                                                 const float *__restrict__ bias, void *out, int accum,
-                                                 int cout, int H, int W) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int nh = blockIdx.y;
-  const int n = nh / H, h = nh - n * H;
-  const int w0 = blockIdx.x * 64 + warp * 16;
-  if (w0 >= W) return;   // whole warp
-  const int co0 = blockIdx.z * (8 * NJ);
-  const int wa = w0 + g, wb = w0 + g + 8;
-  float acc[NJ][4];
+// ---------------------------------------------------------------- 3x3 conv, tcgen05
+// Implicit GEMM on the fifth-generation tensor cores.  A CTA of 128 threads
+// owns 128 consecutive pixels of the flattened (n, h, w) index (M = 128) and
+// every output channel (N = cout, a multiple of 16 up to 256); K = 9 taps x
+// cin, 16 channels per MMA.  The taps go in rounds of T (9, 3 or 1, the most
+// whose tiles fit the shared-memory budget): per round the threads copy, for
+// each of its taps, the 128 shifted pixel rows (zero-filled outside the
+// image) and the tap's weights into shared memory with cp.async, as K-major
+// core matrices without swizzle (8 rows x 16 bytes; the 8-row groups 256 B
+// apart, the two 8-channel halves of a 16-channel chunk 128 B apart).  With
+// more than one round, two stages: while the tensor cores run one round, the
+// copies of the next land in the other stage.  One thread issues a round's
+// T x cin/16 tcgen05.mma into the FP32 accumulator in tensor memory and
+// commits them to the stage's mbarrier; a stage is refilled only after its
+// barrier shows those MMAs done (bounded waits).  Narrow layers take all 9
+// taps in one round: one copy, MMA and commit latency per CTA instead of 9.  The epilogue reads the
+// accumulator 16 columns at a time (warp w holds the tensor-memory lanes,
+// i.e. pixels, 32w .. 32w+31) and writes BF16 with bias and ReLU, or FP32
+// (optionally added to the output).  A wait that gives up sets
+// g_conv_timeout; the CTA still frees its tensor memory.
+__device__ int g_conv_timeout;
+
+namespace tc {
+__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// shared-memory matrix descriptor: start address, leading (K) byte offset
+// 128, stride (8-row group) byte offset 256, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(256u >> 4) << 32) |
+         (1ull << 46);
+}
+__host__ __device__ inline int tmem_cols(int n) { return n <= 32 ? 32 : (n <= 64 ? 64 : (n <= 128 ? 128 : 256)); }
+// 16 bytes global -> shared, zero-filled when !valid (src is then not read)
+__device__ __forceinline__ void cp16(uint32_t dst, const void *src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// bytes of one stage of T taps (A and B tiles)
+__host__ __device__ inline int stage_bytes(int cin, int cout, int T) { return T * (cin / 16) * (4096 + 32 * cout); }
+constexpr int kStageBudget = 96 * 1024;   // shared memory the stages may take
+// taps per round: the most of 9, 3, 1 whose stages fit the budget
+__host__ __device__ inline int taps_per_round(int cin, int cout) {
+  if (stage_bytes(cin, cout, 9) <= kStageBudget) return 9;
+  return 2 * stage_bytes(cin, cout, 3) <= kStageBudget ? 3 : 1;
+}
+}  // namespace tc
+
+template <bool F32>
+__global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ in, int cin,
+                                                    const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                    void *out, int accum, int cout, int N, int H, int W) {
+  using namespace stream_detail;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int KC = cin / 16, T = tc::taps_per_round(cin, cout), R = 9 / T;
+  const int SB = tc::stage_bytes(cin, cout, T), NS = R > 1 ? 2 : 1;
+  // stage s at sm + s*SB: the round's A tiles (T x KC x 4 KB, tap-major),
+  // then its B tiles (T x KC x cout x 32 B)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NS * SB);   // one per stage
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long HW = (long long)H * W, P = (long long)N * HW;
+  const long long p0 = (long long)blockIdx.x * 128;
+  const uint32_t ncols = (uint32_t)tc::tmem_cols(cout);
+  // thread tid copies A row tid (its pixel, decoded once; valid = inside the
+  // batch) and the B rows co = tid, tid + 128, ... of every tap
+  const long long pm = p0 + tid;
+  const bool pin = pm < P;
+  const int pn = pin ? (int)(pm / HW) : 0, pr = pin ? (int)(pm - (long long)pn * HW) : 0;
+  const int ph = pr / W, pw = pr - ph * W;
+  // the row's place in a 16-channel chunk's A tile (core matrix, row within it)
+  const uint32_t arow = (uint32_t)((tid >> 3) * 256 + (tid & 7) * 16);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::saddr(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+  // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+  // K-major, N = cout, M = 128
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((128u >> 4) << 24);
+  const uint32_t sbase = tc::saddr(sm);
+
+  auto load_round = [&](int rd) {
+    const uint32_t sa = sbase + (uint32_t)((rd % NS) * SB), sb = sa + (uint32_t)(T * KC * 4096);
+    for (int t = 0; t < T; t++) {
+      const int tap = rd * T + t, ky = tap / 3, kx = tap - 3 * ky;
+      const uint32_t at = sa + (uint32_t)(t * KC * 4096) + arow, bt = sb + (uint32_t)(t * KC * cout * 32);
+      const int hh = ph + ky - 1, xx = pw + kx - 1;
+      const bool ok = pin && hh >= 0 && hh < H && xx >= 0 && xx < W;
+      const bf16 *src = ok ? in + (((long long)pn * H + hh) * W + xx) * cin : in;
+      // 16 bytes per step along the pixel's channels: chunk q >> 1, half q & 1
+      for (int q = 0; q < 2 * KC; q++)
+        tc::cp16(at + (uint32_t)((q >> 1) * 4096 + (q & 1) * 128), ok ? src + q * 8 : in, ok);
+      for (int co = tid; co < cout; co += 128) {
+        const bf16 *wr = w + ((long long)co * 9 + tap) * cin;
+        const uint32_t brow = bt + (uint32_t)((co >> 3) * 256 + (co & 7) * 16);
+        for (int q = 0; q < 2 * KC; q++)
+          tc::cp16(brow + (uint32_t)((q >> 1) * cout * 32 + (q & 1) * 128), wr + q * 8, true);
+      }
+    }
+    tc::cp_commit();
+  };
+
+  bool ok = true;
+  load_round(0);
+  for (int rd = 0; rd < R && ok; rd++) {
+    if (rd + 1 < R) {
+      // the next round's stage was read by the MMAs of round rd-1: wait for them
+      if (rd >= 1 && !__syncthreads_and(mbar_wait(&bar[(rd + 1) & 1], (uint32_t)(((rd - 1) >> 1) & 1)))) {
+        ok = false;
+        break;
+      }
+      load_round(rd + 1);
+      tc::cp_wait<1>();   // this round's copies are complete, the next round's may be in flight
+    } else {
+      tc::cp_wait<0>();
+    }
+    // the tiles were written through the generic proxy; the MMA reads them
+    // through the async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = sbase + (uint32_t)((rd % NS) * SB), sb = sa + (uint32_t)(T * KC * 4096);
+      for (int kc = 0; kc < T * KC; kc++) {   // (tap within the round, 16-channel chunk)
+        const uint64_t ad = tc::kmajor_desc(sa + kc * 4096);
+        const uint64_t bd = tc::kmajor_desc(sb + kc * cout * 32);
+        const uint32_t acc = (rd > 0 || kc > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(taddr),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       tc::saddr(&bar[rd & 1]))
+                   : "memory");
+    }
+  }
+  // the last commit (round R-1, its barrier's ((R-1)/2 + 1)-th phase) covers every MMA
+  if (ok && !__syncthreads_and(mbar_wait(&bar[(R - 1) & 1], (uint32_t)(((R - 1) >> 1) & 1)))) ok = false;
+  tc::cp_wait<0>();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const long long p = p0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < cout; c0 += 16) {
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (p < P) {
+        if constexpr (F32) {
+          float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(out) + p * cout + c0);
 #pragma unroll
-  for (int j = 0; j < NJ; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-  for (int ky = 0; ky < 3; ky++) {
-    const int hh = h + ky - 1;
-    const bool hok = hh >= 0 && hh < H;
-    const bf16 *row = in + (long long)(n * H + (hok ? hh : 0)) * W * cin;
-    for (int kx = 0; kx < 3; kx++) {
-      const int xa = wa + kx - 1, xb = wb + kx - 1;
-      const bool oka = hok && wa < W && xa >= 0 && xa < W;
-      const bool okb = hok && wb < W && xb >= 0 && xb < W;
-      const bf16 *pa = row + (long long)(oka ? xa : 0) * cin + 2 * t;
-      const bf16 *pb = row + (long long)(okb ? xb : 0) * cin + 2 * t;
-      const bf16 *wt = w + ((long long)(co0 + g) * 9 + ky * 3 + kx) * cin + 2 * t;
-      for (int c0 = 0; c0 < cin; c0 += 16) {
-        const uint32_t a0 = oka ? ldu32(pa + c0) : 0u, a2 = oka ? ldu32(pa + c0 + 8) : 0u;
-        const uint32_t a1 = okb ? ldu32(pb + c0) : 0u, a3 = okb ? ldu32(pb + c0 + 8) : 0u;
+          for (int i = 0; i < 4; i++) {
+            float4 v = make_float4(__uint_as_float(r[4 * i]), __uint_as_float(r[4 * i + 1]),
+                                   __uint_as_float(r[4 * i + 2]), __uint_as_float(r[4 * i + 3]));
+            if (accum) {
+              const float4 q = o[i];
+              v.x += q.x; v.y += q.y; v.z += q.z; v.w += q.w;
+            }
+            o[i] = v;
+          }
+        } else {
+          uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(out) + p * cout + c0);
+          uint32_t pk[8];
 #pragma unroll
-        for (int j = 0; j < NJ; j++) {
-          const bf16 *wj = wt + (long long)j * 8 * 9 * cin + c0;
-          mma_bf16(acc[j], a0, a1, a2, a3, ldu32(wj), ldu32(wj + 8));
+          for (int i = 0; i < 8; i++)
+            pk[i] = pack_bf16(fmaxf(__uint_as_float(r[2 * i]) + bias[c0 + 2 * i], 0.0f),
+                              fmaxf(__uint_as_float(r[2 * i + 1]) + bias[c0 + 2 * i + 1], 0.0f));
+          o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
         }
       }
     }
+  } else if (tid == 0) {
+    atomicExch(&g_conv_timeout, 1);
+    // bounded: whatever MMAs are still in flight, before their tensor memory goes
+    mbar_wait(&bar[0], 0u);
+    mbar_wait(&bar[1], 1u);
   }
-  const long long pixa = (long long)nh * W + wa, pixb = (long long)nh * W + wb;
-#pragma unroll
-  for (int j = 0; j < NJ; j++) {
-    const int co = co0 + j * 8 + 2 * t;
-    if constexpr (F32) {
-      float2 *o = reinterpret_cast<float2 *>(out);
-      if (wa < W) {
-        float2 v = make_float2(acc[j][0], acc[j][1]);
-        if (accum) { float2 q = o[(pixa * cout + co) / 2]; v.x += q.x; v.y += q.y; }
-        o[(pixa * cout + co) / 2] = v;
-      }
-      if (wb < W) {
-        float2 v = make_float2(acc[j][2], acc[j][3]);
-        if (accum) { float2 q = o[(pixb * cout + co) / 2]; v.x += q.x; v.y += q.y; }
-        o[(pixb * cout + co) / 2] = v;
-      }
-    } else {
-      uint32_t *o = reinterpret_cast<uint32_t *>(out);
-      const float b0 = bias[co], b1 = bias[co + 1];
-      if (wa < W)
-        o[(pixa * cout + co) / 2] = pack_bf16(fmaxf(acc[j][0] + b0, 0.0f), fmaxf(acc[j][1] + b1, 0.0f));
-      if (wb < W)
-        o[(pixb * cout + co) / 2] = pack_bf16(fmaxf(acc[j][2] + b0, 0.0f), fmaxf(acc[j][3] + b1, 0.0f));
-    }
-  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
 // Weight gradient of one tap over one chunk of pixels:
@@ -552,11 +684,32 @@ __global__ void k_illum(float *__restrict__ illum, const float *__restrict__ p, 
   }
 }
 
-template <int NJ, bool F32>
-void conv_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out, bool accum,
-             int cout, int N, int H, int W, cudaStream_t st) {
-  dim3 grid((W + 63) / 64, N * H, cout / (8 * NJ));
-  k_conv3x3<NJ, F32><<<grid, 128, 0, st>>>(in, cin, w, bias, out, accum ? 1 : 0, cout, H, W);
+// Dynamic shared memory of a launch: two stages, the barriers, the tensor
+// memory address and the decoded pixels -- raised where needed so that no
+// more CTAs are resident on an SM than its 512 tensor-memory columns hold
+// (a CTA that cannot allocate would wait inside tcgen05.alloc).
+size_t conv_tc_smem(int cin, int cout) {
+  const int T = tc::taps_per_round(cin, cout);
+  const size_t need = (T == 9 ? 1 : 2) * (size_t)tc::stage_bytes(cin, cout, T) + 32;
+  const int fit = 512 / tc::tmem_cols(cout);   // CTAs whose accumulators fit
+  if (fit >= 16) return need;                 // 16 CTAs of 128 threads fill an SM
+  const size_t sm_bytes = 228 * 1024, reserve = 1024;   // per SM, per CTA
+  const size_t cap = sm_bytes / (fit + 1) - reserve + 16;   // fit + 1 CTAs no longer fit
+  return std::max(need, cap);
+}
+
+template <bool F32>
+void conv_tc_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out, bool accum, int cout,
+                int N, int H, int W, cudaStream_t st) {
+  static const bool attr = [] {
+    SWFWI_CUDA(cudaFuncSetAttribute(k_conv3x3_tc<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)conv_tc_smem(128, 256)));   // the largest accepted widths
+    return true;
+  }();
+  (void)attr;
+  const long long P = (long long)N * H * W;
+  k_conv3x3_tc<F32><<<(unsigned)((P + 127) / 128), 128, conv_tc_smem(cin, cout), st>>>(
+      in, cin, w, bias, out, accum ? 1 : 0, cout, N, H, W);
   noted();
 }
 
@@ -595,19 +748,12 @@ int roundup8(int v) { return (v + 7) / 8 * 8; }
 
 void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out,
                     bool out_f32, bool accum, int cout, int N, int H, int W, cudaStream_t st) {
-  SWFWI_REQUIRE(cin > 0 && cin % 16 == 0 && cout > 0 && cout % 16 == 0, "conv widths must be multiples of 16");
-  SWFWI_REQUIRE(N > 0 && H > 0 && W > 0 && (long long)N * H <= 65535, "conv image size out of range");
+  SWFWI_REQUIRE(cin > 0 && cin % 16 == 0 && cin <= 128 && cout > 0 && cout % 16 == 0 && cout <= 256,
+                "conv widths must be multiples of 16, at most 128 in and 256 out");
+  SWFWI_REQUIRE(N > 0 && H > 0 && W > 0, "conv image size out of range");
   SWFWI_REQUIRE(out_f32 || bias, "BF16 conv output needs a bias");
-  const int nj = cout % 64 == 0 ? 8 : (cout % 32 == 0 ? 4 : 2);
-  if (out_f32) {
-    if (nj == 8) conv_go<8, true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
-    else if (nj == 4) conv_go<4, true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
-    else conv_go<2, true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
-  } else {
-    if (nj == 8) conv_go<8, false>(in, cin, w, bias, out, false, cout, N, H, W, st);
-    else if (nj == 4) conv_go<4, false>(in, cin, w, bias, out, false, cout, N, H, W, st);
-    else conv_go<2, false>(in, cin, w, bias, out, false, cout, N, H, W, st);
-  }
+  if (out_f32) conv_tc_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+  else conv_tc_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
 }
 
 size_t conv3x3_wgrad_scratch(int cout, int cin, int N, int H, int W) {
@@ -874,6 +1020,13 @@ double Preconditioner::backward(const float *t) {
   double loss = 0;
   SWFWI_CUDA(cudaMemcpyAsync(&loss, red_.get(), sizeof(double), cudaMemcpyDeviceToHost, st_));
   SWFWI_CUDA(cudaStreamSynchronize(st_));
+  int timeout = 0;
+  SWFWI_CUDA(cudaMemcpyFromSymbol(&timeout, g_conv_timeout, sizeof(int)));
+  if (timeout) {
+    const int zero = 0;
+    SWFWI_CUDA(cudaMemcpyToSymbol(g_conv_timeout, &zero, sizeof(int)));
+    throw Error(SWFWI_ERR_TIMEOUT, "a convolution's bounded wait on its tensor-core MMAs gave up");
+  }
   if (!std::isfinite(loss)) throw Error(SWFWI_ERR_NONFINITE, "preconditioner loss is not finite");
   return loss / (double)P0;
 }
