@@ -23,24 +23,6 @@ inline unsigned blocks_for(long long n, int threads = kEw) {
   return (unsigned)std::max(1LL, std::min(b, 148LL * 64));
 }
 
-__device__ __forceinline__ uint32_t ldu32(const bf16 *p) {
-  return __ldg(reinterpret_cast<const unsigned int *>(p));
-}
-
-// D = A(16x16, row) * B(16x8, col) + D, bf16 operands, f32 accumulate.
-// Fragment layout (PTX ISA, mma.m16n8k16 .bf16): with g = lane/4, t = lane%4,
-// a0 = A[g][2t..2t+1], a1 = A[g+8][2t..], a2 = A[g][2t+8..], a3 = A[g+8][2t+8..],
-// b0 = B[2t..2t+1][g], b1 = B[2t+8..2t+9][g],
-// c0,c1 = D[g][2t..2t+1], c2,c3 = D[g+8][2t..2t+1]; lower k in the low half.
-__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                         uint32_t a3, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t *>(&v);
@@ -247,87 +229,167 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ in,
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-// Weight gradient of one tap over one chunk of pixels:
-// part[chunk][co][tap][ci] = sum_{p in chunk} dz[p][co] x[p + tap][ci].
-// GEMM M = output channels (16 per warp, 64 per CTA), N = input channels
-// (8*NJ), K = pixels (32 per stage, staged transposed in shared memory so
-// that fragment pairs run along pixels).  The chunks are summed afterwards
-// in a fixed order (k_reduce_rows): training is bit-reproducible.
-template <int NJ>
-__global__ void __launch_bounds__(128) k_conv3x3_wgrad(const bf16 *__restrict__ dz, int cout,
-                                                       const bf16 *__restrict__ x,
-                                                       float *__restrict__ part, int N, int H, int W,
-                                                       int pix_per_cta) {
-  constexpr int CIN = 8 * NJ, KS = 32, LD = 40;
-  __shared__ __align__(16) uint16_t zt[64][LD];
-  __shared__ __align__(16) uint16_t xt[CIN][LD];
-  const int tap = blockIdx.y, ky = tap / 3, kx = tap - 3 * (tap / 3);
-  const int co0 = blockIdx.z * 64;
-  const int ncol = min(64, cout - co0);
-  const long long P = (long long)N * H * W;
-  const long long p_begin = (long long)blockIdx.x * pix_per_cta;
-  const long long p_end = min(P, p_begin + pix_per_cta);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const bool mw = warp * 16 < ncol;
-  const int HW = H * W;
-  float acc[NJ][4];
-#pragma unroll
-  for (int j = 0; j < NJ; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-  for (long long pb = p_begin; pb < p_end; pb += KS) {
-    const int zpairs = ncol / 2;
-    for (int e = threadIdx.x; e < KS * zpairs; e += 128) {
-      const int i = e / zpairs, cp = e - i * zpairs;
-      const long long p = pb + i;
-      uint32_t v = 0;
-      if (p < p_end) v = ldu32(dz + p * cout + co0 + 2 * cp);
-      zt[2 * cp][i] = (uint16_t)(v & 0xffffu);
-      zt[2 * cp + 1][i] = (uint16_t)(v >> 16);
-    }
-    constexpr int xpairs = CIN / 2;
-    for (int e = threadIdx.x; e < KS * xpairs; e += 128) {
-      const int i = e / xpairs, cp = e - i * xpairs;
-      const long long p = pb + i;
-      uint32_t v = 0;
-      if (p < p_end) {
-        const int n = (int)(p / HW);
-        const int r = (int)(p - (long long)n * HW);
-        const int h = r / W, w = r - h * W;
-        const int hh = h + ky - 1, ww = w + kx - 1;
-        if (hh >= 0 && hh < H && ww >= 0 && ww < W)
-          v = ldu32(x + ((long long)(n * H + hh) * W + ww) * CIN + 2 * cp);
-      }
-      xt[2 * cp][i] = (uint16_t)(v & 0xffffu);
-      xt[2 * cp + 1][i] = (uint16_t)(v >> 16);
+// ---------------------------------------------------------------- weight gradient, tcgen05
+// part[chunk][co][tap * cin + ci] = sum_{p in chunk} dz[p][co] x[p + tap][ci]
+// as D (M x N) = A (M x K) B (K x N) on the fifth-generation tensor cores:
+// M = output channels (padded to 128 with zero rows), N = a tile of the
+// 9 * cin (tap, input channel) columns, K = the chunk's pixels, 16 per MMA.
+// Both operands are MN-major (NHWC keeps a pixel's channels contiguous), as
+// core matrices without swizzle: 8 pixels x 16 bytes (8 channels), the
+// 8-channel groups 128 B apart, the two 8-pixel halves of a 16-pixel step
+// (16 groups x 128 B) apart.  Rounds of kWgRound steps are copied with
+// cp.async into two stages while the tensor cores run the previous round;
+// each round's MMAs are committed to its stage's mbarrier (bounded waits).
+// The chunks are summed afterwards in a fixed order (k_reduce_rows):
+// training stays bit-reproducible.
+constexpr int kWgRound = 4;   // 16-pixel steps per round (64 pixels)
+
+__host__ __device__ inline int wg_tiles(int cin) { return (9 * cin + 255) / 256; }
+__host__ __device__ inline int wg_cols(int cin) { return ((9 * cin + wg_tiles(cin) - 1) / wg_tiles(cin) + 15) / 16 * 16; }
+__host__ __device__ inline int wg_stage_bytes(int cin) { return kWgRound * (4096 + 32 * wg_cols(cin)); }
+
+__global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dz, int cout, const bf16 *__restrict__ x,
+                                                  int cin, float *__restrict__ part, int N, int H, int W, int ppc) {
+  using namespace stream_detail;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int NT = 9 * cin, NNmax = wg_cols(cin);
+  const int n0 = blockIdx.y * NNmax, NN = min(NNmax, NT - n0);   // this CTA's columns
+  const int SB = wg_stage_bytes(cin);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 2 * SB);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  int *dec = reinterpret_cast<int *>(bar + 3);   // [stage][3][64]: n (-1: none), h, w of the round's pixels
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long HW = (long long)H * W, P = (long long)N * HW;
+  const long long pb = (long long)blockIdx.x * ppc, pe = min(P, pb + ppc);
+  const int R = (int)((pe - pb + 16 * kWgRound - 1) / (16 * kWgRound));   // rounds
+  const uint32_t ncols = (uint32_t)tc::tmem_cols(NN);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::saddr(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+  // kind::f16: FP32 accumulator, BF16 A and B, both MN-major, N = NN, M = 128
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                         ((uint32_t)(NN >> 3) << 17) | ((128u >> 4) << 24);
+  const uint32_t sbase = tc::saddr(sm);
+  const int zgroups = cout / 8, bgroups = NN / 8;
+
+  auto load_round = [&](int rd) {
+    const int st = rd & 1;
+    int *dn = dec + st * 192, *dh = dn + 64, *dw = dh + 64;
+    if (tid < 64) {   // decode the round's 64 pixels once
+      const long long p = pb + (long long)rd * 64 + tid;
+      const int n = p < pe ? (int)(p / HW) : -1;
+      const int r = p < pe ? (int)(p - (long long)n * HW) : 0;
+      dn[tid] = n;
+      dh[tid] = r / W;
+      dw[tid] = r - (r / W) * W;
     }
     __syncthreads();
-    if (mw) {
-      const int r0 = warp * 16 + g;
+    const uint32_t sa = sbase + (uint32_t)(st * SB), sb = sa + (uint32_t)(kWgRound * 4096);
+    // A: 64 pixels x 16 channel groups (groups past cout are zero rows)
+    for (int u = tid; u < 64 * 16; u += 128) {
+      const int g = u & 15, pi = u >> 4, ks = pi >> 4, r = pi & 15;
+      const bool ok = g < zgroups && dn[pi] >= 0;
+      const long long p = pb + (long long)rd * 64 + pi;
+      tc::cp16(sa + (uint32_t)(ks * 4096 + (r >> 3) * 2048 + g * 128 + (r & 7) * 16), ok ? dz + p * cout + g * 8 : dz,
+               ok);
+    }
+    // B: 64 pixels x this tile's (tap, 8-channel) groups, zero outside the image
+    for (int u = tid; u < 64 * bgroups; u += 128) {
+      const int g = u % bgroups, pi = u / bgroups, ks = pi >> 4, r = pi & 15;
+      const int col = n0 + g * 8, tap = col / cin, c8 = col - tap * cin;
+      const int ky = tap / 3, kx = tap - 3 * ky;
+      const int n = dn[pi], hh = dh[pi] + ky - 1, xx = dw[pi] + kx - 1;
+      const bool ok = n >= 0 && hh >= 0 && hh < H && xx >= 0 && xx < W;
+      tc::cp16(sb + (uint32_t)(ks * NN * 32 + (r >> 3) * (NN * 16) + g * 128 + (r & 7) * 16),
+               ok ? x + (((long long)n * H + hh) * W + xx) * cin + c8 : x, ok);
+    }
+    tc::cp_commit();
+  };
+
+  bool ok = true;
+  if (R > 0) load_round(0);
+  for (int rd = 0; rd < R && ok; rd++) {
+    if (rd + 1 < R) {
+      if (rd >= 1 && !__syncthreads_and(mbar_wait(&bar[(rd + 1) & 1], (uint32_t)(((rd - 1) >> 1) & 1)))) {
+        ok = false;
+        break;
+      }
+      load_round(rd + 1);
+      tc::cp_wait<1>();
+    } else {
+      tc::cp_wait<0>();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = sbase + (uint32_t)((rd & 1) * SB), sb = sa + (uint32_t)(kWgRound * 4096);
+      for (int ks = 0; ks < kWgRound; ks++) {
+        // MN-major descriptors: leading (K-half) offset, stride (8-channel group) offset 128
+        const uint64_t ad = (uint64_t)(((sa + ks * 4096) >> 4) & 0x3FFFu) | ((uint64_t)(2048u >> 4) << 16) |
+                            ((uint64_t)(128u >> 4) << 32) | (1ull << 46);
+        const uint64_t bd = (uint64_t)(((sb + ks * NN * 32) >> 4) & 0x3FFFu) |
+                            ((uint64_t)((uint32_t)(NN * 16) >> 4) << 16) | ((uint64_t)(128u >> 4) << 32) | (1ull << 46);
+        const uint32_t acc = (rd > 0 || ks > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(taddr),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       tc::saddr(&bar[rd & 1]))
+                   : "memory");
+    }
+  }
+  if (ok && R > 0 && !__syncthreads_and(mbar_wait(&bar[(R - 1) & 1], (uint32_t)(((R - 1) >> 1) & 1)))) ok = false;
+  tc::cp_wait<0>();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok && warp * 32 < cout) {   // lanes = output channels
+    const int co = warp * 32 + lane;
+    float *dst = part + ((long long)blockIdx.x * cout + co) * NT + n0;
+    for (int c0 = 0; c0 < NN; c0 += 16) {
+      uint32_t r[16];
+      if (R > 0) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
 #pragma unroll
-      for (int ks = 0; ks < KS; ks += 16) {
-        const uint32_t a0 = *reinterpret_cast<const uint32_t *>(&zt[r0][ks + 2 * t]);
-        const uint32_t a1 = *reinterpret_cast<const uint32_t *>(&zt[r0 + 8][ks + 2 * t]);
-        const uint32_t a2 = *reinterpret_cast<const uint32_t *>(&zt[r0][ks + 2 * t + 8]);
-        const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&zt[r0 + 8][ks + 2 * t + 8]);
+        for (int i = 0; i < 16; i++) r[i] = 0u;   // an empty chunk contributes zeros
+      }
+      if (co < cout) {
+        float4 *o = reinterpret_cast<float4 *>(dst + c0);
 #pragma unroll
-        for (int j = 0; j < NJ; j++) {
-          const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&xt[j * 8 + g][ks + 2 * t]);
-          const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&xt[j * 8 + g][ks + 2 * t + 8]);
-          mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
-        }
+        for (int i = 0; i < 4; i++)
+          o[i] = make_float4(__uint_as_float(r[4 * i]), __uint_as_float(r[4 * i + 1]), __uint_as_float(r[4 * i + 2]),
+                             __uint_as_float(r[4 * i + 3]));
       }
     }
-    __syncthreads();
+  } else if (!ok && tid == 0) {
+    atomicExch(&g_conv_timeout, 1);
+    mbar_wait(&bar[0], 0u);   // bounded: whatever MMAs are still in flight
+    mbar_wait(&bar[1], 1u);
   }
-  if (!mw) return;
-  float *dw = part + (long long)blockIdx.x * cout * 9 * CIN;
-  const int coa = co0 + warp * 16 + g, cob = coa + 8;
-#pragma unroll
-  for (int j = 0; j < NJ; j++) {
-    const int ci = j * 8 + 2 * t;
-    *reinterpret_cast<float2 *>(dw + ((long long)coa * 9 + tap) * CIN + ci) = make_float2(acc[j][0], acc[j][1]);
-    *reinterpret_cast<float2 *>(dw + ((long long)cob * 9 + tap) * CIN + ci) = make_float2(acc[j][2], acc[j][3]);
-  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
 // out[i] = sum over r = 0..rows-1, in order, of part[r * len + i]
@@ -713,23 +775,38 @@ void conv_tc_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void 
   noted();
 }
 
-constexpr long long kWgradChunks = 128;   // pixel chunks of a weight gradient (at most)
 constexpr int kRedBlocks = 256;           // blocks of the channel sums
 
-long long wgrad_pix_per_chunk(long long P) {
-  return 32 * std::max(1LL, (P + 32 * kWgradChunks - 1) / (32 * kWgradChunks));
+// Pixels per chunk of a weight gradient: a multiple of one round (64), about
+// 444 CTAs (3 per SM) over the column tiles.
+long long wgrad_pix_per_chunk(long long P, int cin) {
+  const long long chunks = std::max(1, 444 / wg_tiles(cin));
+  return 64 * std::max(1LL, (P + 64 * chunks - 1) / (64 * chunks));
 }
 
-template <int NJ>
-void wgrad_go(const bf16 *dz, int cout, const bf16 *x, float *dw, float *part, int N, int H, int W,
-              cudaStream_t st) {
+size_t wgrad_tc_smem(int cin) {
+  const size_t need = 2 * (size_t)wg_stage_bytes(cin) + 32 + 2 * 3 * 64 * 4;
+  const int fit = 512 / tc::tmem_cols(wg_cols(cin));   // CTAs whose accumulators fit
+  if (fit >= 16) return need;
+  const size_t cap = 228 * 1024 / (fit + 1) - 1024 + 16;   // fit + 1 CTAs no longer fit
+  return std::max(need, cap);
+}
+
+void wgrad_tc_go(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, float *part, int N, int H, int W,
+                 cudaStream_t st) {
+  static const bool attr = [] {
+    SWFWI_CUDA(cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)wgrad_tc_smem(128)));   // the largest accepted width
+    return true;
+  }();
+  (void)attr;
   const long long P = (long long)N * H * W;
-  const long long ppc = wgrad_pix_per_chunk(P);
+  const long long ppc = wgrad_pix_per_chunk(P, cin);
   const unsigned chunks = (unsigned)((P + ppc - 1) / ppc);
-  dim3 grid(chunks, 9, (cout + 63) / 64);
-  k_conv3x3_wgrad<NJ><<<grid, 128, 0, st>>>(dz, cout, x, part, N, H, W, (int)ppc);
+  dim3 grid(chunks, wg_tiles(cin));
+  k_wgrad_tc<<<grid, 128, wgrad_tc_smem(cin), st>>>(dz, cout, x, cin, part, N, H, W, (int)ppc);
   noted();
-  const long long len = (long long)cout * 9 * 8 * NJ;
+  const long long len = (long long)cout * 9 * cin;
   k_reduce_rows<<<blocks_for(len), kEw, 0, st>>>(part, (int)chunks, len, dw);
   noted();
 }
@@ -758,24 +835,17 @@ void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, v
 
 size_t conv3x3_wgrad_scratch(int cout, int cin, int N, int H, int W) {
   const long long P = (long long)N * H * W;
-  const long long ppc = wgrad_pix_per_chunk(P);
+  const long long ppc = wgrad_pix_per_chunk(P, cin);
   return (size_t)((P + ppc - 1) / ppc) * cout * 9 * cin;
 }
 
 void launch_conv3x3_wgrad(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, float *scratch,
                           size_t scratch_floats, int N, int H, int W, cudaStream_t st) {
-  SWFWI_REQUIRE(cout > 0 && cout % 16 == 0, "conv widths must be multiples of 16");
+  SWFWI_REQUIRE(cout > 0 && cout % 16 == 0 && cout <= 128, "weight gradient: output width must be a multiple of 16, at most 128");
+  SWFWI_REQUIRE(cin > 0 && cin % 16 == 0 && cin <= 128, "weight gradient: input width must be a multiple of 16, at most 128");
   SWFWI_REQUIRE(scratch && scratch_floats >= conv3x3_wgrad_scratch(cout, cin, N, H, W),
                 "weight gradient scratch too small");
-  switch (cin) {
-    case 16: wgrad_go<2>(dz, cout, x, dw, scratch, N, H, W, st); break;
-    case 32: wgrad_go<4>(dz, cout, x, dw, scratch, N, H, W, st); break;
-    case 48: wgrad_go<6>(dz, cout, x, dw, scratch, N, H, W, st); break;
-    case 64: wgrad_go<8>(dz, cout, x, dw, scratch, N, H, W, st); break;
-    case 96: wgrad_go<12>(dz, cout, x, dw, scratch, N, H, W, st); break;
-    case 128: wgrad_go<16>(dz, cout, x, dw, scratch, N, H, W, st); break;
-    default: throw Error(SWFWI_ERR_BAD_ARG, "weight gradient: input width must be 16/32/48/64/96/128");
-  }
+  wgrad_tc_go(dz, cout, x, cin, dw, scratch, N, H, W, st);
 }
 
 void launch_illum_accum(float *illum, const float *p, long long fstride, int n, int nxpad, int nzpad,
