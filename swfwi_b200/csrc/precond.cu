@@ -1,7 +1,8 @@
-// Learned preconditioner: BF16 tensor-core convolutions (forward and data
-// gradient on tcgen05 with tensor-memory accumulators; weight gradient on
-// mma.sync), the encoder-decoder around them, its training step and the
-// features/scatter between the padded model grid and the network's image.
+// Learned preconditioner: BF16 convolutions on the fifth-generation tensor
+// cores (forward, data gradient and weight gradient: tcgen05.mma with FP32
+// accumulators in tensor memory), the encoder-decoder around them, its
+// training step and the features/scatter between the padded model grid and
+// the network's image.
 #include <algorithm>
 #include <atomic>
 #include <cmath>

@@ -17,10 +17,10 @@
 //   up 2x, concat s0; d0a,d0b: c1+c0 -> c0 -> c0     -> u0
 //   out: 1x1 conv c0 -> 1 (no activation, FP32)
 // Activations and conv weights are BF16 (NHWC, weights [co][ky][kx][ci]);
-// every product accumulates in FP32 on the tensor cores (mma.sync
-// m16n8k16 bf16); master weights, Adam moments, gradients, the loss and the
-// output layer are FP32.  H and W must be multiples of 8; every width a
-// multiple of 16.
+// every product accumulates in FP32 on the tensor cores (tcgen05.mma
+// kind::f16, BF16 operands, accumulators in tensor memory); master weights,
+// Adam moments, gradients, the loss and the output layer are FP32.  H and W
+// must be multiples of 8; every width a multiple of 16, at most 128.
 #pragma once
 #include <cuda_bf16.h>
 #include <cstdint>
