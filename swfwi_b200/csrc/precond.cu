@@ -230,6 +230,183 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const bf16 *__restrict__ in,
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
+// ---------------------------------------------------------------- 3x3 conv, tcgen05, row tiles
+// The same implicit GEMM with row-aligned tiles: the CTA's 128 pixels are
+// 16 groups of 8 consecutive pixels of one image row each.  For every group
+// the three input rows it needs (h-1, h, h+1) are staged once, 10 pixels
+// wide (the group and a one-pixel halo), as 16-byte rows per 8-channel half:
+// A(tap ky, kx) is then the staged rows of ky seen from a start address
+// shifted by kx rows, with the 8-row groups 160 B apart -- the three column
+// taps share one copy, and the input is copied 30/8 times instead of 9.
+// The rows of ky go in rounds (all three at once when they fit, else one
+// ky a round, double-buffered).
+namespace tg {
+constexpr int kGroupBytes = 160;                  // 10 pixels x 16 bytes
+constexpr int kPlaneRow = 16 * kGroupBytes;       // one ky row of the 16 groups
+__host__ __device__ inline int rows_per_round(int cin, int cout) {
+  const int kc = cin / 16;
+  if (kc * (2 * 3 * kPlaneRow + 9 * 32 * cout) <= 96 * 1024) return 3;
+  return 1;
+}
+__host__ __device__ inline int stage_bytes(int cin, int cout, int nky) {
+  const int kc = cin / 16;
+  return kc * (2 * nky * kPlaneRow + 3 * nky * 32 * cout);
+}
+}  // namespace tg
+
+template <bool F32>
+__global__ void __launch_bounds__(128) k_conv3x3_tg(const bf16 *__restrict__ in, int cin,
+                                                    const bf16 *__restrict__ w, const float *__restrict__ bias,
+                                                    void *out, int accum, int cout, int N, int H, int W) {
+  using namespace stream_detail;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int KC = cin / 16, NKY = tg::rows_per_round(cin, cout), R = 3 / NKY, NS = R > 1 ? 2 : 1;
+  const int SB = tg::stage_bytes(cin, cout, NKY), ABYTES = KC * 2 * NKY * tg::kPlaneRow;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NS * SB);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+  int *gn = reinterpret_cast<int *>(bar + 3), *gh = gn + 16, *gw = gh + 16;   // the 16 groups (n = -1: none)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int GW = (W + 7) / 8;
+  const long long groups = (long long)N * H * GW;
+  const uint32_t ncols = (uint32_t)tc::tmem_cols(cout);
+  if (tid < 16) {
+    const long long gi = (long long)blockIdx.x * 16 + tid;
+    const long long row = gi / GW;
+    gn[tid] = gi < groups ? (int)(row / H) : -1;
+    gh[tid] = gi < groups ? (int)(row % H) : 0;
+    gw[tid] = gi < groups ? (int)(gi % GW) * 8 : 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::saddr(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = *tslot;
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) | ((128u >> 4) << 24);
+  const uint32_t sbase = tc::saddr(sm);
+
+  // round rd: input rows ky = rd*NKY .. +NKY-1 and the taps 3*ky + kx
+  auto load_round = [&](int rd) {
+    const uint32_t sa = sbase + (uint32_t)((rd % NS) * SB), sb = sa + (uint32_t)ABYTES;
+    // A: [kc][half][kyl][group][10 px][16 B], 16 bytes per step along a pixel's channels
+    for (int u = tid; u < NKY * 16 * 10 * 2 * KC; u += 128) {
+      const int q = u % (2 * KC), v = u / (2 * KC), px = v % 10, gk = v / 10, g = gk & 15, kyl = gk >> 4;
+      const int n = gn[g], hh = gh[g] + rd * NKY + kyl - 1, xx = gw[g] + px - 1;
+      const bool ok = n >= 0 && hh >= 0 && hh < H && xx >= 0 && xx < W;
+      tc::cp16(sa + (uint32_t)((((q >> 1) * 2 + (q & 1)) * NKY + kyl) * tg::kPlaneRow + g * tg::kGroupBytes + px * 16),
+               ok ? in + (((long long)n * H + hh) * W + xx) * cin + q * 8 : in, ok);
+    }
+    // B: the round's 3*NKY taps x [kc] x cout rows in K-major core matrices
+    for (int u = tid; u < 3 * NKY * cout * 2 * KC; u += 128) {
+      const int q = u % (2 * KC), v = u / (2 * KC), co = v % cout, t = v / cout;
+      const int tap = rd * 3 * NKY + t;
+      tc::cp16(sb + (uint32_t)((t * KC + (q >> 1)) * cout * 32 + ((co >> 3) * 2 + (q & 1)) * 128 + (co & 7) * 16),
+               w + ((long long)co * 9 + tap) * cin + q * 8, true);
+    }
+    tc::cp_commit();
+  };
+
+  bool ok = true;
+  load_round(0);
+  for (int rd = 0; rd < R && ok; rd++) {
+    if (rd + 1 < R) {
+      if (rd >= 1 && !__syncthreads_and(mbar_wait(&bar[(rd + 1) & 1], (uint32_t)(((rd - 1) >> 1) & 1)))) {
+        ok = false;
+        break;
+      }
+      load_round(rd + 1);
+      tc::cp_wait<1>();
+    } else {
+      tc::cp_wait<0>();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = sbase + (uint32_t)((rd % NS) * SB), sb = sa + (uint32_t)ABYTES;
+      for (int t = 0; t < 3 * NKY; t++) {
+        const int kyl = t / 3, kx = t - 3 * kyl;
+        for (int kc = 0; kc < KC; kc++) {
+          // A rows: group g at g*160, row i of the group at (i + kx)*16; the
+          // channel halves NKY planes apart
+          const uint32_t a_addr = sa + (uint32_t)((kc * 2 * NKY + kyl) * tg::kPlaneRow + kx * 16);
+          const uint64_t ad = (uint64_t)((a_addr >> 4) & 0x3FFFu) |
+                              ((uint64_t)((uint32_t)(NKY * tg::kPlaneRow) >> 4) << 16) |
+                              ((uint64_t)((uint32_t)tg::kGroupBytes >> 4) << 32) | (1ull << 46);
+          const uint64_t bd = tc::kmajor_desc(sb + (uint32_t)((t * KC + kc) * cout * 32));
+          const uint32_t acc = (rd > 0 || t > 0 || kc > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(taddr),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       tc::saddr(&bar[rd & 1]))
+                   : "memory");
+    }
+  }
+  if (ok && !__syncthreads_and(mbar_wait(&bar[(R - 1) & 1], (uint32_t)(((R - 1) >> 1) & 1)))) ok = false;
+  tc::cp_wait<0>();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int r = warp * 32 + lane, g = r >> 3, i = r & 7;
+    const bool valid = gn[g] >= 0 && gw[g] + i < W;
+    const long long p = valid ? ((long long)gn[g] * H + gh[g]) * W + gw[g] + i : 0;
+    for (int c0 = 0; c0 < cout; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (valid) {
+        if constexpr (F32) {
+          float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(out) + p * cout + c0);
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            float4 x4 = make_float4(__uint_as_float(v[4 * k]), __uint_as_float(v[4 * k + 1]),
+                                    __uint_as_float(v[4 * k + 2]), __uint_as_float(v[4 * k + 3]));
+            if (accum) {
+              const float4 q = o[k];
+              x4.x += q.x; x4.y += q.y; x4.z += q.z; x4.w += q.w;
+            }
+            o[k] = x4;
+          }
+        } else {
+          uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(out) + p * cout + c0);
+          uint32_t pk[8];
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            pk[k] = pack_bf16(fmaxf(__uint_as_float(v[2 * k]) + bias[c0 + 2 * k], 0.0f),
+                              fmaxf(__uint_as_float(v[2 * k + 1]) + bias[c0 + 2 * k + 1], 0.0f));
+          o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_conv_timeout, 1);
+    mbar_wait(&bar[0], 0u);   // bounded: whatever MMAs are still in flight
+    mbar_wait(&bar[1], 1u);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
 // ---------------------------------------------------------------- weight gradient, tcgen05
 // part[chunk][co][tap * cin + ci] = sum_{p in chunk} dz[p][co] x[p + tap][ci]
 // as D (M x N) = A (M x K) B (K x N) on the fifth-generation tensor cores:
@@ -824,14 +1001,46 @@ int roundup8(int v) { return (v + 7) / 8 * 8; }
 
 }  // namespace
 
+size_t conv_tg_smem(int cin, int cout) {
+  const int nky = tg::rows_per_round(cin, cout);
+  const size_t need = (nky == 3 ? 1 : 2) * (size_t)tg::stage_bytes(cin, cout, nky) + 24 + 3 * 16 * 4 + 8;
+  const int fit = 512 / tc::tmem_cols(cout);
+  if (fit >= 16) return need;
+  const size_t cap = 228 * 1024 / (fit + 1) - 1024 + 16;
+  return std::max(need, cap);
+}
+
+template <bool F32>
+void conv_tg_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out, bool accum, int cout,
+                int N, int H, int W, cudaStream_t st) {
+  static const bool attr = [] {
+    SWFWI_CUDA(cudaFuncSetAttribute(k_conv3x3_tg<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    227 * 1024));
+    return true;
+  }();
+  (void)attr;
+  const long long groups = (long long)N * H * ((W + 7) / 8);
+  k_conv3x3_tg<F32><<<(unsigned)((groups + 15) / 16), 128, conv_tg_smem(cin, cout), st>>>(
+      in, cin, w, bias, out, accum ? 1 : 0, cout, N, H, W);
+  noted();
+}
+
 void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out,
                     bool out_f32, bool accum, int cout, int N, int H, int W, cudaStream_t st) {
   SWFWI_REQUIRE(cin > 0 && cin % 16 == 0 && cin <= 128 && cout > 0 && cout % 16 == 0 && cout <= 256,
                 "conv widths must be multiples of 16, at most 128 in and 256 out");
   SWFWI_REQUIRE(N > 0 && H > 0 && W > 0, "conv image size out of range");
   SWFWI_REQUIRE(out_f32 || bias, "BF16 conv output needs a bias");
-  if (out_f32) conv_tc_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
-  else conv_tc_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+  // row tiles (each input row staged once) where their stages fit twice on
+  // an SM, else the pixel-run tiles
+  const bool rows = conv_tg_smem(cin, cout) <= 100 * 1024;
+  if (out_f32) {
+    if (rows) conv_tg_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+    else conv_tc_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+  } else {
+    if (rows) conv_tg_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+    else conv_tc_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+  }
 }
 
 size_t conv3x3_wgrad_scratch(int cout, int cin, int N, int H, int W) {
