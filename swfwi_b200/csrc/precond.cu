@@ -254,13 +254,16 @@ __host__ __device__ inline int stage_bytes(int cin, int cout, int nky) {
 }
 }  // namespace tg
 
-template <bool F32>
-__global__ void __launch_bounds__(128) k_conv3x3_tg(const bf16 *__restrict__ in, int cin,
-                                                    const bf16 *__restrict__ w, const float *__restrict__ bias,
-                                                    void *out, int accum, int cout, int N, int H, int W) {
+// KC = cin / 16 is a template parameter: the staging's divisions by the
+// channel count are by constants.
+template <bool F32, int KC>
+__global__ void __launch_bounds__(128) k_conv3x3_tg(const bf16 *__restrict__ in, const bf16 *__restrict__ w,
+                                                    const float *__restrict__ bias, void *out, int accum, int cout,
+                                                    int N, int H, int W) {
   using namespace stream_detail;
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int KC = cin / 16, NKY = tg::rows_per_round(cin, cout), R = 3 / NKY, NS = R > 1 ? 2 : 1;
+  constexpr int cin = 16 * KC;
+  const int NKY = tg::rows_per_round(cin, cout), R = 3 / NKY, NS = R > 1 ? 2 : 1;
   const int SB = tg::stage_bytes(cin, cout, NKY), ABYTES = KC * 2 * NKY * tg::kPlaneRow;
   uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NS * SB);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
@@ -1010,19 +1013,34 @@ size_t conv_tg_smem(int cin, int cout) {
   return std::max(need, cap);
 }
 
-template <bool F32>
-void conv_tg_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out, bool accum, int cout,
-                int N, int H, int W, cudaStream_t st) {
+template <bool F32, int KC>
+void conv_tg_kc(const bf16 *in, const bf16 *w, const float *bias, void *out, bool accum, int cout, int N, int H,
+                int W, cudaStream_t st) {
   static const bool attr = [] {
-    SWFWI_CUDA(cudaFuncSetAttribute(k_conv3x3_tg<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SWFWI_CUDA(cudaFuncSetAttribute(k_conv3x3_tg<F32, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     227 * 1024));
     return true;
   }();
   (void)attr;
   const long long groups = (long long)N * H * ((W + 7) / 8);
-  k_conv3x3_tg<F32><<<(unsigned)((groups + 15) / 16), 128, conv_tg_smem(cin, cout), st>>>(
-      in, cin, w, bias, out, accum ? 1 : 0, cout, N, H, W);
+  k_conv3x3_tg<F32, KC><<<(unsigned)((groups + 15) / 16), 128, conv_tg_smem(16 * KC, cout), st>>>(
+      in, w, bias, out, accum ? 1 : 0, cout, N, H, W);
   noted();
+}
+
+// true when a row-tile kernel exists for cin
+template <bool F32>
+bool conv_tg_go(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out, bool accum, int cout,
+                int N, int H, int W, cudaStream_t st) {
+  switch (cin / 16) {
+    case 1: conv_tg_kc<F32, 1>(in, w, bias, out, accum, cout, N, H, W, st); return true;
+    case 2: conv_tg_kc<F32, 2>(in, w, bias, out, accum, cout, N, H, W, st); return true;
+    case 3: conv_tg_kc<F32, 3>(in, w, bias, out, accum, cout, N, H, W, st); return true;
+    case 4: conv_tg_kc<F32, 4>(in, w, bias, out, accum, cout, N, H, W, st); return true;
+    case 6: conv_tg_kc<F32, 6>(in, w, bias, out, accum, cout, N, H, W, st); return true;
+    case 8: conv_tg_kc<F32, 8>(in, w, bias, out, accum, cout, N, H, W, st); return true;
+    default: return false;
+  }
 }
 
 void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, void *out,
@@ -1035,11 +1053,11 @@ void launch_conv3x3(const bf16 *in, int cin, const bf16 *w, const float *bias, v
   // an SM, else the pixel-run tiles
   const bool rows = conv_tg_smem(cin, cout) <= 100 * 1024;
   if (out_f32) {
-    if (rows) conv_tg_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
-    else conv_tc_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
+    if (!(rows && conv_tg_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st)))
+      conv_tc_go<true>(in, cin, w, bias, out, accum, cout, N, H, W, st);
   } else {
-    if (rows) conv_tg_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
-    else conv_tc_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
+    if (!(rows && conv_tg_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st)))
+      conv_tc_go<false>(in, cin, w, bias, out, false, cout, N, H, W, st);
   }
 }
 
