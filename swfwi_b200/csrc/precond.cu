@@ -429,10 +429,13 @@ __host__ __device__ inline int wg_tiles(int cin) { return (9 * cin + 255) / 256;
 __host__ __device__ inline int wg_cols(int cin) { return ((9 * cin + wg_tiles(cin) - 1) / wg_tiles(cin) + 15) / 16 * 16; }
 __host__ __device__ inline int wg_stage_bytes(int cin) { return kWgRound * (4096 + 32 * wg_cols(cin)); }
 
+// CIN is a template parameter: the staging divides by constants.
+template <int CIN>
 __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dz, int cout, const bf16 *__restrict__ x,
-                                                  int cin, float *__restrict__ part, int N, int H, int W, int ppc) {
+                                                  float *__restrict__ part, int N, int H, int W, int ppc) {
   using namespace stream_detail;
   extern __shared__ __align__(1024) unsigned char sm[];
+  constexpr int cin = CIN;
   const int NT = 9 * cin, NNmax = wg_cols(cin);
   const int n0 = blockIdx.y * NNmax, NN = min(NNmax, NT - n0);   // this CTA's columns
   const int SB = wg_stage_bytes(cin);
@@ -973,19 +976,33 @@ size_t wgrad_tc_smem(int cin) {
   return std::max(need, cap);
 }
 
-void wgrad_tc_go(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, float *part, int N, int H, int W,
-                 cudaStream_t st) {
+template <int CIN>
+void wgrad_tc_cin(const bf16 *dz, int cout, const bf16 *x, float *part, int N, int H, int W, long long ppc,
+                  unsigned chunks, cudaStream_t st) {
   static const bool attr = [] {
-    SWFWI_CUDA(cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)wgrad_tc_smem(128)));   // the largest accepted width
+    SWFWI_CUDA(cudaFuncSetAttribute(k_wgrad_tc<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)wgrad_tc_smem(CIN)));
     return true;
   }();
   (void)attr;
+  dim3 grid(chunks, wg_tiles(CIN));
+  k_wgrad_tc<CIN><<<grid, 128, wgrad_tc_smem(CIN), st>>>(dz, cout, x, part, N, H, W, (int)ppc);
+}
+
+void wgrad_tc_go(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, float *part, int N, int H, int W,
+                 cudaStream_t st) {
   const long long P = (long long)N * H * W;
   const long long ppc = wgrad_pix_per_chunk(P, cin);
   const unsigned chunks = (unsigned)((P + ppc - 1) / ppc);
-  dim3 grid(chunks, wg_tiles(cin));
-  k_wgrad_tc<<<grid, 128, wgrad_tc_smem(cin), st>>>(dz, cout, x, cin, part, N, H, W, (int)ppc);
+  switch (cin) {
+    case 16: wgrad_tc_cin<16>(dz, cout, x, part, N, H, W, ppc, chunks, st); break;
+    case 32: wgrad_tc_cin<32>(dz, cout, x, part, N, H, W, ppc, chunks, st); break;
+    case 48: wgrad_tc_cin<48>(dz, cout, x, part, N, H, W, ppc, chunks, st); break;
+    case 64: wgrad_tc_cin<64>(dz, cout, x, part, N, H, W, ppc, chunks, st); break;
+    case 96: wgrad_tc_cin<96>(dz, cout, x, part, N, H, W, ppc, chunks, st); break;
+    case 128: wgrad_tc_cin<128>(dz, cout, x, part, N, H, W, ppc, chunks, st); break;
+    default: throw Error(SWFWI_ERR_BAD_ARG, "weight gradient: input width must be 16/32/48/64/96/128");
+  }
   noted();
   const long long len = (long long)cout * 9 * cin;
   k_reduce_rows<<<blocks_for(len), kEw, 0, st>>>(part, (int)chunks, len, dw);
@@ -1070,7 +1087,8 @@ size_t conv3x3_wgrad_scratch(int cout, int cin, int N, int H, int W) {
 void launch_conv3x3_wgrad(const bf16 *dz, int cout, const bf16 *x, int cin, float *dw, float *scratch,
                           size_t scratch_floats, int N, int H, int W, cudaStream_t st) {
   SWFWI_REQUIRE(cout > 0 && cout % 16 == 0 && cout <= 128, "weight gradient: output width must be a multiple of 16, at most 128");
-  SWFWI_REQUIRE(cin > 0 && cin % 16 == 0 && cin <= 128, "weight gradient: input width must be a multiple of 16, at most 128");
+  SWFWI_REQUIRE(cin == 16 || cin == 32 || cin == 48 || cin == 64 || cin == 96 || cin == 128,
+                "weight gradient: input width must be 16/32/48/64/96/128");
   SWFWI_REQUIRE(scratch && scratch_floats >= conv3x3_wgrad_scratch(cout, cin, N, H, W),
                 "weight gradient scratch too small");
   wgrad_tc_go(dz, cout, x, cin, dw, scratch, N, H, W, st);
