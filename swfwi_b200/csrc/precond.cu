@@ -44,11 +44,12 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 // T x cin/16 tcgen05.mma into the FP32 accumulator in tensor memory and
 // commits them to the stage's mbarrier; a stage is refilled only after its
 // barrier shows those MMAs done (bounded waits).  Narrow layers take all 9
-// taps in one round: one copy, MMA and commit latency per CTA instead of 9.  The epilogue reads the
-// accumulator 16 columns at a time (warp w holds the tensor-memory lanes,
-// i.e. pixels, 32w .. 32w+31) and writes BF16 with bias and ReLU, or FP32
-// (optionally added to the output).  A wait that gives up sets
-// g_conv_timeout; the CTA still frees its tensor memory.
+// taps in one round: one copy, MMA and commit latency per CTA instead of 9.
+// The epilogue reads the accumulator 16 columns at a time (warp w holds the
+// tensor-memory lanes, i.e. pixels, 32w .. 32w+31) and writes BF16 with
+// bias and ReLU, or FP32 (optionally added to the output).  A wait that
+// gives up sets g_conv_timeout; the CTA still frees its tensor memory.
+// (The row-tile kernel below replaces this one wherever its stages fit.)
 __device__ int g_conv_timeout;
 
 namespace tc {
